@@ -1,0 +1,242 @@
+/*
+ * negf_b200.h -- C ABI of the B200 block-tridiagonal NEGF library
+ * (libnegf_b200.so, sm_100a CUDA).
+ *
+ * It is the drop-in boundary for LibNEGF.jl's hot path: every entry point
+ * below replaces one reference interface, cited as file:line within the
+ * LibNEGF.jl project.  A Julia backend (backend_nvidia.jl, beside
+ * src/backend_cpu.jl) reaches these functions through ccall only.
+ *
+ * Conventions
+ *  - Matrices are complex128 (two doubles, re then im; C99 `double _Complex`,
+ *    Julia ComplexF64), column-major with a leading dimension, exactly as
+ *    Julia stores a Matrix{ComplexF64}.
+ *  - "dptr" arguments are DEVICE pointers (cudaMalloc / CuArray / torch);
+ *    arrays of dptrs are HOST arrays of device pointers.  Functions that take
+ *    host data say so.
+ *  - `stream` is a cudaStream_t (NULL: the legacy default stream).  Sweep
+ *    entry points synchronise the stream before returning so that they can
+ *    report singular pivots; the plan API does not.
+ *  - Every function returns NEGF_SUCCESS or an error code; negf_last_error()
+ *    returns the message of the last failure on the calling thread.  The
+ *    reference prints and calls exit() on a LAPACK failure
+ *    (src/backend_cpu.jl:151-155); this library returns NEGF_ERR_SINGULAR.
+ *  - There is no CPU fallback: without a usable CUDA device every call
+ *    returns NEGF_ERR_CUDA.
+ */
+#ifndef NEGF_B200_H
+#define NEGF_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NEGF_SUCCESS 0
+#define NEGF_ERR_INVALID 1   /* bad argument */
+#define NEGF_ERR_CUDA 2      /* CUDA runtime error / no device */
+#define NEGF_ERR_SINGULAR 3  /* zero pivot in a diagonal block */
+#define NEGF_ERR_NOMEM 4     /* device allocation failed */
+
+/* Message of the last failure on this thread ("" when none). */
+const char* negf_last_error(void);
+/* Library version, 100 * major + minor. */
+int negf_version(void);
+
+/* ------------------------------------------------------------------------
+ * Backend primitives (the be_* layer of src/backend_cpu.jl), batched.
+ * ---------------------------------------------------------------------- */
+
+/* One GEMM problem:  C = alpha * op(A) * op(B) + beta * Cin + diag * I.
+ * op(A) is m x k, op(B) is k x n; Cin may equal C; k = 0 gives
+ * C = beta * Cin + diag * I. */
+typedef struct {
+  const void* A; /* dptr */
+  const void* B; /* dptr */
+  const void* Cin; /* dptr or NULL */
+  void* C;       /* dptr */
+  int32_t m, n, k;
+  int32_t lda, ldb, ldc, ldcin;
+  double alpha[2], beta[2], diag[2];
+} negf_zgemm_problem;
+
+/* Batched be_gemm! (src/backend_cpu.jl:208-219): all problems share
+ * opA, opB in {'N','T','C'}.  One launch on the FP64 tensor path. */
+int negf_zgemm_batched(char opA, char opB, int32_t nprob, const negf_zgemm_problem* probs, void* stream);
+
+/* Batched be_copy_in_hw! / be_ctranspose! (src/backend_cpu.jl:42-68):
+ * C[i] = op(A[i]) with op 'N' (copy) or 'C' (conjugate transpose); C[i] is
+ * m[i] x n[i] (A[i] is n[i] x m[i] for 'C'). */
+int negf_zcopy_batched(char op, int32_t nprob, const int32_t* m, const int32_t* n, void* const* A,
+                       const int32_t* lda, void* const* C, const int32_t* ldc, void* stream);
+
+/* Batched inversion Ainv[i] = A[i]^{-1} by blocked Gauss-Jordan with partial
+ * pivoting; replaces be_lu! + be_mldivide!(identity) / be_inv_from_lu!
+ * (src/backend_cpu.jl:147-206).  A[i] is not modified.  n[i] <= 1024.
+ * info (host, nprob entries, may be NULL) receives 0 or the first zero-pivot
+ * column (1-based) per matrix. */
+int negf_zinv_batched(int32_t nprob, const int32_t* n, void* const* A, const int32_t* lda, void* const* Ainv,
+                      const int32_t* ldainv, int32_t* info, void* stream);
+
+/* Batched LU with partial pivoting, in place, LAPACK getrf semantics;
+ * replaces be_lu! / be_getrf! (src/backend_cpu.jl:147-169, :255-265).
+ * ipiv (dptrs, may be NULL entries) receives 1-based LAPACK pivots. */
+int negf_zgetrf_batched(int32_t nprob, const int32_t* n, void* const* A, const int32_t* lda, void* const* ipiv,
+                        int32_t* info, void* stream);
+
+/* Batched triangular solve with the factors of negf_zgetrf_batched /
+ * be_trsm! (src/backend_cpu.jl:241-253): B[i] = alpha * op(T)^{-1} B[i]
+ * (side 'L') or alpha * B[i] op(T)^{-1} (side 'R'), T the upper ('U') or
+ * unit/non-unit lower ('L') triangle of A[i]; trans 'N' only. */
+int negf_ztrsm_batched(char side, char uplo, char trans, char diag, const double* alpha, int32_t nprob,
+                       const int32_t* m, const int32_t* n, void* const* A, const int32_t* lda, void* const* B,
+                       const int32_t* ldb, void* stream);
+
+/* Batched be_getri! with identity pivots (src/backend_cpu.jl:229-239):
+ * A[i] (holding L\U factors) is replaced by U^{-1} L^{-1}. */
+int negf_zgetri_nopiv_batched(int32_t nprob, const int32_t* n, void* const* A, const int32_t* lda, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Whole-sweep entry points (the reference's algorithm functions).
+ * nsys independent systems of npl layers; block_sizes holds nsys*npl sizes
+ * (system-major); block dptr tables are system-major: Md[s*npl + i] is
+ * M[i,i] of system s, Mu[s*(npl-1)+i] is M[i,i+1], Ml[s*(npl-1)+i] is M[i+1,i].
+ * Blocks are dense with ld = their row count.
+ * ---------------------------------------------------------------------- */
+
+/* Block tridiagonal of M^{-1} by RGF: bndiag_of_inv_rgf_local!
+ * (src/matinvertndiag_rgf.jl:114-200).  Gu / Gl may be NULL.  With Gfull
+ * (nsys*npl*npl dptrs, row-major block index i*npl+j, NULL entries skipped)
+ * every block of the inverse is written (buildFullInv, rgf.jl:185-199). */
+int negf_rgf(int32_t nsys, int32_t npl, const int32_t* block_sizes, void* const* Md, void* const* Mu,
+             void* const* Ml, void* const* Gd, void* const* Gu, void* const* Gl, void* const* Gfull, void* stream);
+
+/* Block tridiagonal of G^n = M^{-1} S M^{-H} by recursive Keldysh:
+ * keldyshndiag! (src/keldyshndiag.jl:120-317).  S is Hermitian, given as
+ * diagonal blocks Sd (nsys*npl) and upper blocks Su (nsys*(npl-1)); it is
+ * overwritten with G^n in the same storage (the reference's auxData.buffS). */
+int negf_keldysh(int32_t nsys, int32_t npl, const int32_t* block_sizes, void* const* Md, void* const* Mu,
+                 void* const* Ml, void* const* Sd, void* const* Su, void* stream);
+
+/* Block n-diagonal (bandwidth w = (ndiag-1)/2) of M^{-1}:
+ * bndiag_of_inv_general_rgf! (src/matinvertndiag_general_rgf.jl:31-146).
+ * Mb holds nsys*npl*npl dptrs (row-major block index i*npl+j), non-NULL
+ * exactly for |i-j| <= w; Gb likewise for the output.  Mb is not modified
+ * (the reference overwrites Min, :86). */
+int negf_general_rgf(int32_t nsys, int32_t npl, int32_t ndiag, const int32_t* block_sizes, void* const* Mb,
+                     void* const* Gb, void* stream);
+
+/* Selected inverse on a general block pattern: Block_factorization! then
+ * Block_inverse! (src/selected_inverse.jl:9-55, :139-206).  Ab holds
+ * npl*npl dptrs (row-major block index), NULL where the block is unassigned;
+ * fill-in blocks created by the factorisation must be provided (pre-zeroed)
+ * and flagged in fill (npl*npl bytes, 1 = fill-in).  All blocks have size b.
+ * mode: 1 = factorisation only, 2 = inverse only (Ab holds factors),
+ * 3 = both.  In place. */
+int negf_selected_inverse(int32_t npl, int32_t b, void* const* Ab, const uint8_t* fill, int32_t mode, void* stream);
+
+/* Domain-decomposed RGF: bndiag_of_inv_ddrgf! with one level
+ * (src/matinvertndiag_ddrgf_core.jl:719-758) and the reference's partition
+ * (separators of one layer at t*(D1+1), src/matinvertndiag_ddrgf_utils.jl:
+ * 278-312, :478-575).  block_size_d1 <= 0 picks the partition from the
+ * library's cost model.  Output as negf_rgf (Gu/Gl may be NULL).
+ * schur (optional, nsys*3*ntasks dptrs: diag, upper, lower of the separator
+ * Schur complement) receives the Schur complement blocks. */
+int negf_ddrgf(int32_t nsys, int32_t npl, const int32_t* block_sizes, void* const* Md, void* const* Mu,
+               void* const* Ml, int32_t block_size_d1, void* const* Gd, void* const* Gu, void* const* Gl,
+               void* stream);
+
+/* The reference's partition helper (src/matinvertndiag_ddrgf_utils.jl:
+ * 278-312): writes nr_tasks (-1: impossible) and the last interior size. */
+int negf_ddrgf_get_nr_tasks(int32_t npl, int32_t block_size_d1, int32_t* nr_tasks, int32_t* last_d1);
+/* Partition choice of the library's cost model for npl layers of size b. */
+int negf_ddrgf_choose_d1(int32_t npl, int32_t b, int32_t nsys, int32_t* block_size_d1);
+
+/* ------------------------------------------------------------------------
+ * Batched-energy NEGF solver (the reference has no energy loop; this is the
+ * batched form of running RGF + keldyshndiag! per energy point).
+ * M(E) = (E + i eta) I - H - Sigma, Sigma_L on layer 0, Sigma_R on layer
+ * N-1; Gamma = i (Sigma - Sigma^H); Sigma^in = f_L Gamma_L (+) f_R Gamma_R;
+ * G^< = i G^R Sigma^in G^A; T(E) = Re Tr[Gamma_L G^R_{1N} Gamma_R G^A_{N1}].
+ * ---------------------------------------------------------------------- */
+typedef struct negf_device_s* negf_device_t;
+
+/* Upload one device: Hd[i] (npl host pointers, b_i x b_i), Hu[i]
+ * (npl-1 host pointers, b_i x b_{i+1}, H_{i+1,i} = Hu[i]^H), sigL (b_0 x b_0),
+ * sigR (b_{N-1} x b_{N-1}); all complex128 column-major host arrays. */
+int negf_device_create(int32_t npl, const int32_t* block_sizes, const void* const* Hd, const void* const* Hu,
+                       const void* sigL, const void* sigR, negf_device_t* out);
+/* Re-upload H and the self-energies of an existing device (same sizes);
+ * solvers built on the device stay valid. */
+int negf_device_upload(negf_device_t dev, const void* const* Hd, const void* const* Hu, const void* sigL,
+                       const void* sigR);
+int negf_device_destroy(negf_device_t dev);
+
+typedef struct {
+  double eta, mu_l, mu_r, kT;
+  int32_t want_gr;   /* diagonal G^R blocks */
+  int32_t want_gl;   /* diagonal G^< blocks */
+  int32_t want_t;    /* transmission */
+  int32_t max_chunk; /* energies per device-resident batch (0: by HBM budget) */
+  double hbm_budget_gb; /* 0: 80% of free device memory */
+} negf_solve_opts;
+
+/* Solve nE energy points (energies: host array).  gr_out / gl_out receive
+ * nE * sum_i b_i^2 complex128 values (energy-major, then layer, column-major
+ * blocks); t_out receives nE doubles.  Outputs are HOST pointers unless
+ * out_on_device != 0.  NULL outputs are skipped. */
+int negf_solve(negf_device_t dev, int32_t nE, const double* energies, const negf_solve_opts* opts, void* gr_out,
+               void* gl_out, double* t_out, int32_t out_on_device, void* stream);
+
+/* Resident-plan form of negf_solve for repeated solves of a fixed number of
+ * energies with inputs and outputs kept in device memory. */
+typedef struct negf_solver_s* negf_solver_t;
+int negf_solver_create(negf_device_t dev, int32_t nE, const negf_solve_opts* opts, negf_solver_t* out);
+int negf_solver_destroy(negf_solver_t s);
+/* energies: host array of nE values (uploaded to a device parameter table). */
+int negf_solver_set_energies(negf_solver_t s, const double* energies, void* stream);
+/* One pass over all energies (captured into a CUDA graph on first use). */
+int negf_solver_run(negf_solver_t s, void* stream);
+/* Device pointers of the resident outputs (valid until destroy): gr/gl as in
+ * negf_solve; t_dev holds 2*nE doubles (re, im of the trace per energy). */
+int negf_solver_outputs(negf_solver_t s, void** gr_dev, void** gl_dev, double** t_dev);
+/* Synchronous check of the zero-pivot flags of the last run. */
+int negf_solver_check(negf_solver_t s);
+/* Real flops of one pass (8mnk per complex GEMM, 8n^3 per inversion),
+ * number of kernel launches per pass and workspace bytes. */
+int negf_solver_stats(negf_solver_t s, double* flops, int64_t* launches, int64_t* workspace_bytes);
+
+/* ------------------------------------------------------------------------
+ * Reference C ABI: src/c_interface/libnegf_c_interface.h:12-38.
+ * Same struct layout and signature, so libnegf_c_example.c links unchanged.
+ * Runs DDRGF (the reference's wrapper does, libnegf_c_interface.jl:119) on
+ * the block n-diagonal band of the input CSC matrix; the returned arrays are
+ * malloc'd and freed by the caller with free().  On failure the result has
+ * m = n = nnz = 0 and NULL arrays (the reference has no error channel).
+ * ---------------------------------------------------------------------- */
+typedef struct {
+  int32_t m;
+  int32_t n;
+  int32_t nnz;
+  int32_t* colptr;
+  int32_t* rowval;
+  void* nzval; /* double complex* */
+} CCscMatrix;
+
+CCscMatrix run_bndiag_wrapper(int32_t m, int32_t n, int32_t nnz_in, int32_t* colptr_in, int32_t* rowval_in,
+                              void* nzval_in, int32_t n_blocks, int32_t* block_sizes_in, int32_t n_dict,
+                              const char** dict_keys_in, int32_t* dict_vals_in, int32_t is_hermitian);
+
+/* ------------------------------------------------------------------------
+ * Measurement helper: FP64 throughput of the tensor (mma.sync f64) and
+ * DFMA paths on the current device, TFLOP/s (the roofline denominator of
+ * the FP64 path; MEASURED_PEAKS.json has no FP64 figure).
+ * ---------------------------------------------------------------------- */
+int negf_probe_fp64_peak(double* dmma_tflops, double* dfma_tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NEGF_B200_H */

@@ -1,0 +1,679 @@
+// Sweep planner: turns the reference's per-block call sequences into batched
+// launches (one launch per recursion step over all systems).
+#include "engine.h"
+
+#include <algorithm>
+#include <cstring>
+#include <set>
+
+namespace negf {
+
+cudaError_t zgj_prepare(size_t smem);
+
+namespace {
+thread_local std::string g_last_error;
+
+inline ZGemmProblem gp(const cplx* A, int lda, const cplx* B, int ldb, cplx* C, int ldc, int m, int n, int k,
+                       cplx alpha, const cplx* Cin = nullptr, int ldcin = 1, cplx beta = {0.0, 0.0},
+                       cplx diag = {0.0, 0.0}) {
+  ZGemmProblem p;
+  p.A = A; p.B = B; p.Cin = Cin; p.C = C; p.diag_ptr = nullptr;
+  p.m = m; p.n = n; p.k = k;
+  p.lda = lda > 0 ? lda : 1; p.ldb = ldb > 0 ? ldb : 1; p.ldc = ldc; p.ldcin = ldcin > 0 ? ldcin : 1;
+  p.pad_ = 0;
+  p.alpha = alpha; p.beta = beta; p.diag = diag;
+  return p;
+}
+constexpr cplx ONE{1.0, 0.0};
+constexpr cplx MONE{-1.0, 0.0};
+constexpr cplx ZERO{0.0, 0.0};
+inline cplx cscale(cplx a, double s) { return make_double2(a.x * s, a.y * s); }
+}  // namespace
+
+std::string& last_error() { return g_last_error; }
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int gj_panel_width(int max_n) {
+  if (max_n <= 112) return max_n;
+  if (max_n <= 400) return 32;
+  if (max_n <= 800) return 16;
+  return 8;
+}
+
+int TriSystem::maxb() const {
+  int m = 0;
+  for (int x : b) m = std::max(m, x);
+  return m;
+}
+
+// ---------------------------------------------------------------------------
+// Plan
+
+Plan::~Plan() {
+  if (gexec_) cudaGraphExecDestroy(gexec_);
+  if (graph_) cudaGraphDestroy(graph_);
+  if (dblob_) cudaFree(dblob_);
+  for (void* p : owned_) cudaFree(p);
+}
+
+void* Plan::alloc(size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  void* p = nullptr;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) throw std::bad_alloc();
+  if (cudaMemset(p, 0, bytes) != cudaSuccess) {
+    cudaFree(p);
+    throw std::bad_alloc();
+  }
+  owned_.push_back(p);
+  owned_bytes_ += bytes;
+  return p;
+}
+
+size_t Plan::push_bytes(const void* p, size_t n) {
+  size_t off = (blob_.size() + 255) & ~size_t(255);
+  blob_.resize(off + n);
+  if (n) std::memcpy(blob_.data() + off, p, n);
+  return off;
+}
+
+void Plan::gemm(char opA, char opB, const std::vector<ZGemmProblem>& probs) {
+  std::vector<ZGemmProblem> v;
+  std::vector<int> starts;
+  int total = 0;
+  double fl = 0.0;
+  for (const auto& p : probs) {
+    int t = zgemm_tiles(p.m, p.n);
+    if (t == 0) continue;
+    v.push_back(p);
+    starts.push_back(total);
+    total += t;
+    fl += 8.0 * p.m * (double)p.n * p.k;
+  }
+  if (v.empty()) return;
+  Step s;
+  s.kind = Step::GEMM;
+  s.opA = opA;
+  s.opB = opB;
+  s.off = push_bytes(v.data(), v.size() * sizeof(ZGemmProblem));
+  s.tiles_off = push_bytes(starts.data(), starts.size() * sizeof(int));
+  s.count = static_cast<int>(v.size());
+  s.total_tiles = total;
+  s.flops = fl;
+  steps.push_back(s);
+}
+
+void Plan::inv(const std::vector<InvSpec>& specs) {
+  std::vector<ZInvProblem> v;
+  int max_n = 0;
+  for (const auto& sp : specs) {
+    if (sp.n <= 0) continue;
+    ZInvProblem p;
+    p.W = sp.W; p.F = sp.F; p.Bbuf = sp.Bbuf; p.used = sp.used; p.piv = sp.piv; p.out = sp.out;
+    p.info = sp.info; p.n = sp.n; p.ld = sp.ld; p.ldo = sp.ldo; p.pad_ = 0;
+    v.push_back(p);
+    max_n = std::max(max_n, sp.n);
+  }
+  if (v.empty()) return;
+  int nb = gj_panel_width(max_n);
+  bool blocked = nb < max_n;
+  size_t off = push_bytes(v.data(), v.size() * sizeof(ZInvProblem));
+  double gj_flops = 0.0;
+  for (const auto& p : v) gj_flops += 8.0 * p.n * (double)p.n * p.n;
+  if (!blocked) {
+    Step s;
+    s.kind = Step::GJ_PANEL;
+    s.off = off; s.count = (int)v.size(); s.k0 = 0; s.nb = nb; s.blocked = 0;
+    s.smem = zgj_panel_smem_bytes(max_n, nb);
+    s.max_n = max_n;
+    s.flops = gj_flops;
+    steps.push_back(s);
+    return;
+  }
+  for (int k0 = 0; k0 < max_n; k0 += nb) {
+    Step s;
+    s.kind = Step::GJ_PANEL;
+    s.off = off; s.count = (int)v.size(); s.k0 = k0; s.nb = nb; s.blocked = 1;
+    s.smem = zgj_panel_smem_bytes(max_n, nb);
+    s.max_n = max_n;
+    steps.push_back(s);
+    std::vector<ZGemmProblem> g;
+    for (const auto& p : v) {
+      if (p.n <= k0) continue;
+      int w = std::min(nb, p.n - k0);
+      g.push_back(gp(p.F, p.n, p.Bbuf, w, p.W, p.ld, p.n, p.n, w, ONE, p.W, p.ld, ONE));
+    }
+    gemm('N', 'N', g);
+  }
+  // the GEMM updates carry their own flop count; the panel work is the rest
+  Step u;
+  u.kind = Step::GJ_UNPERMUTE;
+  u.off = off; u.count = (int)v.size(); u.max_n = max_n;
+  steps.push_back(u);
+}
+
+int lu_panel_width(int max_n) {
+  if (max_n <= 96) return max_n;
+  if (max_n <= 400) return 32;
+  if (max_n <= 800) return 16;
+  return 8;
+}
+
+void Plan::getrf(const std::vector<LuSpec>& specs) {
+  std::vector<ZLuProblem> v;
+  int max_n = 0;
+  for (const auto& s : specs) {
+    if (s.n <= 0) continue;
+    ZLuProblem p;
+    p.A = s.A; p.ipiv = s.ipiv; p.Linv = s.Linv; p.T = s.T; p.info = s.info;
+    p.n = s.n; p.ld = s.ld; p.pad0_ = p.pad1_ = 0;
+    v.push_back(p);
+    max_n = std::max(max_n, s.n);
+  }
+  if (v.empty()) return;
+  const int nb = lu_panel_width(max_n);
+  size_t off = push_bytes(v.data(), v.size() * sizeof(ZLuProblem));
+  for (int k0 = 0; k0 < max_n; k0 += nb) {
+    Step s;
+    s.kind = Step::LU_PANEL;
+    s.off = off; s.count = (int)v.size(); s.k0 = k0; s.nb = nb; s.max_n = max_n;
+    s.smem = zgetrf_panel_smem_bytes(max_n - k0, nb);
+    steps.push_back(s);
+    if (nb >= max_n) break;
+    Step w = s;
+    w.kind = Step::LU_SWAP;
+    w.smem = 0;
+    steps.push_back(w);
+    // A12 = L11^{-1} T ;  A22 -= A21 A12
+    std::vector<ZGemmProblem> g1, g2;
+    for (const auto& p : v) {
+      if (p.n <= k0 + nb) continue;
+      int wd = std::min(nb, p.n - k0);
+      int rest = p.n - k0 - wd;
+      cplx* A12 = p.A + k0 + (size_t)(k0 + wd) * p.ld;
+      g1.push_back(gp(p.Linv, wd, p.T, wd, A12, p.ld, wd, rest, wd, ONE));
+      const cplx* A21 = p.A + (k0 + wd) + (size_t)k0 * p.ld;
+      cplx* A22 = p.A + (k0 + wd) + (size_t)(k0 + wd) * p.ld;
+      g2.push_back(gp(A21, p.ld, A12, p.ld, A22, p.ld, rest, rest, wd, MONE, A22, p.ld, ONE));
+    }
+    gemm('N', 'N', g1);
+    gemm('N', 'N', g2);
+  }
+}
+
+void Plan::trtri(const std::vector<TriSpec>& specs, bool upper) {
+  std::vector<ZTriProblem> v;
+  int max_n = 0;
+  std::vector<ZBlockOp> zero;
+  for (const auto& s : specs) {
+    if (s.n <= 0) continue;
+    ZTriProblem p;
+    p.A = s.A; p.X = s.X; p.n = s.n; p.lda = s.lda; p.ldx = s.ldx; p.pad_ = 0;
+    v.push_back(p);
+    max_n = std::max(max_n, s.n);
+    ZBlockOp z{};
+    z.C = s.X; z.ldc = s.ldx; z.m = z.n = s.n; z.kind = ZOP_FILL;
+    zero.push_back(z);
+  }
+  if (v.empty()) return;
+  blockops(zero);
+  const int nb = kTriNb;
+  Step s;
+  s.kind = Step::TRI_DIAG;
+  s.off = push_bytes(v.data(), v.size() * sizeof(ZTriProblem));
+  s.count = (int)v.size(); s.nb = nb; s.blocked = upper ? 1 : 0; s.max_n = max_n;
+  s.smem = ztrtri_smem_bytes(nb);
+  steps.push_back(s);
+  const int q = (max_n + nb - 1) / nb;
+  for (int j = 1; j < q; ++j) {
+    std::vector<ZGemmProblem> g1, g2;
+    for (size_t t = 0; t < v.size(); ++t) {
+      const ZTriProblem& p = v[t];
+      const TriSpec& sp = specs[t];
+      int j0 = j * nb;
+      if (j0 >= p.n) continue;
+      int wj = std::min(nb, p.n - j0);
+      if (upper) {
+        // T = X[0:j0, 0:j0] U[0:j0, j-block];  X[0:j0, j-block] = -T X[j-block, j-block]
+        g1.push_back(gp(p.X, p.ldx, p.A + (size_t)j0 * p.lda, p.lda, sp.T, p.n, j0, wj, j0, ONE));
+        g2.push_back(gp(sp.T, p.n, p.X + j0 + (size_t)j0 * p.ldx, p.ldx, p.X + (size_t)j0 * p.ldx, p.ldx, j0, wj,
+                        wj, MONE));
+      } else {
+        // T = L[j-block, 0:j0] Y[0:j0, 0:j0];  Y[j-block, 0:j0] = -Y[j-block, j-block] T
+        g1.push_back(gp(p.A + j0, p.lda, p.X, p.ldx, sp.T, nb, wj, j0, j0, ONE));
+        g2.push_back(gp(p.X + j0 + (size_t)j0 * p.ldx, p.ldx, sp.T, nb, p.X + j0, p.ldx, wj, j0, wj, MONE));
+      }
+    }
+    gemm('N', 'N', g1);
+    gemm('N', 'N', g2);
+  }
+}
+
+void Plan::blockops(const std::vector<ZBlockOp>& ops) {
+  if (ops.empty()) return;
+  Step s;
+  s.kind = Step::BLOCKOP;
+  s.off = push_bytes(ops.data(), ops.size() * sizeof(ZBlockOp));
+  s.count = (int)ops.size();
+  for (const auto& o : ops) { s.max_m = std::max(s.max_m, o.m); s.max_n = std::max(s.max_n, o.n); }
+  steps.push_back(s);
+}
+
+void Plan::trace(const std::vector<ZTraceProblemHost>& probs) {
+  if (probs.empty()) return;
+  Step s;
+  s.kind = Step::TRACE;
+  s.off = push_bytes(probs.data(), probs.size() * sizeof(ZTraceProblemHost));
+  s.count = (int)probs.size();
+  steps.push_back(s);
+}
+
+cudaError_t Plan::finalize() {
+  if (finalized_) return cudaSuccess;
+  if (!blob_.empty()) {
+    cudaError_t e = cudaMalloc(&dblob_, blob_.size());
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpy(dblob_, blob_.data(), blob_.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return e;
+  }
+  std::set<std::pair<char, char>> ops;
+  size_t max_smem = 0, lu_smem = 0, tri_smem = 0;
+  for (const auto& s : steps) {
+    if (s.kind == Step::GEMM) ops.insert({s.opA, s.opB});
+    if (s.kind == Step::GJ_PANEL) max_smem = std::max(max_smem, s.smem);
+    if (s.kind == Step::LU_PANEL) lu_smem = std::max(lu_smem, s.smem);
+    if (s.kind == Step::TRI_DIAG) tri_smem = std::max(tri_smem, s.smem);
+  }
+  if (lu_smem || tri_smem) {
+    cudaError_t e = zlu_prepare(lu_smem, tri_smem);
+    if (e != cudaSuccess) return e;
+  }
+  for (auto& o : ops) {
+    cudaError_t e = zgemm_prepare(o.first, o.second);
+    if (e != cudaSuccess) return e;
+  }
+  if (max_smem) {
+    cudaError_t e = zgj_prepare(max_smem);
+    if (e != cudaSuccess) return e;
+  }
+  finalized_ = true;
+  return cudaSuccess;
+}
+
+double Plan::flops() const {
+  double f = 0.0;
+  for (const auto& s : steps) f += s.flops;
+  return f;
+}
+
+size_t Plan::num_launches() const { return steps.size(); }
+
+cudaError_t Plan::run(cudaStream_t stream, bool use_graph) {
+  cudaError_t e = finalize();
+  if (e != cudaSuccess) return e;
+  if (use_graph && gexec_ && graph_stream_ == stream) return cudaGraphLaunch(gexec_, stream);
+  if (use_graph) {
+    e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+  }
+  const unsigned char* base = static_cast<const unsigned char*>(dblob_);
+  for (const auto& s : steps) {
+    switch (s.kind) {
+      case Step::GEMM:
+        e = launch_zgemm_batched(s.opA, s.opB, reinterpret_cast<const ZGemmProblem*>(base + s.off),
+                                 reinterpret_cast<const int*>(base + s.tiles_off), s.count, s.total_tiles, stream);
+        break;
+      case Step::GJ_PANEL:
+        e = launch_zgj_panel(reinterpret_cast<const ZInvProblem*>(base + s.off), s.count, s.k0, s.nb, s.blocked,
+                             s.smem, stream);
+        break;
+      case Step::GJ_UNPERMUTE:
+        e = launch_zgj_unpermute(reinterpret_cast<const ZInvProblem*>(base + s.off), s.count, s.max_n, stream);
+        break;
+      case Step::BLOCKOP:
+        e = launch_zblockops(reinterpret_cast<const ZBlockOp*>(base + s.off), s.count, s.max_m, s.max_n, stream);
+        break;
+      case Step::TRACE:
+        e = launch_ztrace_prod(base + s.off, s.count, stream);
+        break;
+      case Step::LU_PANEL:
+        e = launch_zgetrf_panel(base + s.off, s.count, s.k0, s.nb, s.smem, stream);
+        break;
+      case Step::LU_SWAP:
+        e = launch_zlaswp_copy(base + s.off, s.count, s.k0, s.nb, s.max_n, stream);
+        break;
+      case Step::TRI_DIAG:
+        e = launch_ztrtri_diag(base + s.off, s.count, s.nb, s.blocked, s.max_n, s.smem, stream);
+        break;
+    }
+    if (e != cudaSuccess) break;
+  }
+  if (use_graph) {
+    cudaGraph_t g = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(stream, &g);
+    if (e != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return e;
+    }
+    if (e2 != cudaSuccess) return e2;
+    if (gexec_) cudaGraphExecDestroy(gexec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    graph_ = g;
+    e = cudaGraphInstantiate(&gexec_, graph_, 0);
+    if (e != cudaSuccess) return e;
+    graph_stream_ = stream;
+    return cudaGraphLaunch(gexec_, stream);
+  }
+  return e;
+}
+
+// ---------------------------------------------------------------------------
+// RGF
+
+void alloc_rgf_work(Plan& plan, const TriSystem& s, RgfWork& w) {
+  int n = s.npl();
+  int mb = s.maxb();
+  int nb = gj_panel_width(mb);
+  w.g.assign(n, nullptr);
+  w.R.assign(n > 0 ? n - 1 : 0, nullptr);
+  w.L.assign(n > 0 ? n - 1 : 0, nullptr);
+  size_t total = 0;
+  for (int i = 0; i < n; ++i) total += (size_t)s.b[i] * s.b[i];
+  for (int i = 0; i + 1 < n; ++i) total += 2 * (size_t)s.b[i] * s.b[i + 1];
+  total += (size_t)mb * mb;              // W
+  total += 2 * (size_t)mb * nb;          // F, Bbuf
+  cplx* arena = plan.alloc_c(total);
+  size_t o = 0;
+  for (int i = 0; i < n; ++i) { w.g[i] = arena + o; o += (size_t)s.b[i] * s.b[i]; }
+  for (int i = 0; i + 1 < n; ++i) {
+    w.R[i] = arena + o; o += (size_t)s.b[i] * s.b[i + 1];
+    w.L[i] = arena + o; o += (size_t)s.b[i] * s.b[i + 1];
+  }
+  w.W = arena + o; o += (size_t)mb * mb;
+  w.F = arena + o; o += (size_t)mb * nb;
+  w.Bbuf = arena + o; o += (size_t)mb * nb;
+  w.used = static_cast<uint8_t*>(plan.alloc(mb));
+  w.piv = static_cast<int*>(plan.alloc(sizeof(int) * mb));
+}
+
+static InvSpec inv_spec(const TriSystem& s, RgfWork& w, int i) {
+  InvSpec sp;
+  sp.W = w.W; sp.n = s.b[i]; sp.ld = s.b[i];
+  sp.out = w.g[i]; sp.ldo = s.b[i];
+  sp.F = w.F; sp.Bbuf = w.Bbuf; sp.used = w.used; sp.piv = w.piv; sp.info = s.info;
+  return sp;
+}
+
+void build_rgf_upward(Plan& plan, const std::vector<TriSystem>& sys, std::vector<RgfWork>& work) {
+  int maxN = 0;
+  for (const auto& s : sys) maxN = std::max(maxN, s.npl());
+  // bottom layer: X_{N-1} = M[N-1,N-1]  (rgf.jl:144)
+  {
+    std::vector<ZGemmProblem> pr;
+    std::vector<InvSpec> iv;
+    for (size_t k = 0; k < sys.size(); ++k) {
+      const auto& s = sys[k];
+      int i = s.npl() - 1;
+      if (i < 0) continue;
+      pr.push_back(gp(nullptr, 1, nullptr, 1, work[k].W, s.b[i], s.b[i], s.b[i], 0, ZERO, s.D[i], s.ldD[i],
+                      s.dscale, s.shift));
+      pr.back().diag_ptr = s.shift_ptr;
+      iv.push_back(inv_spec(s, work[k], i));
+    }
+    plan.gemm('N', 'N', pr);
+    plan.inv(iv);
+  }
+  for (int j = 1; j < maxN; ++j) {
+    // R_i = M[i,i+1] g_{i+1}  (rgf.jl:152-154) and L_{i+1} = g_{i+1} M[i+1,i]  (rgf.jl:157)
+    std::vector<ZGemmProblem> rN, lN, lC;
+    for (size_t k = 0; k < sys.size(); ++k) {
+      const auto& s = sys[k];
+      int i = s.npl() - 1 - j;
+      if (i < 0) continue;
+      RgfWork& w = work[k];
+      rN.push_back(gp(s.U[i], s.ldU[i], w.g[i + 1], s.b[i + 1], w.R[i], s.b[i], s.b[i], s.b[i + 1], s.b[i + 1],
+                      s.uscale));
+      auto p = gp(w.g[i + 1], s.b[i + 1], s.Lw[i], s.ldL[i], w.L[i], s.b[i + 1], s.b[i + 1], s.b[i], s.b[i + 1],
+                  s.lscale);
+      (s.lop == 'N' ? lN : lC).push_back(p);
+    }
+    std::vector<ZGemmProblem> nn = rN;
+    nn.insert(nn.end(), lN.begin(), lN.end());
+    plan.gemm('N', 'N', nn);
+    plan.gemm('N', 'C', lC);
+    // X_i = M[i,i] - M[i,i+1] L_{i+1}  (rgf.jl:159-160), then its inverse (rgf.jl:161)
+    std::vector<ZGemmProblem> xp;
+    std::vector<InvSpec> iv;
+    for (size_t k = 0; k < sys.size(); ++k) {
+      const auto& s = sys[k];
+      int i = s.npl() - 1 - j;
+      if (i < 0) continue;
+      RgfWork& w = work[k];
+      xp.push_back(gp(s.U[i], s.ldU[i], w.L[i], s.b[i + 1], w.W, s.b[i], s.b[i], s.b[i], s.b[i + 1],
+                      cscale(s.uscale, -1.0), s.D[i], s.ldD[i], s.dscale, s.shift));
+      xp.back().diag_ptr = s.shift_ptr;
+      iv.push_back(inv_spec(s, w, i));
+    }
+    plan.gemm('N', 'N', xp);
+    plan.inv(iv);
+  }
+}
+
+void build_rgf_downward(Plan& plan, const std::vector<TriSystem>& sys, std::vector<RgfWork>& work,
+                        std::vector<TriOut>& out) {
+  int maxN = 0;
+  for (const auto& s : sys) maxN = std::max(maxN, s.npl());
+  // G_11 = X_1^{-1}  (rgf.jl:169)
+  {
+    std::vector<ZBlockOp> ops;
+    for (size_t k = 0; k < sys.size(); ++k) {
+      const auto& s = sys[k];
+      if (s.npl() == 0) continue;
+      ZBlockOp o{};
+      o.A = work[k].g[0]; o.lda = s.b[0]; o.C = out[k].d[0]; o.ldc = out[k].ldd[0];
+      o.m = o.n = s.b[0]; o.kind = ZOP_COPY;
+      ops.push_back(o);
+    }
+    plan.blockops(ops);
+  }
+  for (int i = 1; i < maxN; ++i) {
+    // G[i-1,i] = -G[i-1,i-1] R_{i-1};  G[i,i-1] = -L_i G[i-1,i-1]  (rgf.jl:174,177)
+    std::vector<ZGemmProblem> pr;
+    for (size_t k = 0; k < sys.size(); ++k) {
+      const auto& s = sys[k];
+      if (i >= s.npl()) continue;
+      RgfWork& w = work[k];
+      TriOut& o = out[k];
+      pr.push_back(gp(o.d[i - 1], o.ldd[i - 1], w.R[i - 1], s.b[i - 1], o.u[i - 1], o.ldu[i - 1], s.b[i - 1], s.b[i],
+                      s.b[i - 1], MONE));
+      pr.push_back(gp(w.L[i - 1], s.b[i], o.d[i - 1], o.ldd[i - 1], o.l[i - 1], o.ldl[i - 1], s.b[i], s.b[i - 1],
+                      s.b[i - 1], MONE));
+    }
+    plan.gemm('N', 'N', pr);
+    // G[i,i] = X_i^{-1} - L_i G[i-1,i]  (rgf.jl:180-181)
+    std::vector<ZGemmProblem> dp;
+    for (size_t k = 0; k < sys.size(); ++k) {
+      const auto& s = sys[k];
+      if (i >= s.npl()) continue;
+      RgfWork& w = work[k];
+      TriOut& o = out[k];
+      dp.push_back(gp(w.L[i - 1], s.b[i], o.u[i - 1], o.ldu[i - 1], o.d[i], o.ldd[i], s.b[i], s.b[i], s.b[i - 1],
+                      MONE, w.g[i], s.b[i], ONE));
+    }
+    plan.gemm('N', 'N', dp);
+  }
+}
+
+void build_rgf_full_inverse(Plan& plan, const std::vector<TriSystem>& sys, std::vector<RgfWork>& work,
+                            std::vector<std::vector<cplx*>>& full) {
+  // G[i,j] = -G[i,j-1] R_{j-1};  G[j,i] = -L_j G[j-1,i]  for j >= i+2  (rgf.jl:185-199)
+  int maxN = 0;
+  for (const auto& s : sys) maxN = std::max(maxN, s.npl());
+  for (int d = 2; d < maxN; ++d) {
+    std::vector<ZGemmProblem> pr;
+    for (size_t k = 0; k < sys.size(); ++k) {
+      const auto& s = sys[k];
+      int n = s.npl();
+      auto& F = full[k];
+      RgfWork& w = work[k];
+      for (int i = 0; i + d < n; ++i) {
+        int j = i + d;
+        if (F[i * n + j] && F[i * n + j - 1])
+          pr.push_back(gp(F[i * n + j - 1], s.b[i], w.R[j - 1], s.b[j - 1], F[i * n + j], s.b[i], s.b[i], s.b[j],
+                          s.b[j - 1], MONE));
+        if (F[j * n + i] && F[(j - 1) * n + i])
+          pr.push_back(gp(w.L[j - 1], s.b[j], F[(j - 1) * n + i], s.b[j - 1], F[j * n + i], s.b[j], s.b[j], s.b[i],
+                          s.b[j - 1], MONE));
+      }
+    }
+    plan.gemm('N', 'N', pr);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// RKD (recursive Keldysh), src/keldyshndiag.jl:221-317, with every
+// be_mldivide!('N', ., ., LU(X_i)) applied as a product with g_i = X_i^{-1}.
+
+void build_rkd(Plan& plan, const std::vector<TriSystem>& sys, std::vector<RgfWork>& work,
+               std::vector<HermBlocks>& S) {
+  int maxN = 0;
+  for (const auto& s : sys) maxN = std::max(maxN, s.npl());
+  // workspace: xb diagonal chain (npl blocks), m2/t temporaries (npl blocks each)
+  std::vector<std::vector<cplx*>> xb(sys.size()), t1(sys.size()), t2(sys.size());
+  for (size_t k = 0; k < sys.size(); ++k) {
+    const auto& s = sys[k];
+    int n = s.npl();
+    size_t tot = 0;
+    for (int i = 0; i < n; ++i) tot += 3 * (size_t)s.maxb() * s.maxb();
+    cplx* a = plan.alloc_c(tot);
+    size_t o = 0;
+    size_t bb = (size_t)s.maxb() * s.maxb();
+    for (int i = 0; i < n; ++i) {
+      xb[k].push_back(a + o); o += bb;
+      t1[k].push_back(a + o); o += bb;
+      t2[k].push_back(a + o); o += bb;
+    }
+  }
+  // upward RKD pass (keldyshndiag.jl:230-234), ix = N-2 .. 0
+  for (int j = 1; j < maxN; ++j) {
+    std::vector<ZGemmProblem> p1, p2, p3;
+    for (size_t k = 0; k < sys.size(); ++k) {
+      const auto& s = sys[k];
+      int i = s.npl() - 1 - j;
+      if (i < 0) continue;
+      RgfWork& w = work[k];
+      HermBlocks& h = S[k];
+      // S[i,i] -= R_i S[i,i+1]^H
+      p1.push_back(gp(w.R[i], s.b[i], h.u[i], h.ldu[i], h.d[i], h.ldd[i], s.b[i], s.b[i], s.b[i + 1], MONE, h.d[i],
+                      h.ldd[i], ONE));
+      // S[i,i+1] -= R_i S[i+1,i+1]
+      p2.push_back(gp(w.R[i], s.b[i], h.d[i + 1], h.ldd[i + 1], h.u[i], h.ldu[i], s.b[i], s.b[i + 1], s.b[i + 1],
+                      MONE, h.u[i], h.ldu[i], ONE));
+      // S[i,i] -= S[i,i+1] R_i^H
+      p3.push_back(gp(h.u[i], h.ldu[i], w.R[i], s.b[i], h.d[i], h.ldd[i], s.b[i], s.b[i], s.b[i + 1], MONE, h.d[i],
+                      h.ldd[i], ONE));
+    }
+    plan.gemm('N', 'C', p1);
+    plan.gemm('N', 'N', p2);
+    plan.gemm('N', 'C', p3);
+  }
+  // central pass, phase A: the X chain (keldyshndiag.jl:270-283)
+  //   xb[0] = I;  xb[i] = I + M[i,i-1] g_{i-1} xb[i-1] R_{i-1}
+  {
+    std::vector<ZBlockOp> ops;
+    for (size_t k = 0; k < sys.size(); ++k) {
+      const auto& s = sys[k];
+      if (s.npl() < 2) continue;
+      ZBlockOp o{};
+      o.C = xb[k][0]; o.ldc = s.b[0]; o.m = o.n = s.b[0]; o.kind = ZOP_IDENTITY; o.alpha = ONE;
+      ops.push_back(o);
+    }
+    plan.blockops(ops);
+  }
+  for (int i = 1; i + 1 < maxN; ++i) {
+    std::vector<ZGemmProblem> a1, a2, a3N, a3C;
+    for (size_t k = 0; k < sys.size(); ++k) {
+      const auto& s = sys[k];
+      if (i + 1 >= s.npl()) continue;
+      RgfWork& w = work[k];
+      // m2[i-1,i] = xb[i-1] R_{i-1}  (:273)
+      a1.push_back(gp(xb[k][i - 1], s.b[i - 1], w.R[i - 1], s.b[i - 1], t1[k][i], s.b[i - 1], s.b[i - 1], s.b[i],
+                      s.b[i - 1], ONE));
+      // xbo[i-1,i] = g_{i-1} m2[i-1,i]  (:274)
+      a2.push_back(gp(w.g[i - 1], s.b[i - 1], t1[k][i], s.b[i - 1], t2[k][i], s.b[i - 1], s.b[i - 1], s.b[i],
+                      s.b[i - 1], ONE));
+      // xb[i] = M[i,i-1] xbo[i-1,i] + I  (:275, :280-283)
+      auto p = gp(s.Lw[i - 1], s.ldL[i - 1], t2[k][i], s.b[i - 1], xb[k][i], s.b[i], s.b[i], s.b[i], s.b[i - 1],
+                  s.lscale, nullptr, 1, ZERO, ONE);
+      (s.lop == 'N' ? a3N : a3C).push_back(p);
+    }
+    plan.gemm('N', 'N', a1);
+    plan.gemm('N', 'N', a2);
+    plan.gemm('N', 'N', a3N);
+    plan.gemm('C', 'N', a3C);
+  }
+  // central pass, phase B (all layers at once), keldyshndiag.jl:257-260 and :285-291:
+  //   m2[i,i] = g_i xb[i];  m2[i,i+1] = m2[i,i] S[i,i+1];  S[i,i+1] = m2[i,i+1] g_{i+1}^H
+  {
+    std::vector<ZGemmProblem> b1, b2, b3;
+    for (size_t k = 0; k < sys.size(); ++k) {
+      const auto& s = sys[k];
+      RgfWork& w = work[k];
+      HermBlocks& h = S[k];
+      for (int i = 0; i + 1 < s.npl(); ++i) {
+        b1.push_back(gp(w.g[i], s.b[i], xb[k][i], s.b[i], t1[k][i], s.b[i], s.b[i], s.b[i], s.b[i], ONE));
+        b2.push_back(gp(t1[k][i], s.b[i], h.u[i], h.ldu[i], t2[k][i], s.b[i], s.b[i], s.b[i + 1], s.b[i], ONE));
+        b3.push_back(gp(t2[k][i], s.b[i], w.g[i + 1], s.b[i + 1], h.u[i], h.ldu[i], s.b[i], s.b[i + 1], s.b[i + 1],
+                        ONE));
+      }
+    }
+    plan.gemm('N', 'N', b1);
+    plan.gemm('N', 'N', b2);
+    plan.gemm('N', 'C', b3);
+  }
+  // diagonal rescale (keldyshndiag.jl:296-301): S[i,i] = g_i S[i,i] g_i^H
+  {
+    std::vector<ZGemmProblem> c1, c2;
+    for (size_t k = 0; k < sys.size(); ++k) {
+      const auto& s = sys[k];
+      RgfWork& w = work[k];
+      HermBlocks& h = S[k];
+      for (int i = 0; i < s.npl(); ++i) {
+        c1.push_back(gp(w.g[i], s.b[i], h.d[i], h.ldd[i], t1[k][i], s.b[i], s.b[i], s.b[i], s.b[i], ONE));
+        c2.push_back(gp(t1[k][i], s.b[i], w.g[i], s.b[i], h.d[i], h.ldd[i], s.b[i], s.b[i], s.b[i], ONE));
+      }
+    }
+    plan.gemm('N', 'N', c1);
+    plan.gemm('N', 'C', c2);
+  }
+  // downward RKD pass (keldyshndiag.jl:313-317), ix = 0 .. N-2
+  for (int i = 0; i + 1 < maxN; ++i) {
+    std::vector<ZGemmProblem> d1, d2, d3;
+    for (size_t k = 0; k < sys.size(); ++k) {
+      const auto& s = sys[k];
+      if (i + 1 >= s.npl()) continue;
+      RgfWork& w = work[k];
+      HermBlocks& h = S[k];
+      // S[i+1,i+1] -= S[i,i+1]^H L_{i+1}^H
+      d1.push_back(gp(h.u[i], h.ldu[i], w.L[i], s.b[i + 1], h.d[i + 1], h.ldd[i + 1], s.b[i + 1], s.b[i + 1], s.b[i],
+                      MONE, h.d[i + 1], h.ldd[i + 1], ONE));
+      // S[i,i+1] -= S[i,i] L_{i+1}^H
+      d2.push_back(gp(h.d[i], h.ldd[i], w.L[i], s.b[i + 1], h.u[i], h.ldu[i], s.b[i], s.b[i + 1], s.b[i], MONE,
+                      h.u[i], h.ldu[i], ONE));
+    }
+    plan.gemm('C', 'C', d1);
+    plan.gemm('N', 'C', d2);
+    std::vector<ZGemmProblem> d3v;
+    for (size_t k = 0; k < sys.size(); ++k) {
+      const auto& s = sys[k];
+      if (i + 1 >= s.npl()) continue;
+      RgfWork& w = work[k];
+      HermBlocks& h = S[k];
+      // S[i+1,i+1] -= L_{i+1} S[i,i+1]
+      d3v.push_back(gp(w.L[i], s.b[i + 1], h.u[i], h.ldu[i], h.d[i + 1], h.ldd[i + 1], s.b[i + 1], s.b[i + 1], s.b[i],
+                       MONE, h.d[i + 1], h.ldd[i + 1], ONE));
+    }
+    plan.gemm('N', 'N', d3v);
+  }
+}
+
+}  // namespace negf

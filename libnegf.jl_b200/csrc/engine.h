@@ -1,0 +1,203 @@
+// Host-side sweep planner of the B200 NEGF library.
+//
+// A sweep (RGF, RKD, general RGF, selected inverse, DDRGF, the batched-energy
+// NEGF solve) is compiled once into a Plan: an ordered list of batched kernel
+// launches whose problem descriptors live in one device buffer.  Every launch
+// covers all independent systems (energies, devices, DDRGF domains) of one
+// step of the recursion, so the serial dependency of the reference's loops is
+// kept while each step fills the GPU.  A Plan is replayed with run(); with
+// use_graph it is captured once into a CUDA graph and relaunched from there.
+#pragma once
+
+#include <string>
+#include <vector>
+#include <cstddef>
+
+#include "negf_common.cuh"
+
+namespace negf {
+
+// launchers (zgemm.cu, zinv.cu, zelem.cu)
+cudaError_t launch_zgemm_batched(char opA, char opB, const ZGemmProblem* probs_dev, const int* tile_start_dev,
+                                 int nprob, int total_tiles, cudaStream_t stream);
+int zgemm_tiles(int m, int n);
+size_t zgemm_smem_bytes();
+cudaError_t zgemm_prepare(char opA, char opB);
+size_t zgj_panel_smem_bytes(int n, int nb);
+cudaError_t launch_zgj_panel(const ZInvProblem* probs_dev, int nprob, int k0, int nb, int blocked, size_t smem,
+                             cudaStream_t stream);
+cudaError_t launch_zgj_unpermute(const ZInvProblem* probs_dev, int nprob, int max_n, cudaStream_t stream);
+cudaError_t launch_zblockops(const ZBlockOp* ops_dev, int nops, int max_m, int max_n, cudaStream_t stream);
+cudaError_t launch_ztrace_prod(const void* probs_dev, int nprob, cudaStream_t stream);
+size_t zgetrf_panel_smem_bytes(int n, int nb);
+size_t ztrtri_smem_bytes(int nb);
+cudaError_t zlu_prepare(size_t panel_smem, size_t tri_smem);
+cudaError_t launch_zgetrf_panel(const void* probs, int nprob, int k0, int nb, size_t smem, cudaStream_t st);
+cudaError_t launch_zlaswp_copy(const void* probs, int nprob, int k0, int nb, int max_n, cudaStream_t st);
+cudaError_t launch_ztrtri_diag(const void* probs, int nprob, int nb, int upper, int max_n, size_t smem,
+                               cudaStream_t st);
+
+// LU request (LAPACK getrf semantics, in place).  ipiv receives 0-based
+// global pivot rows; ipiv_lapack (optional, device int32) 1-based ones.
+struct LuSpec {
+  cplx* A;
+  int n, ld;
+  int* ipiv;
+  cplx* Linv;  // scratch nb x nb
+  cplx* T;     // scratch nb x n
+  int* info;
+};
+// Triangular inverse request: X = inverse of the upper (non-unit) or unit
+// lower triangle of the packed factors A; T is scratch n x nb.
+struct TriSpec {
+  const cplx* A;
+  int n, lda;
+  cplx* X;
+  int ldx;
+  cplx* T;
+};
+constexpr int kTriNb = 32;
+int lu_panel_width(int max_n);
+
+struct ZTraceProblemHost {
+  const cplx* X;
+  const cplx* Y;
+  int n, ldx, ldy, pad_;
+  double* out;
+};
+
+// Largest block size the Gauss-Jordan inversion supports (panel in shared memory).
+constexpr int kMaxBlock = 1024;
+
+// Panel width used for an inversion batch whose largest block is max_n
+// (max_n itself when the whole block fits in shared memory).
+int gj_panel_width(int max_n);
+
+// Inversion request: W (n x n, ld) holds X and is destroyed; out receives X^{-1}.
+struct InvSpec {
+  cplx* W;
+  int n, ld;
+  cplx* out;
+  int ldo;
+  cplx* F;        // scratch n x nb
+  cplx* Bbuf;     // scratch nb x n
+  uint8_t* used;  // scratch n
+  int* piv;       // scratch n
+  int* info;
+};
+
+struct Step {
+  enum Kind {
+    GEMM = 0, GJ_PANEL = 1, GJ_UNPERMUTE = 2, BLOCKOP = 3, TRACE = 4, LU_PANEL = 5, LU_SWAP = 6, TRI_DIAG = 7
+  } kind;
+  char opA = 'N', opB = 'N';
+  size_t off = 0;        // descriptor offset in the blob
+  size_t tiles_off = 0;  // tile prefix-sum offset (GEMM)
+  int count = 0, total_tiles = 0, max_m = 0, max_n = 0;
+  int k0 = 0, nb = 0, blocked = 0;
+  size_t smem = 0;
+  double flops = 0.0;    // real flops of the step (8mnk per complex GEMM)
+};
+
+class Plan {
+ public:
+  Plan() = default;
+  ~Plan();
+  Plan(const Plan&) = delete;
+  Plan& operator=(const Plan&) = delete;
+
+  // device memory owned by the plan (workspace); zero-initialised
+  void* alloc(size_t bytes);
+  cplx* alloc_c(size_t n) { return static_cast<cplx*>(alloc(n * sizeof(cplx))); }
+
+  void gemm(char opA, char opB, const std::vector<ZGemmProblem>& probs);
+  void inv(const std::vector<InvSpec>& specs);
+  void blockops(const std::vector<ZBlockOp>& ops);
+  void trace(const std::vector<ZTraceProblemHost>& probs);
+  void getrf(const std::vector<LuSpec>& specs);
+  void trtri(const std::vector<TriSpec>& specs, bool upper);
+
+  cudaError_t finalize();
+  cudaError_t run(cudaStream_t stream, bool use_graph);
+
+  double flops() const;
+  size_t num_launches() const;
+  size_t workspace_bytes() const { return owned_bytes_; }
+  std::vector<Step> steps;
+
+ private:
+  size_t push_bytes(const void* p, size_t n);
+  std::vector<unsigned char> blob_;
+  void* dblob_ = nullptr;
+  std::vector<void*> owned_;
+  size_t owned_bytes_ = 0;
+  bool finalized_ = false;
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t gexec_ = nullptr;
+  cudaStream_t graph_stream_ = nullptr;
+};
+
+// ---------------------------------------------------------------------------
+// Block-tridiagonal systems and the sweeps over them.
+
+// View of one block-tridiagonal matrix M through its operand blocks:
+//   M[i,i]   = dscale * D[i] + shift * I
+//   M[i,i+1] = uscale * U[i]
+//   M[i+1,i] = lscale * op(Lw[i]),  op = identity (lop 'N') or conjugate
+//              transpose (lop 'C', Lw[i] then has the (i,i+1) shape).
+// The NEGF device path uses D = H_ii (+Sigma), U = Lw = H_{i,i+1}, dscale =
+// uscale = lscale = -1, shift = E + i*eta, lop = 'C'; the reference API path
+// uses the M blocks themselves with unit scales.
+struct TriSystem {
+  std::vector<int> b;
+  std::vector<const cplx*> D, U, Lw;
+  std::vector<int> ldD, ldU, ldL;
+  cplx dscale{1.0, 0.0}, shift{0.0, 0.0}, uscale{1.0, 0.0}, lscale{1.0, 0.0};
+  const cplx* shift_ptr = nullptr;  // when set, the shift is read from device memory
+  char lop = 'N';
+  int* info = nullptr;  // device int, set on a zero pivot
+  int npl() const { return static_cast<int>(b.size()); }
+  int maxb() const;
+};
+
+// Workspace of the RGF upward pass of one system.
+struct RgfWork {
+  std::vector<cplx*> g;   // g[i] = X_i^{-1}          (b_i x b_i)
+  std::vector<cplx*> R;   // R[i] = M[i,i+1] g[i+1]   (b_i x b_{i+1})
+  std::vector<cplx*> L;   // L[i] = g[i+1] M[i+1,i]   (b_{i+1} x b_i), index i for L_{i+1}
+  cplx* W = nullptr;      // inversion workspace (maxb^2)
+  cplx* F = nullptr;
+  cplx* Bbuf = nullptr;
+  uint8_t* used = nullptr;
+  int* piv = nullptr;
+};
+
+// Output block pointers of a tridiagonal result (null entries: not wanted).
+struct TriOut {
+  std::vector<cplx*> d, u, l;   // d[i] (i,i); u[i] (i,i+1); l[i] (i+1,i)
+  std::vector<int> ldd, ldu, ldl;
+};
+
+void alloc_rgf_work(Plan& plan, const TriSystem& s, RgfWork& w);
+// Upward pass (src/matinvertndiag_rgf.jl:143-162), all systems batched per layer.
+void build_rgf_upward(Plan& plan, const std::vector<TriSystem>& sys, std::vector<RgfWork>& work);
+// Downward pass (src/matinvertndiag_rgf.jl:166-182) writing the tridiagonal of
+// M^{-1}; with full_rows/full_cols the whole inverse (rgf.jl:185-199) is
+// written into full[s][i*npl+j] (null = skip).
+void build_rgf_downward(Plan& plan, const std::vector<TriSystem>& sys, std::vector<RgfWork>& work,
+                        std::vector<TriOut>& out);
+void build_rgf_full_inverse(Plan& plan, const std::vector<TriSystem>& sys, std::vector<RgfWork>& work,
+                            std::vector<std::vector<cplx*>>& full);
+// RKD passes (src/keldyshndiag.jl:221-317).  S holds the Hermitian middle
+// operator (diagonal + upper blocks) on entry and G^n on exit.
+struct HermBlocks {
+  std::vector<cplx*> d, u;
+  std::vector<int> ldd, ldu;
+};
+void build_rkd(Plan& plan, const std::vector<TriSystem>& sys, std::vector<RgfWork>& work,
+               std::vector<HermBlocks>& S);
+
+std::string& last_error();
+void set_error(const std::string& msg);
+
+}  // namespace negf

@@ -1,0 +1,759 @@
+// extern "C" entry points of libnegf_b200.so (declared in include/negf_b200.h).
+#include "../../include/negf_b200.h"
+#include "engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+using namespace negf;
+
+namespace {
+
+int fail(int code, const std::string& msg) {
+  set_error(msg);
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where) {
+  return fail(NEGF_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define NEGF_TRY_CUDA(expr, where)                  \
+  do {                                              \
+    cudaError_t e__ = (expr);                       \
+    if (e__ != cudaSuccess) return cuda_fail(e__, where); \
+  } while (0)
+
+int check_device() {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0)
+    return fail(NEGF_ERR_CUDA, std::string("no usable CUDA device: ") + cudaGetErrorString(e));
+  return NEGF_SUCCESS;
+}
+
+inline cplx c2(const double* v) { return make_double2(v[0], v[1]); }
+
+// Run a finished plan once, synchronously, and read the per-system info codes.
+int run_plan_sync(Plan& plan, cudaStream_t st, int* dinfo, int nsys, const char* what) {
+  cudaError_t e = plan.run(st, false);
+  if (e != cudaSuccess) return cuda_fail(e, what);
+  e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, what);
+  if (dinfo) {
+    std::vector<int> info(nsys);
+    e = cudaMemcpy(info.data(), dinfo, sizeof(int) * nsys, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    for (int s = 0; s < nsys; ++s)
+      if (info[s] != 0) {
+        char buf[160];
+        std::snprintf(buf, sizeof buf, "%s: zero pivot in system %d (column %d of a diagonal block)", what, s,
+                      info[s]);
+        return fail(NEGF_ERR_SINGULAR, buf);
+      }
+  }
+  return NEGF_SUCCESS;
+}
+
+// Build the TriSystem list of the reference-API sweeps from pointer tables.
+int make_systems(int nsys, int npl, const int32_t* bs, void* const* Md, void* const* Mu, void* const* Ml,
+                 int* dinfo, std::vector<TriSystem>& sys) {
+  if (nsys <= 0 || npl <= 0 || !bs || !Md) return fail(NEGF_ERR_INVALID, "nsys, npl, block_sizes and Md are required");
+  if (npl > 1 && (!Mu || !Ml)) return fail(NEGF_ERR_INVALID, "Mu and Ml are required when npl > 1");
+  sys.resize(nsys);
+  for (int s = 0; s < nsys; ++s) {
+    TriSystem& t = sys[s];
+    t.b.assign(bs + (size_t)s * npl, bs + (size_t)(s + 1) * npl);
+    for (int x : t.b)
+      if (x <= 0 || x > kMaxBlock) return fail(NEGF_ERR_INVALID, "block sizes must be in [1, 1024]");
+    for (int i = 0; i < npl; ++i) {
+      t.D.push_back(static_cast<const cplx*>(Md[(size_t)s * npl + i]));
+      t.ldD.push_back(t.b[i]);
+      if (!t.D.back()) return fail(NEGF_ERR_INVALID, "NULL diagonal block");
+    }
+    for (int i = 0; i + 1 < npl; ++i) {
+      t.U.push_back(static_cast<const cplx*>(Mu[(size_t)s * (npl - 1) + i]));
+      t.ldU.push_back(t.b[i]);
+      t.Lw.push_back(static_cast<const cplx*>(Ml[(size_t)s * (npl - 1) + i]));
+      t.ldL.push_back(t.b[i + 1]);
+      if (!t.U.back() || !t.Lw.back()) return fail(NEGF_ERR_INVALID, "NULL off-diagonal block");
+    }
+    t.info = dinfo + s;
+  }
+  return NEGF_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 peak probe kernels (throughput loops, no memory traffic)
+__global__ void probe_dmma(double* out, int iters) {
+  double a0 = threadIdx.x * 1e-3, a1 = 1.0 + a0, b0 = 0.5 + a0;
+  double c[4] = {0, 0, 0, 0}, d[4] = {0, 0, 0, 0};
+  for (int i = 0; i < iters; ++i) {
+    asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
+                 : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3]) : "d"(a0), "d"(a1), "d"(b0));
+    asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
+                 : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3]) : "d"(a1), "d"(a0), "d"(b0));
+  }
+  out[blockIdx.x * blockDim.x + threadIdx.x] = c[0] + c[1] + c[2] + c[3] + d[0] + d[1] + d[2] + d[3];
+}
+
+__global__ void probe_dfma(double* out, int iters) {
+  double x[8];
+  for (int j = 0; j < 8; ++j) x[j] = threadIdx.x * 1e-3 + j;
+  double y = 0.999999, z = 1e-9;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x[j] = fma(x[j], y, z);
+  }
+  double s = 0;
+  for (int j = 0; j < 8; ++j) s += x[j];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Device object and resident solver of the batched-energy NEGF path.
+
+struct negf_device_s {
+  int npl = 0;
+  std::vector<int> b;
+  std::vector<cplx*> D;   // H_ii (+ Sigma_L on layer 0, + Sigma_R on layer N-1)
+  std::vector<cplx*> Hu;  // H_{i,i+1}
+  cplx* gamL = nullptr;
+  cplx* gamR = nullptr;
+  std::vector<void*> owned;
+  ~negf_device_s() {
+    for (void* p : owned) cudaFree(p);
+  }
+};
+
+struct negf_solver_s {
+  negf_device_s* dev = nullptr;
+  int nE = 0;
+  negf_solve_opts opts{};
+  std::unique_ptr<Plan> plan;
+  cplx* params = nullptr;  // [shift (nE) | f_L (nE) | f_R (nE) | i (1)]
+  cplx* gr = nullptr;      // nE * sum b_i^2
+  cplx* gl = nullptr;
+  double* t2 = nullptr;    // 2 * nE (re, im)
+  int* info = nullptr;
+  size_t per_energy = 0;   // sum b_i^2
+};
+
+namespace {
+
+size_t solver_bytes_per_energy(const negf_device_s& d, const negf_solve_opts& o) {
+  size_t n = d.npl, mb = 0, sb2 = 0, sbb = 0;
+  for (int x : d.b) { mb = std::max<size_t>(mb, x); sb2 += (size_t)x * x; }
+  for (size_t i = 0; i + 1 < n; ++i) sbb += (size_t)d.b[i] * d.b[i + 1];
+  size_t nb = gj_panel_width((int)mb);
+  size_t c = sb2 + 2 * sbb + mb * mb + 2 * mb * nb;  // RGF work
+  if (o.want_gr) c += sb2 + 4 * mb * mb;              // G^R diagonal + rings
+  if (o.want_gl) c += sb2 + sbb + 3 * n * mb * mb;    // G^n storage + RKD scratch
+  if (o.want_t) c += 4 * mb * mb;
+  return c * sizeof(cplx) + 64;
+}
+
+int build_solver(negf_solver_s& S) {
+  negf_device_s& d = *S.dev;
+  const int n = d.npl;
+  const int nE = S.nE;
+  Plan& plan = *S.plan;
+  S.per_energy = 0;
+  for (int x : d.b) S.per_energy += (size_t)x * x;
+  S.params = plan.alloc_c(3 * (size_t)nE + 1);
+  S.info = static_cast<int*>(plan.alloc(sizeof(int) * nE));
+  if (S.opts.want_gr) S.gr = plan.alloc_c(S.per_energy * nE);
+  if (S.opts.want_gl) S.gl = plan.alloc_c(S.per_energy * nE);
+  if (S.opts.want_t) S.t2 = static_cast<double*>(plan.alloc(sizeof(double) * 2 * nE));
+  const cplx i_unit = make_double2(0.0, 1.0);
+  NEGF_TRY_CUDA(cudaMemcpy(S.params + 3 * nE, &i_unit, sizeof(cplx), cudaMemcpyHostToDevice), "solver params");
+
+  std::vector<TriSystem> sys(nE);
+  std::vector<RgfWork> work(nE);
+  for (int e = 0; e < nE; ++e) {
+    TriSystem& t = sys[e];
+    t.b = d.b;
+    for (int i = 0; i < n; ++i) { t.D.push_back(d.D[i]); t.ldD.push_back(d.b[i]); }
+    for (int i = 0; i + 1 < n; ++i) {
+      t.U.push_back(d.Hu[i]); t.ldU.push_back(d.b[i]);
+      t.Lw.push_back(d.Hu[i]); t.ldL.push_back(d.b[i]);
+    }
+    t.dscale = make_double2(-1.0, 0.0);
+    t.uscale = make_double2(-1.0, 0.0);
+    t.lscale = make_double2(-1.0, 0.0);
+    t.lop = 'C';
+    t.shift_ptr = S.params + e;
+    t.info = S.info + e;
+    alloc_rgf_work(plan, t, work[e]);
+  }
+  // block pointers inside the output arrays
+  auto out_blocks = [&](cplx* base, int e) {
+    std::vector<cplx*> v;
+    size_t o = (size_t)e * S.per_energy;
+    for (int i = 0; i < n; ++i) { v.push_back(base + o); o += (size_t)d.b[i] * d.b[i]; }
+    return v;
+  };
+  std::vector<HermBlocks> herm(nE);
+  if (S.opts.want_gl) {
+    // Sigma^in = f_L Gamma_L (+) f_R Gamma_R in Hermitian storage
+    std::vector<ZBlockOp> zero, setL, addR;
+    for (int e = 0; e < nE; ++e) {
+      HermBlocks& h = herm[e];
+      h.d = out_blocks(S.gl, e);
+      for (int i = 0; i < n; ++i) h.ldd.push_back(d.b[i]);
+      for (int i = 0; i + 1 < n; ++i) {
+        h.u.push_back(plan.alloc_c((size_t)d.b[i] * d.b[i + 1]));
+        h.ldu.push_back(d.b[i]);
+      }
+      for (int i = 0; i < n; ++i) {
+        ZBlockOp z{}; z.C = h.d[i]; z.ldc = d.b[i]; z.m = z.n = d.b[i]; z.kind = ZOP_FILL;
+        zero.push_back(z);
+      }
+      ZBlockOp l{}; l.A = d.gamL; l.lda = d.b[0]; l.C = h.d[0]; l.ldc = d.b[0]; l.m = l.n = d.b[0];
+      l.kind = ZOP_AXPBY; l.alpha_ptr = S.params + nE + e; l.beta = make_double2(1.0, 0.0);
+      setL.push_back(l);
+      ZBlockOp r{}; r.A = d.gamR; r.lda = d.b[n - 1]; r.C = h.d[n - 1]; r.ldc = d.b[n - 1];
+      r.m = r.n = d.b[n - 1]; r.kind = ZOP_AXPBY; r.alpha_ptr = S.params + 2 * nE + e; r.beta = make_double2(1.0, 0.0);
+      addR.push_back(r);
+    }
+    plan.blockops(zero);
+    plan.blockops(setL);
+    plan.blockops(addR);
+  }
+  build_rgf_upward(plan, sys, work);
+  if (S.opts.want_gr) {
+    std::vector<TriOut> out(nE);
+    for (int e = 0; e < nE; ++e) {
+      TriOut& o = out[e];
+      o.d = out_blocks(S.gr, e);
+      for (int i = 0; i < n; ++i) o.ldd.push_back(d.b[i]);
+      int mb = sys[e].maxb();
+      cplx* ring = plan.alloc_c(4 * (size_t)mb * mb);
+      for (int i = 0; i + 1 < n; ++i) {
+        o.u.push_back(ring + (size_t)(i % 2) * mb * mb);
+        o.l.push_back(ring + (size_t)(2 + i % 2) * mb * mb);
+        o.ldu.push_back(d.b[i]);
+        o.ldl.push_back(d.b[i + 1]);
+      }
+    }
+    build_rgf_downward(plan, sys, work, out);
+  }
+  if (S.opts.want_gl) {
+    build_rkd(plan, sys, work, herm);
+    // G^< = i G^n
+    std::vector<ZBlockOp> sc;
+    for (int e = 0; e < nE; ++e)
+      for (int i = 0; i < n; ++i) {
+        ZBlockOp o{}; o.A = herm[e].d[i]; o.lda = d.b[i]; o.C = herm[e].d[i]; o.ldc = d.b[i];
+        o.m = o.n = d.b[i]; o.kind = ZOP_AXPBY; o.alpha_ptr = S.params + 3 * nE; o.beta = make_double2(0.0, 0.0);
+        sc.push_back(o);
+      }
+    plan.blockops(sc);
+  }
+  if (S.opts.want_t) {
+    // G^R_{1N} by G_{1,j} = -G_{1,j-1} R_{j-1}, G_{1,1} = g_1 (rgf.jl:169, :185-199)
+    const int b0 = d.b[0], bN = d.b[n - 1];
+    std::vector<std::vector<cplx*>> Y(nE);
+    std::vector<cplx*> P(nE), Q(nE);
+    int mb = 0;
+    for (int x : d.b) mb = std::max(mb, x);
+    for (int e = 0; e < nE; ++e) {
+      cplx* a = plan.alloc_c(4 * (size_t)mb * mb);
+      Y[e] = {a, a + (size_t)mb * mb};
+      P[e] = a + 2 * (size_t)mb * mb;
+      Q[e] = a + 3 * (size_t)mb * mb;
+    }
+    auto ycur = [&](int e, int j) -> const cplx* { return j == 0 ? work[e].g[0] : Y[e][j % 2]; };
+    for (int j = 1; j < n; ++j) {
+      std::vector<ZGemmProblem> pr;
+      for (int e = 0; e < nE; ++e) {
+        ZGemmProblem p{};
+        p.A = ycur(e, j - 1); p.lda = b0;
+        p.B = work[e].R[j - 1]; p.ldb = d.b[j - 1];
+        p.C = Y[e][j % 2]; p.ldc = b0; p.ldcin = 1;
+        p.m = b0; p.n = d.b[j]; p.k = d.b[j - 1];
+        p.alpha = make_double2(-1.0, 0.0);
+        pr.push_back(p);
+      }
+      plan.gemm('N', 'N', pr);
+    }
+    std::vector<ZGemmProblem> p1, p2;
+    std::vector<ZTraceProblemHost> tr;
+    for (int e = 0; e < nE; ++e) {
+      const cplx* G1N = ycur(e, n - 1);
+      ZGemmProblem a{};  // P = Gamma_L G1N  (b0 x bN)
+      a.A = d.gamL; a.lda = b0; a.B = G1N; a.ldb = b0; a.C = P[e]; a.ldc = b0; a.ldcin = 1;
+      a.m = b0; a.n = bN; a.k = b0; a.alpha = make_double2(1.0, 0.0);
+      p1.push_back(a);
+      ZGemmProblem c{};  // Q = Gamma_R G1N^H  (bN x b0)
+      c.A = d.gamR; c.lda = bN; c.B = G1N; c.ldb = b0; c.C = Q[e]; c.ldc = bN; c.ldcin = 1;
+      c.m = bN; c.n = b0; c.k = bN; c.alpha = make_double2(1.0, 0.0);
+      p2.push_back(c);
+      ZTraceProblemHost t{};
+      t.X = P[e]; t.ldx = b0; t.Y = Q[e]; t.ldy = bN; t.n = b0; t.out = S.t2 + 2 * e;
+      tr.push_back(t);
+      if (b0 != bN) return fail(NEGF_ERR_INVALID, "transmission needs equal first and last block sizes");
+    }
+    plan.gemm('N', 'N', p1);
+    plan.gemm('N', 'C', p2);
+    plan.trace(tr);
+  }
+  NEGF_TRY_CUDA(plan.finalize(), "solver finalize");
+  return NEGF_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* negf_last_error(void) { return last_error().c_str(); }
+
+int negf_version(void) { return 100; }
+
+int negf_zgemm_batched(char opA, char opB, int32_t nprob, const negf_zgemm_problem* probs, void* stream) {
+  if (int r = check_device()) return r;
+  if (nprob < 0 || (nprob > 0 && !probs)) return fail(NEGF_ERR_INVALID, "bad problem list");
+  auto okop = [](char c) { return c == 'N' || c == 'T' || c == 'C'; };
+  if (!okop(opA) || !okop(opB)) return fail(NEGF_ERR_INVALID, "op must be N, T or C");
+  try {
+    Plan plan;
+    std::vector<ZGemmProblem> v(nprob);
+    for (int i = 0; i < nprob; ++i) {
+      const negf_zgemm_problem& q = probs[i];
+      if (q.m < 0 || q.n < 0 || q.k < 0) return fail(NEGF_ERR_INVALID, "negative dimension");
+      ZGemmProblem& p = v[i];
+      p.A = static_cast<const cplx*>(q.A); p.B = static_cast<const cplx*>(q.B);
+      p.Cin = static_cast<const cplx*>(q.Cin); p.C = static_cast<cplx*>(q.C); p.diag_ptr = nullptr;
+      p.m = q.m; p.n = q.n; p.k = q.k;
+      p.lda = std::max(1, q.lda); p.ldb = std::max(1, q.ldb); p.ldc = std::max(1, q.ldc);
+      p.ldcin = std::max(1, q.ldcin); p.pad_ = 0;
+      p.alpha = c2(q.alpha); p.beta = c2(q.beta); p.diag = c2(q.diag);
+      if (p.m > 0 && p.n > 0 && !p.C) return fail(NEGF_ERR_INVALID, "NULL C");
+      if (p.k > 0 && (!p.A || !p.B)) return fail(NEGF_ERR_INVALID, "NULL A or B");
+    }
+    plan.gemm(opA, opB, v);
+    return run_plan_sync(plan, static_cast<cudaStream_t>(stream), nullptr, 0, "negf_zgemm_batched");
+  } catch (const std::bad_alloc&) {
+    return fail(NEGF_ERR_NOMEM, "device allocation failed");
+  }
+}
+
+int negf_zcopy_batched(char op, int32_t nprob, const int32_t* m, const int32_t* n, void* const* A,
+                       const int32_t* lda, void* const* C, const int32_t* ldc, void* stream) {
+  if (int r = check_device()) return r;
+  if (op != 'N' && op != 'C') return fail(NEGF_ERR_INVALID, "op must be N or C");
+  if (nprob < 0 || (nprob > 0 && (!m || !n || !A || !lda || !C || !ldc))) return fail(NEGF_ERR_INVALID, "bad arguments");
+  try {
+    Plan plan;
+    std::vector<ZBlockOp> ops;
+    for (int i = 0; i < nprob; ++i) {
+      if (m[i] <= 0 || n[i] <= 0) continue;
+      ZBlockOp o{};
+      o.A = static_cast<const cplx*>(A[i]); o.lda = std::max(1, lda[i]);
+      o.C = static_cast<cplx*>(C[i]); o.ldc = std::max(1, ldc[i]);
+      o.m = m[i]; o.n = n[i]; o.kind = op == 'N' ? ZOP_COPY : ZOP_CTRANSPOSE;
+      ops.push_back(o);
+    }
+    plan.blockops(ops);
+    return run_plan_sync(plan, static_cast<cudaStream_t>(stream), nullptr, 0, "negf_zcopy_batched");
+  } catch (const std::bad_alloc&) {
+    return fail(NEGF_ERR_NOMEM, "device allocation failed");
+  }
+}
+
+int negf_zinv_batched(int32_t nprob, const int32_t* n, void* const* A, const int32_t* lda, void* const* Ainv,
+                      const int32_t* ldainv, int32_t* info, void* stream) {
+  if (int r = check_device()) return r;
+  if (nprob < 0 || (nprob > 0 && (!n || !A || !lda || !Ainv || !ldainv))) return fail(NEGF_ERR_INVALID, "bad arguments");
+  try {
+    Plan plan;
+    int* dinfo = static_cast<int*>(plan.alloc(sizeof(int) * std::max(1, nprob)));
+    std::vector<ZBlockOp> copies;
+    std::vector<InvSpec> specs;
+    for (int i = 0; i < nprob; ++i) {
+      if (n[i] < 0 || n[i] > kMaxBlock) return fail(NEGF_ERR_INVALID, "n must be in [0, 1024]");
+      if (n[i] == 0) continue;
+      int mb = n[i], nb = gj_panel_width(mb);
+      InvSpec sp;
+      sp.W = plan.alloc_c((size_t)mb * mb);
+      sp.n = mb; sp.ld = mb; sp.out = static_cast<cplx*>(Ainv[i]); sp.ldo = ldainv[i];
+      sp.F = plan.alloc_c((size_t)mb * nb);
+      sp.Bbuf = plan.alloc_c((size_t)mb * nb);
+      sp.used = static_cast<uint8_t*>(plan.alloc(mb));
+      sp.piv = static_cast<int*>(plan.alloc(sizeof(int) * mb));
+      sp.info = dinfo + i;
+      specs.push_back(sp);
+      ZBlockOp o{}; o.A = static_cast<const cplx*>(A[i]); o.lda = lda[i]; o.C = sp.W; o.ldc = mb;
+      o.m = o.n = mb; o.kind = ZOP_COPY;
+      copies.push_back(o);
+    }
+    plan.blockops(copies);
+    plan.inv(specs);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = plan.run(st, false);
+    if (e != cudaSuccess) return cuda_fail(e, "negf_zinv_batched");
+    NEGF_TRY_CUDA(cudaStreamSynchronize(st), "negf_zinv_batched");
+    std::vector<int> h(std::max(1, nprob));
+    NEGF_TRY_CUDA(cudaMemcpy(h.data(), dinfo, sizeof(int) * std::max(1, nprob), cudaMemcpyDeviceToHost),
+                  "negf_zinv_batched");
+    int bad = -1;
+    for (int i = 0; i < nprob; ++i) {
+      if (info) info[i] = h[i];
+      if (h[i] && bad < 0) bad = i;
+    }
+    if (bad >= 0) {
+      char buf[128];
+      std::snprintf(buf, sizeof buf, "negf_zinv_batched: matrix %d is singular (zero pivot in column %d)", bad, h[bad]);
+      return fail(NEGF_ERR_SINGULAR, buf);
+    }
+    return NEGF_SUCCESS;
+  } catch (const std::bad_alloc&) {
+    return fail(NEGF_ERR_NOMEM, "device allocation failed");
+  }
+}
+
+int negf_rgf(int32_t nsys, int32_t npl, const int32_t* block_sizes, void* const* Md, void* const* Mu,
+             void* const* Ml, void* const* Gd, void* const* Gu, void* const* Gl, void* const* Gfull, void* stream) {
+  if (int r = check_device()) return r;
+  if (!Gd && !Gfull) return fail(NEGF_ERR_INVALID, "Gd or Gfull is required");
+  try {
+    Plan plan;
+    int* dinfo = static_cast<int*>(plan.alloc(sizeof(int) * nsys));
+    std::vector<TriSystem> sys;
+    if (int r = make_systems(nsys, npl, block_sizes, Md, Mu, Ml, dinfo, sys)) return r;
+    std::vector<RgfWork> work(nsys);
+    for (int s = 0; s < nsys; ++s) alloc_rgf_work(plan, sys[s], work[s]);
+    build_rgf_upward(plan, sys, work);
+    std::vector<TriOut> out(nsys);
+    std::vector<std::vector<cplx*>> full(nsys);
+    for (int s = 0; s < nsys; ++s) {
+      const TriSystem& t = sys[s];
+      TriOut& o = out[s];
+      auto pick = [&](void* const* tab, size_t idx, int i, int j) -> cplx* {
+        if (Gfull) return static_cast<cplx*>(Gfull[(size_t)s * npl * npl + (size_t)i * npl + j]);
+        return tab ? static_cast<cplx*>(tab[idx]) : nullptr;
+      };
+      for (int i = 0; i < npl; ++i) {
+        cplx* p = pick(Gd, (size_t)s * npl + i, i, i);
+        if (!p) return fail(NEGF_ERR_INVALID, "NULL diagonal output block");
+        o.d.push_back(p);
+        o.ldd.push_back(t.b[i]);
+      }
+      for (int i = 0; i + 1 < npl; ++i) {
+        cplx* u = pick(Gu, (size_t)s * (npl - 1) + i, i, i + 1);
+        cplx* l = pick(Gl, (size_t)s * (npl - 1) + i, i + 1, i);
+        if (!u) u = plan.alloc_c((size_t)t.b[i] * t.b[i + 1]);
+        if (!l) l = plan.alloc_c((size_t)t.b[i] * t.b[i + 1]);
+        o.u.push_back(u); o.ldu.push_back(t.b[i]);
+        o.l.push_back(l); o.ldl.push_back(t.b[i + 1]);
+      }
+      if (Gfull) {
+        full[s].assign((size_t)npl * npl, nullptr);
+        for (int i = 0; i < npl; ++i)
+          for (int j = 0; j < npl; ++j)
+            full[s][(size_t)i * npl + j] = static_cast<cplx*>(Gfull[(size_t)s * npl * npl + (size_t)i * npl + j]);
+        for (int i = 0; i < npl; ++i) full[s][(size_t)i * npl + i] = o.d[i];
+        for (int i = 0; i + 1 < npl; ++i) {
+          full[s][(size_t)i * npl + i + 1] = o.u[i];
+          full[s][(size_t)(i + 1) * npl + i] = o.l[i];
+        }
+      }
+    }
+    build_rgf_downward(plan, sys, work, out);
+    if (Gfull) build_rgf_full_inverse(plan, sys, work, full);
+    return run_plan_sync(plan, static_cast<cudaStream_t>(stream), dinfo, nsys, "negf_rgf");
+  } catch (const std::bad_alloc&) {
+    return fail(NEGF_ERR_NOMEM, "device allocation failed");
+  }
+}
+
+int negf_keldysh(int32_t nsys, int32_t npl, const int32_t* block_sizes, void* const* Md, void* const* Mu,
+                 void* const* Ml, void* const* Sd, void* const* Su, void* stream) {
+  if (int r = check_device()) return r;
+  if (!Sd || (npl > 1 && !Su)) return fail(NEGF_ERR_INVALID, "Sd and Su are required");
+  try {
+    Plan plan;
+    int* dinfo = static_cast<int*>(plan.alloc(sizeof(int) * nsys));
+    std::vector<TriSystem> sys;
+    if (int r = make_systems(nsys, npl, block_sizes, Md, Mu, Ml, dinfo, sys)) return r;
+    std::vector<RgfWork> work(nsys);
+    std::vector<HermBlocks> herm(nsys);
+    for (int s = 0; s < nsys; ++s) {
+      alloc_rgf_work(plan, sys[s], work[s]);
+      for (int i = 0; i < npl; ++i) {
+        herm[s].d.push_back(static_cast<cplx*>(Sd[(size_t)s * npl + i]));
+        herm[s].ldd.push_back(sys[s].b[i]);
+      }
+      for (int i = 0; i + 1 < npl; ++i) {
+        herm[s].u.push_back(static_cast<cplx*>(Su[(size_t)s * (npl - 1) + i]));
+        herm[s].ldu.push_back(sys[s].b[i]);
+      }
+    }
+    build_rgf_upward(plan, sys, work);
+    build_rkd(plan, sys, work, herm);
+    return run_plan_sync(plan, static_cast<cudaStream_t>(stream), dinfo, nsys, "negf_keldysh");
+  } catch (const std::bad_alloc&) {
+    return fail(NEGF_ERR_NOMEM, "device allocation failed");
+  }
+}
+
+// --- batched-energy NEGF solver ---------------------------------------------
+
+int negf_device_create(int32_t npl, const int32_t* block_sizes, const void* const* Hd, const void* const* Hu,
+                       const void* sigL, const void* sigR, negf_device_t* out) {
+  if (int r = check_device()) return r;
+  if (!out || npl <= 0 || !block_sizes || !Hd || (npl > 1 && !Hu) || !sigL || !sigR)
+    return fail(NEGF_ERR_INVALID, "bad arguments");
+  std::unique_ptr<negf_device_s> d(new negf_device_s);
+  d->npl = npl;
+  d->b.assign(block_sizes, block_sizes + npl);
+  for (int x : d->b)
+    if (x <= 0 || x > kMaxBlock) return fail(NEGF_ERR_INVALID, "block sizes must be in [1, 1024]");
+  auto dalloc = [&](size_t elems) -> cplx* {
+    void* p = nullptr;
+    if (cudaMalloc(&p, elems * sizeof(cplx)) != cudaSuccess) return nullptr;
+    d->owned.push_back(p);
+    return static_cast<cplx*>(p);
+  };
+  for (int i = 0; i < npl; ++i) {
+    cplx* p = dalloc((size_t)d->b[i] * d->b[i]);
+    if (!p) return fail(NEGF_ERR_NOMEM, "device allocation failed");
+    d->D.push_back(p);
+  }
+  for (int i = 0; i + 1 < npl; ++i) {
+    cplx* p = dalloc((size_t)d->b[i] * d->b[i + 1]);
+    if (!p) return fail(NEGF_ERR_NOMEM, "device allocation failed");
+    d->Hu.push_back(p);
+  }
+  d->gamL = dalloc((size_t)d->b[0] * d->b[0]);
+  d->gamR = dalloc((size_t)d->b[npl - 1] * d->b[npl - 1]);
+  if (!d->gamL || !d->gamR) return fail(NEGF_ERR_NOMEM, "device allocation failed");
+  negf_device_t h = d.release();
+  return negf_device_upload(h, Hd, Hu, sigL, sigR) == NEGF_SUCCESS ? (*out = h, NEGF_SUCCESS)
+                                                                   : (delete h, NEGF_ERR_CUDA);
+}
+
+int negf_device_upload(negf_device_t d, const void* const* Hd, const void* const* Hu, const void* sigL,
+                       const void* sigR) {
+  if (!d) return fail(NEGF_ERR_INVALID, "NULL device");
+  const int n = d->npl;
+  // host-side assembly of D_0 = H_00 + Sigma_L, D_{N-1} = H + Sigma_R and the Gammas
+  for (int i = 0; i < n; ++i) {
+    size_t cnt = (size_t)d->b[i] * d->b[i];
+    std::vector<cplx> h(cnt);
+    std::memcpy(h.data(), Hd[i], cnt * sizeof(cplx));
+    if (i == 0)
+      for (size_t k = 0; k < cnt; ++k) h[k] = cadd(h[k], static_cast<const cplx*>(sigL)[k]);
+    if (i == n - 1)
+      for (size_t k = 0; k < cnt; ++k) h[k] = cadd(h[k], static_cast<const cplx*>(sigR)[k]);
+    NEGF_TRY_CUDA(cudaMemcpy(d->D[i], h.data(), cnt * sizeof(cplx), cudaMemcpyHostToDevice), "device upload");
+  }
+  for (int i = 0; i + 1 < n; ++i)
+    NEGF_TRY_CUDA(cudaMemcpy(d->Hu[i], Hu[i], (size_t)d->b[i] * d->b[i + 1] * sizeof(cplx), cudaMemcpyHostToDevice),
+                  "device upload");
+  auto gamma = [](const cplx* s, int b, std::vector<cplx>& g) {
+    g.resize((size_t)b * b);
+    for (int c = 0; c < b; ++c)
+      for (int r = 0; r < b; ++r) {
+        cplx a = s[r + (size_t)c * b], at = s[c + (size_t)r * b];
+        cplx diff = make_double2(a.x - at.x, a.y + at.y);  // Sigma - Sigma^H
+        g[r + (size_t)c * b] = make_double2(-diff.y, diff.x);  // i * diff
+      }
+  };
+  std::vector<cplx> g;
+  gamma(static_cast<const cplx*>(sigL), d->b[0], g);
+  NEGF_TRY_CUDA(cudaMemcpy(d->gamL, g.data(), g.size() * sizeof(cplx), cudaMemcpyHostToDevice), "device upload");
+  gamma(static_cast<const cplx*>(sigR), d->b[n - 1], g);
+  NEGF_TRY_CUDA(cudaMemcpy(d->gamR, g.data(), g.size() * sizeof(cplx), cudaMemcpyHostToDevice), "device upload");
+  return NEGF_SUCCESS;
+}
+
+int negf_device_destroy(negf_device_t dev) {
+  delete dev;
+  return NEGF_SUCCESS;
+}
+
+int negf_solver_create(negf_device_t dev, int32_t nE, const negf_solve_opts* opts, negf_solver_t* out) {
+  if (int r = check_device()) return r;
+  if (!dev || nE <= 0 || !opts || !out) return fail(NEGF_ERR_INVALID, "bad arguments");
+  std::unique_ptr<negf_solver_s> s(new negf_solver_s);
+  s->dev = dev;
+  s->nE = nE;
+  s->opts = *opts;
+  s->plan.reset(new Plan);
+  try {
+    if (int r = build_solver(*s)) return r;
+  } catch (const std::bad_alloc&) {
+    return fail(NEGF_ERR_NOMEM, "device allocation failed (reduce the number of energies per batch)");
+  }
+  *out = s.release();
+  return NEGF_SUCCESS;
+}
+
+int negf_solver_destroy(negf_solver_t s) {
+  delete s;
+  return NEGF_SUCCESS;
+}
+
+int negf_solver_set_energies(negf_solver_t s, const double* energies, void* stream) {
+  if (!s || !energies) return fail(NEGF_ERR_INVALID, "bad arguments");
+  const int nE = s->nE;
+  std::vector<cplx> p(3 * (size_t)nE);
+  const negf_solve_opts& o = s->opts;
+  for (int e = 0; e < nE; ++e) {
+    double E = energies[e];
+    p[e] = make_double2(E, o.eta);
+    p[nE + e] = make_double2(1.0 / (1.0 + std::exp((E - o.mu_l) / o.kT)), 0.0);
+    p[2 * nE + e] = make_double2(1.0 / (1.0 + std::exp((E - o.mu_r) / o.kT)), 0.0);
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  NEGF_TRY_CUDA(cudaMemcpyAsync(s->params, p.data(), p.size() * sizeof(cplx), cudaMemcpyHostToDevice, st),
+                "set energies");
+  NEGF_TRY_CUDA(cudaMemsetAsync(s->info, 0, sizeof(int) * nE, st), "set energies");
+  return NEGF_SUCCESS;
+}
+
+int negf_solver_run(negf_solver_t s, void* stream) {
+  if (!s) return fail(NEGF_ERR_INVALID, "NULL solver");
+  // the legacy NULL stream cannot be captured: replay the launches directly there
+  cudaError_t e = s->plan->run(static_cast<cudaStream_t>(stream), stream != nullptr);
+  if (e != cudaSuccess) return cuda_fail(e, "negf_solver_run");
+  return NEGF_SUCCESS;
+}
+
+int negf_solver_outputs(negf_solver_t s, void** gr_dev, void** gl_dev, double** t_dev) {
+  if (!s) return fail(NEGF_ERR_INVALID, "NULL solver");
+  if (gr_dev) *gr_dev = s->gr;
+  if (gl_dev) *gl_dev = s->gl;
+  if (t_dev) *t_dev = s->t2;
+  return NEGF_SUCCESS;
+}
+
+int negf_solver_stats(negf_solver_t s, double* flops, int64_t* launches, int64_t* workspace_bytes) {
+  if (!s) return fail(NEGF_ERR_INVALID, "NULL solver");
+  if (flops) *flops = s->plan->flops();
+  if (launches) *launches = (int64_t)s->plan->num_launches();
+  if (workspace_bytes) *workspace_bytes = (int64_t)s->plan->workspace_bytes();
+  return NEGF_SUCCESS;
+}
+
+int negf_solver_check(negf_solver_t s) {
+  if (!s) return fail(NEGF_ERR_INVALID, "NULL solver");
+  std::vector<int> h(s->nE);
+  NEGF_TRY_CUDA(cudaMemcpy(h.data(), s->info, sizeof(int) * s->nE, cudaMemcpyDeviceToHost), "solver check");
+  for (int e = 0; e < s->nE; ++e)
+    if (h[e]) {
+      char buf[128];
+      std::snprintf(buf, sizeof buf, "energy %d: zero pivot (column %d of a diagonal block)", e, h[e]);
+      return fail(NEGF_ERR_SINGULAR, buf);
+    }
+  return NEGF_SUCCESS;
+}
+
+int negf_solve(negf_device_t dev, int32_t nE, const double* energies, const negf_solve_opts* opts, void* gr_out,
+               void* gl_out, double* t_out, int32_t out_on_device, void* stream) {
+  if (int r = check_device()) return r;
+  if (!dev || nE <= 0 || !energies || !opts) return fail(NEGF_ERR_INVALID, "bad arguments");
+  negf_solve_opts o = *opts;
+  o.want_gr = gr_out != nullptr;
+  o.want_gl = gl_out != nullptr;
+  o.want_t = t_out != nullptr;
+  int chunk = o.max_chunk > 0 ? std::min(o.max_chunk, nE) : nE;
+  if (o.max_chunk <= 0) {
+    size_t fr = 0, tot = 0;
+    NEGF_TRY_CUDA(cudaMemGetInfo(&fr, &tot), "negf_solve");
+    double budget = o.hbm_budget_gb > 0 ? o.hbm_budget_gb * 1e9 : 0.8 * (double)fr;
+    size_t per = solver_bytes_per_energy(*dev, o);
+    int fit = (int)std::max(1.0, std::floor(budget / (double)per));
+    chunk = std::min(nE, fit);
+  }
+  negf_solver_t s = nullptr;
+  if (int r = negf_solver_create(dev, chunk, &o, &s)) return r;
+  std::unique_ptr<negf_solver_s> guard(s);
+  cudaStream_t own = nullptr;
+  if (!stream) {
+    NEGF_TRY_CUDA(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking), "negf_solve");
+    stream = own;
+  }
+  struct StreamGuard {
+    cudaStream_t s;
+    ~StreamGuard() { if (s) cudaStreamDestroy(s); }
+  } sg{own};
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t per = s->per_energy;
+  std::vector<double> eb(chunk);
+  std::vector<double> t2(2 * (size_t)chunk);
+  cudaMemcpyKind kind = out_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  for (int e0 = 0; e0 < nE; e0 += chunk) {
+    int cnt = std::min(chunk, nE - e0);
+    for (int e = 0; e < chunk; ++e) eb[e] = energies[e0 + std::min(e, cnt - 1)];
+    if (int r = negf_solver_set_energies(s, eb.data(), stream)) return r;
+    if (int r = negf_solver_run(s, stream)) return r;
+    if (gr_out)
+      NEGF_TRY_CUDA(cudaMemcpyAsync(static_cast<cplx*>(gr_out) + (size_t)e0 * per, s->gr, (size_t)cnt * per * sizeof(cplx),
+                                    kind, st), "negf_solve output");
+    if (gl_out)
+      NEGF_TRY_CUDA(cudaMemcpyAsync(static_cast<cplx*>(gl_out) + (size_t)e0 * per, s->gl, (size_t)cnt * per * sizeof(cplx),
+                                    kind, st), "negf_solve output");
+    if (t_out) {
+      NEGF_TRY_CUDA(cudaMemcpyAsync(t2.data(), s->t2, 2 * (size_t)cnt * sizeof(double), cudaMemcpyDeviceToHost, st),
+                    "negf_solve output");
+    }
+    NEGF_TRY_CUDA(cudaStreamSynchronize(st), "negf_solve");
+    if (int r = negf_solver_check(s)) return r;
+    if (t_out) {
+      if (out_on_device) {
+        std::vector<double> tr(cnt);
+        for (int e = 0; e < cnt; ++e) tr[e] = t2[2 * e];
+        NEGF_TRY_CUDA(cudaMemcpy(t_out + e0, tr.data(), cnt * sizeof(double), cudaMemcpyHostToDevice), "negf_solve");
+      } else {
+        for (int e = 0; e < cnt; ++e) t_out[e0 + e] = t2[2 * e];
+      }
+    }
+  }
+  return NEGF_SUCCESS;
+}
+
+int negf_probe_fp64_peak(double* dmma_tflops, double* dfma_tflops) {
+  if (int r = check_device()) return r;
+  int dev = 0, sms = 0;
+  NEGF_TRY_CUDA(cudaGetDevice(&dev), "probe");
+  NEGF_TRY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "probe");
+  const int blocks = sms * 4, threads = 256, iters = 20000;
+  double* out = nullptr;
+  NEGF_TRY_CUDA(cudaMalloc(&out, sizeof(double) * blocks * threads), "probe");
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  float ms = 0.f;
+  probe_dmma<<<blocks, threads>>>(out, 100);
+  cudaEventRecord(a);
+  probe_dmma<<<blocks, threads>>>(out, iters);
+  cudaEventRecord(b);
+  cudaEventSynchronize(b);
+  cudaEventElapsedTime(&ms, a, b);
+  if (dmma_tflops) *dmma_tflops = 2.0 * 16 * 8 * 4 * 2.0 * iters * blocks * (threads / 32) / (ms * 1e9);
+  probe_dfma<<<blocks, threads>>>(out, 100);
+  cudaEventRecord(a);
+  probe_dfma<<<blocks, threads>>>(out, iters);
+  cudaEventRecord(b);
+  cudaEventSynchronize(b);
+  cudaEventElapsedTime(&ms, a, b);
+  if (dfma_tflops) *dfma_tflops = 2.0 * 8 * iters * (double)blocks * threads / (ms * 1e9);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaError_t e = cudaGetLastError();
+  cudaFree(out);
+  if (e != cudaSuccess) return cuda_fail(e, "probe");
+  return NEGF_SUCCESS;
+}
+
+}  // extern "C"

@@ -1,0 +1,243 @@
+// Batched complex FP64 GEMM on the sm_100a FP64 tensor path (DMMA).
+//
+// Every Schur-complement product of the RGF / RKD / selected-inverse / DDRGF
+// sweeps (the reference's be_gemm!, src/backend_cpu.jl:208-219, and the
+// getrs-with-explicit-inverse products that replace be_mldivide!) runs here.
+//
+// Design:
+//  * one launch covers a whole list of independent problems of arbitrary
+//    (m, n, k) -- all energies x all blocks of one sweep step; CTAs map to
+//    (problem, 64x64 output tile) through a prefix sum of tile counts;
+//  * a CTA computes a 64x64 complex tile with 4 warps (2x2 of 32x32); the
+//    K loop stages 64x16 complex A and 16x64 complex B tiles through a
+//    3-stage cp.async pipeline (each complex double is one 16-byte cp.async,
+//    so transposed / conjugated operands are handled on the copy);
+//  * the complex product uses four real mma.sync m16n8k4 f64 products
+//    (re += Ar*Br - Ai*Bi, im += Ar*Bi + Ai*Br); FP64 has no tcgen05 kind,
+//    and on B200 mma.sync f64 and DFMA both peak near 37 TFLOP/s (measured
+//    by negf_probe_fp64_peak), so DMMA is the FP64 tensor path;
+//  * epilogue: C = alpha*acc + beta*Cin + diag*I, bounds-checked.
+#include "negf_common.cuh"
+
+namespace negf {
+
+namespace gemm {
+constexpr int BM = 64, BN = 64, BK = 16;
+constexpr int THREADS = 128;
+constexpr int STAGES = 3;
+constexpr int AS_LD = BM + 1;  // As[k][m]
+constexpr int BS_LD = BK + 1;  // Bs[n][k]
+constexpr int AS_SIZE = BK * AS_LD;
+constexpr int BS_SIZE = BN * BS_LD;
+constexpr int STAGE_SIZE = AS_SIZE + BS_SIZE;  // complex elements per stage
+constexpr size_t SMEM_BYTES = size_t(STAGES) * STAGE_SIZE * sizeof(cplx);
+}  // namespace gemm
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool pred) {
+  unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  int sz = pred ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ void dmma16x8x4(double& c0, double& c1, double& c2, double& c3, double a0, double a1,
+                                           double b0) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+      : "+d"(c0), "+d"(c1), "+d"(c2), "+d"(c3)
+      : "d"(a0), "d"(a1), "d"(b0));
+}
+
+// Stage one K-slab of A (BM x BK of op(A)) and B (BK x BN of op(B)).
+template <bool TA, bool TB>
+__device__ __forceinline__ void load_stage(cplx* As, cplx* Bs, const ZGemmProblem& p, int m0, int n0, int k0,
+                                           int tid) {
+  using namespace gemm;
+  // A tile: element (r, kk) of op(A)
+#pragma unroll
+  for (int i = 0; i < (BM * BK) / THREADS; ++i) {
+    int idx = tid + i * THREADS;
+    int r, kk;
+    if (!TA) { r = idx % BM; kk = idx / BM; }   // contiguous in r for column-major A
+    else     { kk = idx % BK; r = idx / BK; }   // contiguous in k for A^T / A^H
+    int gr = m0 + r, gk = k0 + kk;
+    bool ok = gr < p.m && gk < p.k;
+    const cplx* src = p.A;
+    if (ok) src = TA ? (p.A + gk + (size_t)gr * p.lda) : (p.A + gr + (size_t)gk * p.lda);
+    cp_async16(&As[kk * AS_LD + r], src, ok);
+  }
+  // B tile: element (kk, c) of op(B)
+#pragma unroll
+  for (int i = 0; i < (BN * BK) / THREADS; ++i) {
+    int idx = tid + i * THREADS;
+    int c, kk;
+    if (!TB) { kk = idx % BK; c = idx / BK; }   // contiguous in k for column-major B
+    else     { c = idx % BN; kk = idx / BN; }   // contiguous in n for B^T / B^H
+    int gc = n0 + c, gk = k0 + kk;
+    bool ok = gc < p.n && gk < p.k;
+    const cplx* src = p.B;
+    if (ok) src = TB ? (p.B + gc + (size_t)gk * p.ldb) : (p.B + gk + (size_t)gc * p.ldb);
+    cp_async16(&Bs[c * BS_LD + kk], src, ok);
+  }
+}
+
+template <bool TA, bool CA, bool TB, bool CB>
+__global__ void __launch_bounds__(gemm::THREADS, 2)
+    zgemm_batched_kernel(const ZGemmProblem* __restrict__ probs, const int* __restrict__ tile_start, int nprob) {
+  using namespace gemm;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx* smem = reinterpret_cast<cplx*>(smem_raw);
+
+  // map CTA -> (problem, tile) by binary search over the tile prefix sum
+  int bid = blockIdx.x;
+  int lo = 0, hi = nprob - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (tile_start[mid] <= bid) lo = mid; else hi = mid - 1;
+  }
+  const ZGemmProblem p = probs[lo];
+  int t = bid - tile_start[lo];
+  int tiles_m = (p.m + BM - 1) / BM;
+  int m0 = (t % tiles_m) * BM;
+  int n0 = (t / tiles_m) * BN;
+
+  int tid = threadIdx.x;
+  int warp = tid >> 5, lane = tid & 31;
+  int g = lane >> 2, tq = lane & 3;
+  int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
+
+  double acc_re[2][4][4], acc_im[2][4][4];
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) { acc_re[a][b][c] = 0.0; acc_im[a][b][c] = 0.0; }
+
+  int nk = (p.k + BK - 1) / BK;
+  // prologue
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < nk) load_stage<TA, TB>(smem + s * STAGE_SIZE, smem + s * STAGE_SIZE + AS_SIZE, p, m0, n0, s * BK, tid);
+    cp_async_commit();
+  }
+
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    // prefetch the slab STAGES-1 ahead into the buffer freed last iteration
+    int kn = kt + STAGES - 1;
+    if (kn < nk) {
+      int s = kn % STAGES;
+      load_stage<TA, TB>(smem + s * STAGE_SIZE, smem + s * STAGE_SIZE + AS_SIZE, p, m0, n0, kn * BK, tid);
+    }
+    cp_async_commit();
+
+    const cplx* As = smem + (kt % STAGES) * STAGE_SIZE;
+    const cplx* Bs = As + AS_SIZE;
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 4) {
+      double ar[2][2], ai[2][2], br[4], bi[4], nbi[4];
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi) {
+        cplx x0 = As[(kk + tq) * AS_LD + wm + mi * 16 + g];
+        cplx x1 = As[(kk + tq) * AS_LD + wm + mi * 16 + g + 8];
+        ar[mi][0] = x0.x; ai[mi][0] = CA ? -x0.y : x0.y;
+        ar[mi][1] = x1.x; ai[mi][1] = CA ? -x1.y : x1.y;
+      }
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) {
+        cplx y = Bs[(wn + ni * 8 + g) * BS_LD + kk + tq];
+        br[ni] = y.x;
+        bi[ni] = CB ? -y.y : y.y;
+        nbi[ni] = -bi[ni];
+      }
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) {
+          double* cr = acc_re[mi][ni];
+          double* ci = acc_im[mi][ni];
+          dmma16x8x4(cr[0], cr[1], cr[2], cr[3], ar[mi][0], ar[mi][1], br[ni]);
+          dmma16x8x4(cr[0], cr[1], cr[2], cr[3], ai[mi][0], ai[mi][1], nbi[ni]);
+          dmma16x8x4(ci[0], ci[1], ci[2], ci[3], ar[mi][0], ar[mi][1], bi[ni]);
+          dmma16x8x4(ci[0], ci[1], ci[2], ci[3], ai[mi][0], ai[mi][1], br[ni]);
+        }
+    }
+  }
+  cp_async_wait<0>();
+
+  // epilogue
+  const bool has_ab = p.k > 0;
+  const bool has_cin = (p.beta.x != 0.0 || p.beta.y != 0.0) && p.Cin != nullptr;
+  const cplx dg = p.diag_ptr ? *p.diag_ptr : p.diag;
+#pragma unroll
+  for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        int r = m0 + wm + mi * 16 + g + ((e >> 1) << 3);
+        int c = n0 + wn + ni * 8 + 2 * tq + (e & 1);
+        if (r < p.m && c < p.n) {
+          cplx v = make_double2(0.0, 0.0);
+          if (has_ab) {
+            double xr = acc_re[mi][ni][e], xi = acc_im[mi][ni][e];
+            v.x = p.alpha.x * xr - p.alpha.y * xi;
+            v.y = p.alpha.x * xi + p.alpha.y * xr;
+          }
+          if (has_cin) {
+            cplx ci = p.Cin[r + (size_t)c * p.ldcin];
+            v.x += p.beta.x * ci.x - p.beta.y * ci.y;
+            v.y += p.beta.x * ci.y + p.beta.y * ci.x;
+          }
+          if (r == c) { v.x += dg.x; v.y += dg.y; }
+          p.C[r + (size_t)c * p.ldc] = v;
+        }
+      }
+}
+
+using ZGemmKernel = void (*)(const ZGemmProblem*, const int*, int);
+
+static ZGemmKernel pick_kernel(char opA, char opB) {
+  int ia = opA == 'N' ? 0 : (opA == 'T' ? 1 : 2);
+  int ib = opB == 'N' ? 0 : (opB == 'T' ? 1 : 2);
+  switch (ia * 3 + ib) {
+    case 0: return zgemm_batched_kernel<false, false, false, false>;
+    case 1: return zgemm_batched_kernel<false, false, true, false>;
+    case 2: return zgemm_batched_kernel<false, false, true, true>;
+    case 3: return zgemm_batched_kernel<true, false, false, false>;
+    case 4: return zgemm_batched_kernel<true, false, true, false>;
+    case 5: return zgemm_batched_kernel<true, false, true, true>;
+    case 6: return zgemm_batched_kernel<true, true, false, false>;
+    case 7: return zgemm_batched_kernel<true, true, true, false>;
+    default: return zgemm_batched_kernel<true, true, true, true>;
+  }
+}
+
+size_t zgemm_smem_bytes() { return gemm::SMEM_BYTES; }
+
+// Raise the dynamic shared-memory limit of one op variant on the current
+// device; done when a plan is finalised, outside any stream capture.
+cudaError_t zgemm_prepare(char opA, char opB) {
+  return cudaFuncSetAttribute(pick_kernel(opA, opB), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)gemm::SMEM_BYTES);
+}
+
+// Host launcher.  probs_dev / tile_start_dev are device arrays prepared by the
+// caller (tile_start has nprob entries, exclusive prefix sum of tile counts).
+cudaError_t launch_zgemm_batched(char opA, char opB, const ZGemmProblem* probs_dev, const int* tile_start_dev,
+                                 int nprob, int total_tiles, cudaStream_t stream) {
+  if (nprob <= 0 || total_tiles <= 0) return cudaSuccess;
+  pick_kernel(opA, opB)<<<total_tiles, gemm::THREADS, gemm::SMEM_BYTES, stream>>>(probs_dev, tile_start_dev, nprob);
+  return cudaGetLastError();
+}
+
+int zgemm_tiles(int m, int n) {
+  if (m <= 0 || n <= 0) return 0;
+  return ((m + gemm::BM - 1) / gemm::BM) * ((n + gemm::BN - 1) / gemm::BN);
+}
+
+}  // namespace negf

@@ -1,0 +1,200 @@
+// Batched complex FP64 block inversion by blocked Gauss-Jordan with partial
+// pivoting.
+//
+// The reference factors every diagonal Schur complement with zgetrf and then
+// applies X^{-1} through zgetrs (be_lu! / be_mldivide!, src/backend_cpu.jl:
+// 147-206); the downward pass needs X^{-1} explicitly anyway
+// (src/matinvertndiag_rgf.jl:169,180).  Here X^{-1} is formed once, so every
+// later use is a tensor-core GEMM.
+//
+// Algorithm (per matrix, n x n, panel width nb):
+//   for each panel K = [k0, k0+nb):
+//     * panel kernel (one CTA per matrix): the n x nb slab W[:,K] is held in
+//       shared memory; for each column c: warp-level arg-max of |re|+|im| over
+//       rows not yet used as pivots (LAPACK's izamax rule, ties to the lowest
+//       row), then the in-place Gauss-Jordan step on the slab.  No rows are
+//       swapped; the pivot row of column c is recorded in piv[c].  The kernel
+//       writes the slab back and prepares the rank-nb update
+//         F = slab - E_P (E_P has 1 at (piv[k0+i], i)),  Bbuf = W[P, :] with
+//         the K columns zeroed;
+//     * a batched GEMM applies W += F * Bbuf (the same kernel as all other
+//       products).
+//   Finally inv(X)[r, piv[c]] = W[piv[r], c]; a gather kernel writes the
+//   un-permuted inverse to its destination.
+// When n * n fits in shared memory the whole matrix is one panel and no GEMM
+// is needed.
+#include "negf_common.cuh"
+
+namespace negf {
+
+constexpr int GJ_THREADS = 512;
+
+struct GjPanelArgs {
+  int k0;      // first column of this panel
+  int nb;      // panel width (columns)
+  int blocked; // 1: write F/Bbuf for the trailing GEMM; 0: whole matrix in one panel
+};
+
+__device__ __forceinline__ void argmax_merge(double& v, int& r, double v2, int r2) {
+  if (v2 > v || (v2 == v && r2 >= 0 && (r < 0 || r2 < r))) { v = v2; r = r2; }
+}
+
+__global__ void __launch_bounds__(GJ_THREADS)
+    zgj_panel_kernel(const ZInvProblem* __restrict__ probs, GjPanelArgs args) {
+  const ZInvProblem p = probs[blockIdx.x];
+  const int n = p.n;
+  const int k0 = args.k0;
+  if (n <= 0 || k0 >= n) return;
+  const int w = min(args.nb, n - k0);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx* S = reinterpret_cast<cplx*>(smem_raw);  // n x w, column-major
+  cplx* colbuf = S + (size_t)n * w;               // n
+  cplx* rowbuf = colbuf + n;                       // w
+  double* redv = reinterpret_cast<double*>(rowbuf + w);  // GJ_THREADS/32
+  int* redr = reinterpret_cast<int*>(redv + GJ_THREADS / 32);
+  int* sh_piv = redr + GJ_THREADS / 32;            // w
+  uint8_t* used = reinterpret_cast<uint8_t*>(sh_piv + w);  // n
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int idx = tid; idx < n * w; idx += GJ_THREADS) {
+    int c = idx / n, r = idx - c * n;
+    S[idx] = p.W[r + (size_t)(k0 + c) * p.ld];
+  }
+  for (int r = tid; r < n; r += GJ_THREADS) used[r] = (k0 == 0) ? 0 : p.used[r];
+  __syncthreads();
+
+  for (int c = 0; c < w; ++c) {
+    // pivot search over unused rows
+    double bv = -1.0;
+    int br = -1;
+    for (int r = tid; r < n; r += GJ_THREADS)
+      if (!used[r]) argmax_merge(bv, br, cabs1(S[(size_t)c * n + r]), r);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      double v2 = __shfl_down_sync(0xffffffffu, bv, off);
+      int r2 = __shfl_down_sync(0xffffffffu, br, off);
+      argmax_merge(bv, br, v2, r2);
+    }
+    if (lane == 0) { redv[warp] = bv; redr[warp] = br; }
+    __syncthreads();
+    if (warp == 0) {
+      bv = lane < GJ_THREADS / 32 ? redv[lane] : -1.0;
+      br = lane < GJ_THREADS / 32 ? redr[lane] : -1;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        double v2 = __shfl_down_sync(0xffffffffu, bv, off);
+        int r2 = __shfl_down_sync(0xffffffffu, br, off);
+        argmax_merge(bv, br, v2, r2);
+      }
+      if (lane == 0) {
+        sh_piv[c] = br;
+        if (br < 0 || bv == 0.0) {
+          if (p.info) atomicCAS(p.info, 0, k0 + c + 1);
+        }
+      }
+    }
+    __syncthreads();
+    const int pr = sh_piv[c];
+    if (pr < 0) break;  // no candidate row: the host reports the info code
+    cplx pivv = S[(size_t)c * n + pr];
+    cplx pv = (pivv.x == 0.0 && pivv.y == 0.0) ? make_double2(0.0, 0.0) : cinv(pivv);
+    // stage column c and the scaled pivot row
+    for (int r = tid; r < n; r += GJ_THREADS) colbuf[r] = S[(size_t)c * n + r];
+    for (int j = tid; j < w; j += GJ_THREADS) rowbuf[j] = (j == c) ? pv : cmul(S[(size_t)j * n + pr], pv);
+    __syncthreads();
+    for (int idx = tid; idx < n * w; idx += GJ_THREADS) {
+      int j = idx / n, r = idx - j * n;
+      cplx v;
+      if (r == pr) v = rowbuf[j];
+      else if (j == c) v = cneg(cmul(colbuf[r], pv));
+      else v = cfms(S[idx], colbuf[r], rowbuf[j]);
+      S[idx] = v;
+    }
+    if (tid == 0) used[pr] = 1;
+    __syncthreads();
+  }
+
+  if (!args.blocked) {
+    // whole matrix in one panel: write the un-permuted inverse directly,
+    // out[r, piv[c]] = S[piv[r], c]
+    bool ok = true;
+    for (int c = 0; c < w; ++c) ok = ok && sh_piv[c] >= 0;
+    if (!ok) return;  // singular: info is set, out is left untouched
+    for (int idx = tid; idx < n * n; idx += GJ_THREADS) {
+      int c = idx / n, r = idx - c * n;
+      p.out[r + (size_t)sh_piv[c] * p.ldo] = S[(size_t)c * n + sh_piv[r]];
+    }
+    return;
+  }
+  // write back slab, pivots and used flags
+  for (int idx = tid; idx < n * w; idx += GJ_THREADS) {
+    int c = idx / n, r = idx - c * n;
+    p.W[r + (size_t)(k0 + c) * p.ld] = S[idx];
+  }
+  for (int c = tid; c < w; c += GJ_THREADS) p.piv[k0 + c] = sh_piv[c];
+  {
+    for (int r = tid; r < n; r += GJ_THREADS) p.used[r] = used[r];
+    // F = slab - E_P  (n x w, ld n)
+    for (int idx = tid; idx < n * w; idx += GJ_THREADS) {
+      int c = idx / n, r = idx - c * n;
+      cplx v = S[idx];
+      if (r == sh_piv[c]) v.x -= 1.0;
+      p.F[idx] = v;
+    }
+    // Bbuf = W[P, :] with panel columns zeroed  (w x n, ld w); the non-panel
+    // columns of W are not modified by this kernel, so these are old values
+    for (int idx = tid; idx < n * w; idx += GJ_THREADS) {
+      int j = idx / w, c = idx - j * w;
+      int pr = sh_piv[c];
+      cplx v = make_double2(0.0, 0.0);
+      if ((j < k0 || j >= k0 + w) && pr >= 0) v = p.W[pr + (size_t)j * p.ld];
+      p.Bbuf[idx] = v;
+    }
+  }
+}
+
+// out[r, j] = W[piv[r], q[j]] with q the inverse permutation of piv:
+// out[r, piv[c]] = W[piv[r], c].
+__global__ void zgj_unpermute_kernel(const ZInvProblem* __restrict__ probs) {
+  const ZInvProblem p = probs[blockIdx.y];
+  const int n = p.n;
+  // one thread per (r, c) element of W's column c -> output column piv[c]
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n * n; idx += gridDim.x * blockDim.x) {
+    int c = idx / n, r = idx - c * n;
+    int pc = p.piv[c], pr = p.piv[r];
+    if (pc < 0 || pr < 0) continue;
+    p.out[r + (size_t)pc * p.ldo] = p.W[pr + (size_t)c * p.ld];
+  }
+}
+
+size_t zgj_panel_smem_bytes(int n, int nb) {
+  int w = nb < n ? nb : n;
+  size_t b = (size_t)n * w * sizeof(cplx) + (size_t)n * sizeof(cplx) + (size_t)w * sizeof(cplx);
+  b += (GJ_THREADS / 32) * (sizeof(double) + sizeof(int)) + (size_t)w * sizeof(int) + (size_t)n;
+  return (b + 15) & ~size_t(15);
+}
+
+cudaError_t launch_zgj_panel(const ZInvProblem* probs_dev, int nprob, int k0, int nb, int blocked, size_t smem,
+                             cudaStream_t stream) {
+  if (nprob <= 0) return cudaSuccess;
+  GjPanelArgs a{k0, nb, blocked};
+  zgj_panel_kernel<<<nprob, GJ_THREADS, smem, stream>>>(probs_dev, a);
+  return cudaGetLastError();
+}
+
+// Raise the dynamic shared-memory limit of the panel kernel (outside capture).
+cudaError_t zgj_prepare(size_t smem) {
+  return cudaFuncSetAttribute(zgj_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+cudaError_t launch_zgj_unpermute(const ZInvProblem* probs_dev, int nprob, int max_n, cudaStream_t stream) {
+  if (nprob <= 0) return cudaSuccess;
+  int per = max_n * max_n;
+  int bx = (per + 255) / 256;
+  if (bx > 64) bx = 64;
+  dim3 grid(bx, nprob);
+  zgj_unpermute_kernel<<<grid, 256, 0, stream>>>(probs_dev);
+  return cudaGetLastError();
+}
+
+}  // namespace negf

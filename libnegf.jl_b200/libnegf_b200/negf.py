@@ -1,0 +1,152 @@
+"""Batched-energy NEGF solves on the B200 library.
+
+The reference computes one energy point per call (RGF for G^R, RKD for G^n);
+here a ``Device`` keeps H, Sigma_L, Sigma_R resident on the GPU and a
+``Solver`` runs RGF + RKD + transmission for a whole list of energies in one
+replayed launch sequence (CUDA graph).
+
+Physics: M(E) = (E + i eta) I - H - Sigma (Sigma_L on layer 0, Sigma_R on layer
+N-1), Gamma = i (Sigma - Sigma^H), Sigma^in = f_L Gamma_L (+) f_R Gamma_R with
+Fermi functions at mu_L / mu_R and temperature kT, G^< = i G^R Sigma^in G^A,
+T(E) = Re Tr[Gamma_L G^R_{1N} Gamma_R G^A_{N1}].
+"""
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, load, ptr_array, int_array
+
+
+def _host_blocks(blocks):
+    """Keep column-major complex128 copies alive and return their addresses."""
+    keep = [np.asfortranarray(np.asarray(b, dtype=np.complex128)) for b in blocks]
+    return keep, [k.ctypes.data for k in keep]
+
+
+def make_opts(eta=1e-6, mu_l=0.1, mu_r=-0.1, kT=0.025, want_gr=True, want_gl=True, want_t=True, max_chunk=0,
+              hbm_budget_gb=0.0):
+    o = _lib.SolveOpts()
+    o.eta, o.mu_l, o.mu_r, o.kT = eta, mu_l, mu_r, kT
+    o.want_gr, o.want_gl, o.want_t = int(want_gr), int(want_gl), int(want_t)
+    o.max_chunk = int(max_chunk)
+    o.hbm_budget_gb = float(hbm_budget_gb)
+    return o
+
+
+class Device:
+    """One device (block-tridiagonal H and lead self-energies) on the GPU."""
+
+    def __init__(self, Hd, Hu, sigL, sigR):
+        self.sizes = [int(h.shape[0]) for h in Hd]
+        self.npl = len(Hd)
+        self._handle = ctypes.c_void_p()
+        kd, pd = _host_blocks(Hd)
+        ku, pu = _host_blocks(Hu)
+        sl = np.asfortranarray(np.asarray(sigL, dtype=np.complex128))
+        sr = np.asfortranarray(np.asarray(sigR, dtype=np.complex128))
+        check(load().negf_device_create(self.npl, int_array(self.sizes), ptr_array(pd), ptr_array(pu),
+                                        sl.ctypes.data, sr.ctypes.data, ctypes.byref(self._handle)))
+
+    def upload(self, Hd, Hu, sigL, sigR):
+        kd, pd = _host_blocks(Hd)
+        ku, pu = _host_blocks(Hu)
+        sl = np.asfortranarray(np.asarray(sigL, dtype=np.complex128))
+        sr = np.asfortranarray(np.asarray(sigR, dtype=np.complex128))
+        check(load().negf_device_upload(self._handle, ptr_array(pd), ptr_array(pu), sl.ctypes.data, sr.ctypes.data))
+
+    @property
+    def handle(self):
+        return self._handle
+
+    def close(self):
+        if self._handle:
+            load().negf_device_destroy(self._handle)
+            self._handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solve(self, energies, eta=1e-6, mu_l=0.1, mu_r=-0.1, kT=0.025, want_gr=True, want_gl=True, want_t=True,
+              max_chunk=0):
+        """G^R / G^< diagonal blocks and T(E) for every energy (host arrays).
+
+        Returns (gr, gl, t): gr/gl are lists (per energy) of lists (per layer)
+        of b_i x b_i arrays, or None."""
+        E = np.ascontiguousarray(np.asarray(energies, dtype=np.float64))
+        nE = len(E)
+        per = sum(b * b for b in self.sizes)
+        gr = np.empty(nE * per, dtype=np.complex128) if want_gr else None
+        gl = np.empty(nE * per, dtype=np.complex128) if want_gl else None
+        t = np.empty(nE, dtype=np.float64) if want_t else None
+        o = make_opts(eta, mu_l, mu_r, kT, want_gr, want_gl, want_t, max_chunk)
+        check(load().negf_solve(self._handle, nE, E.ctypes.data_as(_lib.c_double_p), ctypes.byref(o),
+                                gr.ctypes.data if gr is not None else None,
+                                gl.ctypes.data if gl is not None else None,
+                                t.ctypes.data_as(_lib.c_double_p) if t is not None else None, 0, None))
+        return self._split(gr, nE), self._split(gl, nE), t
+
+    def _split(self, flat, nE):
+        if flat is None:
+            return None
+        per = sum(b * b for b in self.sizes)
+        out = []
+        for e in range(nE):
+            o = e * per
+            row = []
+            for b in self.sizes:
+                row.append(flat[o:o + b * b].reshape(b, b, order="F"))
+                o += b * b
+            out.append(row)
+        return out
+
+
+class Solver:
+    """Resident plan for repeated solves of nE energies (device outputs)."""
+
+    def __init__(self, device, nE, **kw):
+        self.device = device
+        self.nE = int(nE)
+        self.opts = make_opts(**kw)
+        self._h = ctypes.c_void_p()
+        check(load().negf_solver_create(device.handle, self.nE, ctypes.byref(self.opts), ctypes.byref(self._h)))
+
+    def set_energies(self, energies, stream=None):
+        E = np.ascontiguousarray(np.asarray(energies, dtype=np.float64))
+        assert len(E) == self.nE
+        check(load().negf_solver_set_energies(self._h, E.ctypes.data_as(_lib.c_double_p), stream))
+
+    def run(self, stream=None):
+        check(load().negf_solver_run(self._h, stream))
+
+    def check(self):
+        check(load().negf_solver_check(self._h))
+
+    def outputs(self):
+        gr = ctypes.c_void_p()
+        gl = ctypes.c_void_p()
+        t = ctypes.POINTER(ctypes.c_double)()
+        check(load().negf_solver_outputs(self._h, ctypes.byref(gr), ctypes.byref(gl), ctypes.byref(t)))
+        return gr.value, gl.value, ctypes.cast(t, ctypes.c_void_p).value
+
+    def stats(self):
+        f = ctypes.c_double()
+        n = ctypes.c_int64()
+        w = ctypes.c_int64()
+        check(load().negf_solver_stats(self._h, ctypes.byref(f), ctypes.byref(n), ctypes.byref(w)))
+        return {"flops": f.value, "launches": n.value, "workspace_bytes": w.value}
+
+    def close(self):
+        if self._h:
+            load().negf_solver_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,191 @@
+"""GPU parity of general RGF, the fused variant, the selected inverse, DDRGF,
+the LU backend primitives and the reference's C entry point.
+
+Tolerances follow the reference tests: 1e-12 for general RGF / fused
+(test_matinvertndiag_general_rgf*.jl, roundoffs[ComplexF64]*1e3), 2.5e-10 for
+DDRGF vs sequential RGF (test_matinvertndiag_ddrgf.jl:16), 1e-13 absolute for
+the selected inverse (test_selected_inverse.jl:51) and 1e-15-scale relative
+for the block LU (:20-21, relaxed to 1e-14 for GPU summation order).
+"""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import rel_fro
+from oracle import rgf as o_rgf, general_rgf as o_grgf, selected_inverse as o_si, ddrgf as o_dd
+from oracle.blockmatrix import bm_convert_dense, band_of_dense, bm_fuse_to_tridiagonal as o_fuse
+from oracle.generators import bm_create_synthetic_random, set_sparse_block, full_of_blocks
+
+pytestmark = pytest.mark.gpu
+
+
+def _to_gpu_bm(negf, bm):
+    out = negf.BlockMatrix(bm.blockSizes, None, bm.ndiag, False, bm.isHermitian)
+    for k, v in bm.M.items():
+        out.M[k] = negf.to_device(v)
+    return out
+
+
+@pytest.mark.parametrize("npl,b,nd", [(10, 32, 5), (7, 20, 7), (6, 40, 3), (3, 16, 5), (1, 8, 5)])
+def test_general_rgf(negf, npl, b, nd):
+    M = bm_create_synthetic_random(npl, b, seed=npl + b + nd, ndiag=nd)
+    ref = bm_convert_dense(o_grgf.bndiag_of_inv_general_rgf(M))
+    dM = _to_gpu_bm(negf, M)
+    before = {k: negf.to_host(v).copy() for k, v in dM.M.items()}
+    out = negf.BlockMatrix(M.blockSizes)
+    negf.bndiag_of_inv_general_rgf_(out, dM, negf.allocate_aux_data_general_RGF(dM))
+    G = negf.bm_to_dense(out)
+    assert rel_fro(G, ref) < 1e-12
+    exact = band_of_dense(np.linalg.inv(bm_convert_dense(M)), M.blockSizes, {"in": nd, "out": nd})
+    assert rel_fro(G, exact) < 1e-12
+    for k, v in dM.M.items():  # input left unchanged
+        assert np.array_equal(negf.to_host(v), before[k])
+
+
+def test_general_rgf_vs_fused(negf):
+    # test_matinvertndiag_general_rgf_fused.jl: general n-diagonal RGF vs fuse + RGF
+    M = bm_create_synthetic_random(10, 32, seed=77, ndiag=5)
+    dM = _to_gpu_bm(negf, M)
+    gen = negf.BlockMatrix(M.blockSizes)
+    negf.bndiag_of_inv_general_rgf_(gen, dM)
+    fused = negf.bm_fuse_to_tridiagonal(dM)
+    o_fused = o_fuse(M)
+    assert rel_fro(negf.bm_to_dense(fused), bm_convert_dense(o_fused)) == 0.0
+    fout = negf.BlockMatrix(fused.blockSizes)
+    negf.bndiag_of_inv_rgf_local_(fout, fused)
+    aligned = band_of_dense(negf.bm_to_dense(fout), M.blockSizes, {"in": 5, "out": 5})
+    assert rel_fro(negf.bm_to_dense(gen), aligned) < 1e-12
+
+
+RIND = [1, 1, 1, 2, 3, 3, 3, 4, 5]
+CIND = [1, 3, 5, 2, 3, 4, 5, 4, 5]
+
+
+def _gpu_blocks(negf, A):
+    return {k: negf.Block(negf.to_device(v)) for k, v in A.items()}
+
+
+@pytest.mark.parametrize("bs", [100, 1, 33])
+def test_block_factorization(negf, bs):
+    A = set_sparse_block([bs] * 5, RIND, CIND, True, seed=bs)
+    F_ref = o_si.block_factorization(A, 5)
+    F = negf.Block_factorization(_gpu_blocks(negf, A))
+    Fm = negf.full(F, 5)
+    assert rel_fro(Fm, full_of_blocks(F_ref, [bs] * 5)) < 1e-14
+    # test_selected_inverse.jl:17-21
+    T = full_of_blocks(A, [bs] * 5)
+    n = 5 * bs
+    LU = (np.tril(Fm, -1) + np.eye(n)) @ np.triu(Fm)
+    assert rel_fro(LU, T) < 1e-14
+    import scipy.linalg as sl
+    P, L, U = sl.lu(T)
+    if np.allclose(P, np.eye(n)):
+        assert rel_fro(Fm, np.tril(L, -1) + U) < 1e-14
+
+
+@pytest.mark.parametrize("bs", [1, 100, 24])
+def test_block_inverse(negf, bs):
+    A = set_sparse_block([bs] * 5, RIND, CIND, True, seed=10 + bs)
+    T = full_of_blocks(A, [bs] * 5)
+    Z_ref = o_si.block_inverse(o_si.block_factorization(A, 5), 5)
+    Z = negf.Block_inverse(negf.Block_factorization(_gpu_blocks(negf, A)))
+    invT = np.linalg.inv(T)
+    for (i, j), blk in Z.items():
+        z = negf.to_host(blk.Full)
+        assert np.allclose(z, invT[i * bs:(i + 1) * bs, j * bs:(j + 1) * bs], atol=1e-13, rtol=0)
+        assert np.allclose(z, Z_ref[(i, j)], atol=1e-13, rtol=0)
+    # diag(A * si(A)) = 1 (test_selected_inverse.jl:38-42) on the full inverse
+    full = negf.full(Z, 5)
+    mask = np.zeros_like(T, dtype=bool)
+    for (i, j) in Z:
+        mask[i * bs:(i + 1) * bs, j * bs:(j + 1) * bs] = True
+    assert np.all(np.abs(full[mask] - invT[mask]) < 1e-13)
+
+
+@pytest.mark.parametrize("n", [5, 64, 96, 97, 200, 513])
+def test_getrf_trsm_getri(negf, n):
+    rng = np.random.default_rng(n)
+    A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    import scipy.linalg.lapack as la
+    lu_ref, piv_ref, info = la.zgetrf(A)
+    dA = negf.to_device(A)
+    lib = negf.load()
+    import torch
+    piv = torch.zeros(n, dtype=torch.int32, device="cuda")
+    from libnegf_b200._lib import int_array, ptr_array, check
+    infos = (ctypes.c_int32 * 1)()
+    check(lib.negf_zgetrf_batched(1, int_array([n]), ptr_array([dA.data_ptr()]), int_array([n]),
+                                  ptr_array([piv.data_ptr()]), infos, None))
+    assert np.array_equal(piv.cpu().numpy() - 1, piv_ref)
+    assert rel_fro(negf.to_host(dA), lu_ref) < 1e-13
+    # trsm with the factors: the four forms used by selected_inverse.jl
+    B = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    U = np.triu(lu_ref)
+    L = np.tril(lu_ref, -1) + np.eye(n)
+    cases = [("R", "U", "N", 1.0, B @ np.linalg.inv(U)), ("L", "L", "U", 1.0, np.linalg.solve(L, B)),
+             ("L", "U", "N", -1.0, -np.linalg.solve(U, B)), ("R", "L", "U", -1.0, -B @ np.linalg.inv(L))]
+    for side, uplo, diag, a, ref in cases:
+        alpha = (ctypes.c_double * 2)(a, 0.0)
+        dB = negf.to_device(B)
+        check(lib.negf_ztrsm_batched(side.encode(), uplo.encode(), b"N", diag.encode(), alpha, 1, int_array([n]),
+                                     int_array([n]), ptr_array([dA.data_ptr()]), int_array([n]),
+                                     ptr_array([dB.data_ptr()]), int_array([n]), None))
+        assert rel_fro(negf.to_host(dB), ref) < 1e-11
+    check(lib.negf_zgetri_nopiv_batched(1, int_array([n]), ptr_array([dA.data_ptr()]), int_array([n]), None))
+    assert rel_fro(negf.to_host(dA), np.linalg.inv(U) @ np.linalg.inv(L)) < 1e-11
+
+
+@pytest.mark.parametrize("npl,b,d1", [(32, 16, 6), (128, 24, 15), (20, 40, 4), (18, 8, 3), (8, 30, 1)])
+def test_ddrgf_vs_rgf(negf, npl, b, d1):
+    M = bm_create_synthetic_random(npl, b, seed=npl * 3 + d1)
+    seq = bm_convert_dense(o_rgf.bndiag_of_inv_rgf_local(M))
+    o_par, _ = o_dd.bndiag_of_inv_ddrgf(M, d1)
+    assert rel_fro(bm_convert_dense(o_par), seq) < 2.5e-10
+    dM = _to_gpu_bm(negf, M)
+    aux = negf.allocate_aux_data_DDRGF(dM, blockSizeD1=d1)
+    assert aux[0].nrTasks == o_dd.get_nr_tasks(npl, d1)[0]
+    negf.bndiag_of_inv_ddrgf_(dM, aux)
+    G = negf.bm_to_dense(aux[0].buffMout)
+    assert rel_fro(G, seq) < 2.5e-10
+    assert rel_fro(G, bm_convert_dense(o_par)) < 2.5e-10
+
+
+def test_ddrgf_auto_partition(negf):
+    M = bm_create_synthetic_random(40, 16, seed=9)
+    dM = _to_gpu_bm(negf, M)
+    aux = negf.allocate_aux_data_DDRGF(dM)
+    negf.bndiag_of_inv_ddrgf_(dM, aux)
+    seq = bm_convert_dense(o_rgf.bndiag_of_inv_rgf_local(M))
+    assert rel_fro(negf.bm_to_dense(aux[0].buffMout), seq) < 2.5e-10
+
+
+def test_run_bndiag_wrapper(negf):
+    # the reference C example (src/c_interface/libnegf_c_example.c) builds a
+    # random block tridiagonal CSC matrix and calls run_bndiag_wrapper
+    import scipy.sparse as sp
+    from libnegf_b200._lib import int_array
+    npl, b = 12, 16
+    M = bm_create_synthetic_random(npl, b, seed=123, uniform=True)
+    D = bm_convert_dense(M)
+    csc = sp.csc_matrix(D)
+    n = D.shape[0]
+    colptr = np.ascontiguousarray(csc.indptr, dtype=np.int32)
+    rowval = np.ascontiguousarray(csc.indices, dtype=np.int32)
+    nz = np.ascontiguousarray(csc.data, dtype=np.complex128)
+    keys = (ctypes.c_char_p * 2)(b"in", b"out")
+    lib = negf.load()
+    res = lib.run_bndiag_wrapper(n, n, csc.nnz, colptr.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                 rowval.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), nz.ctypes.data, npl,
+                                 int_array([b] * npl), 2, keys, int_array([3, 3]), 0)
+    assert res.m == n and res.nnz > 0
+    cp = np.ctypeslib.as_array(res.colptr, shape=(n + 1,)).copy()
+    rv = np.ctypeslib.as_array(res.rowval, shape=(res.nnz,)).copy()
+    vals = np.ctypeslib.as_array(ctypes.cast(res.nzval, ctypes.POINTER(ctypes.c_double)), shape=(2 * res.nnz,)).copy()
+    out = sp.csc_matrix((vals[0::2] + 1j * vals[1::2], rv, cp), shape=(n, n)).toarray()
+    libc = ctypes.CDLL(None)
+    for p in (res.colptr, res.rowval, res.nzval):
+        libc.free(ctypes.cast(p, ctypes.c_void_p))
+    ref = band_of_dense(np.linalg.inv(D), M.blockSizes, {"in": 3, "out": 3})
+    assert rel_fro(out, ref) < 2.5e-10

@@ -1,0 +1,216 @@
+"""CPU tests: the oracle against the reference's own test oracles and the
+committed golden fixtures; the DDRGF partition helper; the C ABI exports."""
+
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, rel_fro
+from oracle import rgf, general_rgf, keldysh, selected_inverse, ddrgf, physics
+from oracle.blockmatrix import bm_convert_dense, band_of_dense, bm_from_dense, bm_fuse_to_tridiagonal
+from oracle.generators import bm_create_synthetic_random, hermitian_random_like, set_sparse_block, full_of_blocks
+
+GOLD = os.path.join(ROOT, "tests", "golden")
+ROUNDOFF64 = 1e-15  # test/common_to_test.jl:25-27
+
+
+def _gold(name):
+    return dict(np.load(os.path.join(GOLD, name + ".npz")))
+
+
+@pytest.mark.parametrize("npl,b", [(10, 32), (1, 7), (2, 5), (6, 17)])
+def test_rgf_vs_dense(npl, b):
+    M = bm_create_synthetic_random(npl, b, seed=npl)
+    G = bm_convert_dense(rgf.bndiag_of_inv_rgf_local(M))
+    ref = band_of_dense(np.linalg.inv(bm_convert_dense(M)), M.blockSizes, {"in": 3, "out": 3})
+    assert rel_fro(G, ref) < ROUNDOFF64 * 1e3
+
+
+def test_rgf_full_inverse_vs_dense():
+    M = bm_create_synthetic_random(7, 12, seed=3)
+    G = bm_convert_dense(rgf.bndiag_of_inv_rgf_local(M, build_full_inv=True))
+    assert rel_fro(G, np.linalg.inv(bm_convert_dense(M))) < ROUNDOFF64 * 1e3
+
+
+def test_keldysh_vs_dense():
+    # test_keldyshndiag.jl:60-95
+    M = bm_create_synthetic_random(10, 32, seed=1)
+    S = hermitian_random_like(M, seed=2)
+    Gn = bm_convert_dense(keldysh.keldyshndiag(M, S))
+    Gr = np.linalg.inv(bm_convert_dense(M))
+    bf = Gr @ bm_convert_dense(S) @ Gr.conj().T
+    assert rel_fro(Gn, band_of_dense(bf, M.blockSizes, {"in": 3, "out": 3}, True)) < ROUNDOFF64 * 1e3
+
+
+@pytest.mark.parametrize("nd", [5, 7])
+def test_general_rgf_vs_dense_and_fused(nd):
+    # test_matinvertndiag_general_rgf.jl and _fused.jl
+    M = bm_create_synthetic_random(10, 32, seed=nd, ndiag=nd)
+    G = bm_convert_dense(general_rgf.bndiag_of_inv_general_rgf(M))
+    nd_ = {"in": nd, "out": nd}
+    ref = band_of_dense(np.linalg.inv(bm_convert_dense(M)), M.blockSizes, nd_)
+    assert rel_fro(G, ref) < ROUNDOFF64 * 1e3
+    F = bm_fuse_to_tridiagonal(M)
+    Gf = band_of_dense(bm_convert_dense(rgf.bndiag_of_inv_rgf_local(F)), M.blockSizes, nd_)
+    assert rel_fro(G, Gf) < ROUNDOFF64 * 1e3
+
+
+def test_selected_inverse_reference_cases():
+    # test_selected_inverse.jl:6-55
+    rind = [1, 1, 1, 2, 3, 3, 3, 4, 5]
+    cind = [1, 3, 5, 2, 3, 4, 5, 4, 5]
+    A = set_sparse_block([100] * 5, rind, cind, True, seed=0)
+    F = full_of_blocks(selected_inverse.block_factorization(A, 5), [100] * 5)
+    T = full_of_blocks(A, [100] * 5)
+    import scipy.linalg as sl
+    P, L, U = sl.lu(T)
+    assert np.allclose(P, np.eye(500))
+    assert rel_fro(F, np.tril(L, -1) + U) <= 1e-14
+    assert rel_fro((np.tril(F, -1) + np.eye(500)) @ np.triu(F), T) <= 1e-14
+    A1 = set_sparse_block([1] * 5, rind, cind, True, seed=1)
+    Z = selected_inverse.block_inverse(selected_inverse.block_factorization(A1, 5), 5)
+    T1 = full_of_blocks(A1, [1] * 5)
+    invT = np.linalg.inv(T1)
+    d = np.diag(T1 @ full_of_blocks(Z, [1] * 5))
+    for (i, j), z in Z.items():
+        assert abs(z[0, 0] - invT[i, j]) < 1e-13
+
+
+@pytest.mark.parametrize("npl,d1", [(128, 15), (64, 15), (32, 6), (8, 1), (18, 3)])
+def test_ddrgf_vs_sequential(npl, d1):
+    # test_matinvertndiag_ddrgf.jl:245-293 (2.5e-10)
+    b = 8 if npl > 60 else 16
+    M = bm_create_synthetic_random(npl, b, seed=npl + d1)
+    Gs = bm_convert_dense(rgf.bndiag_of_inv_rgf_local(M))
+    Gp, S = ddrgf.bndiag_of_inv_ddrgf(M, d1)
+    assert rel_fro(bm_convert_dense(Gp), Gs) < ROUNDOFF64 * 2.5e5
+
+
+def test_ddrgf_schur_complement_exact():
+    # test_matinvertndiag_ddrgf.jl:209-241: Schur complement vs exact
+    M = bm_create_synthetic_random(20, 10, seed=5)
+    D = bm_convert_dense(M)
+    seps, doms, perm = ddrgf.partition(20, 4)
+    off = M.offsets()
+    idx = lambda layers: np.concatenate([np.arange(off[l], off[l + 1]) for l in layers])
+    i2 = idx(seps)
+    i1 = idx([l for d in doms for l in d])
+    exact = D[np.ix_(i2, i2)] - D[np.ix_(i2, i1)] @ np.linalg.solve(D[np.ix_(i1, i1)], D[np.ix_(i1, i2)])
+    _, S = ddrgf.bndiag_of_inv_ddrgf(M, 4)
+    sb = [M.blockSizes[s] for s in seps]
+    so = np.concatenate([[0], np.cumsum(sb)])
+    approx = np.zeros_like(exact)
+    for (t, u), blk in S.items():
+        approx[so[t]:so[t + 1], so[u]:so[u + 1]] = blk
+    assert rel_fro(approx, exact) < ROUNDOFF64 * 2.5e5
+
+
+@pytest.mark.parametrize("npl,d1,expect", [(64, 15, (4, 0)), (128, 15, (8, 0)), (40, 6, (6, 4)), (17, 3, (-1, 0)),
+                                           (18, 3, (5, 1)), (9, 1, (-1, 0)), (8, 1, (4, 0)), (10, 4, (2, 0)),
+                                           (32, 6, (5, 3))])
+def test_ddrgf_get_nr_tasks(npl, d1, expect):
+    # matinvertndiag_ddrgf_utils.jl:278-312, worked by hand
+    assert ddrgf.get_nr_tasks(npl, d1) == expect
+
+
+def test_physics_oracle_vs_dense():
+    sysm = physics.physics_system(5, 20, seed=3)
+    for E in (-0.5, 0.25):
+        r = physics.solve_energy(sysm, E)
+        D = bm_convert_dense(sysm.M_of_E(E))
+        Gi = np.linalg.inv(D)
+        nd = {"in": 3, "out": 3}
+        assert rel_fro(bm_convert_dense(r["GR"]), band_of_dense(Gi, sysm.sizes, nd)) < 1e-12
+        Sin = bm_convert_dense(sysm.sigma_in(E))
+        assert rel_fro(bm_convert_dense(r["Gn"]), band_of_dense(Gi @ Sin @ Gi.conj().T, sysm.sizes, nd, True)) < 1e-12
+        b = sysm.sizes[0]
+        g1n = Gi[:b, -b:]
+        T = np.trace(sysm.gamma(sysm.sigL) @ g1n @ sysm.gamma(sysm.sigR) @ g1n.conj().T).real
+        assert abs(r["T"] - T) < 1e-10 * max(1, abs(T))
+
+
+# -- golden fixtures --------------------------------------------------------
+
+def test_golden_rgf_keldysh():
+    g = _gold("rgf_npl10_b32")
+    M = bm_from_dense(g["M"], list(g["sizes"]), {"in": 3, "out": 3})
+    assert rel_fro(bm_convert_dense(rgf.bndiag_of_inv_rgf_local(M)), g["G"]) < 1e-14
+    k = _gold("keldysh_npl10_b32")
+    S = bm_from_dense(k["S"], list(g["sizes"]), {"in": 3, "out": 3}, True)
+    assert rel_fro(bm_convert_dense(keldysh.keldyshndiag(M, S)), k["Gn"]) < 1e-14
+
+
+def test_golden_general_rgf():
+    g = _gold("general_rgf_npl8_b24_n5")
+    M = bm_from_dense(g["M"], list(g["sizes"]), {"in": 5, "out": 5})
+    assert rel_fro(bm_convert_dense(general_rgf.bndiag_of_inv_general_rgf(M)), g["G"]) < 1e-14
+
+
+def test_golden_selected_inverse():
+    g = _gold("selinv_5x40")
+    A = {}
+    for (i, j) in g["pattern"]:
+        blk = g["A"][i * 40:(i + 1) * 40, j * 40:(j + 1) * 40]
+        if np.any(blk != 0):
+            A[(int(i), int(j))] = blk
+    F = selected_inverse.block_factorization(A, 5)
+    assert rel_fro(full_of_blocks(F, [40] * 5).real, g["F"]) < 1e-14
+    Z = selected_inverse.block_inverse(F, 5)
+    assert rel_fro(full_of_blocks(Z, [40] * 5).real, g["Z"]) < 1e-14
+
+
+def test_golden_ddrgf():
+    g = _gold("ddrgf_npl24_b12_d6")
+    M = bm_from_dense(g["M"], list(g["sizes"]), {"in": 3, "out": 3})
+    G, _ = ddrgf.bndiag_of_inv_ddrgf(M, int(g["d1"]))
+    assert rel_fro(bm_convert_dense(G), g["G"]) < 1e-14
+
+
+def test_golden_negf():
+    g = _gold("negf_npl6_b24")
+    sysm = physics.DeviceSystem(list(g["Hd"]), list(g["Hu"]), g["sigL"], g["sigR"], eta=float(g["eta"]))
+    for e, E in enumerate(g["E"]):
+        r = physics.solve_energy(sysm, E)
+        for i in range(6):
+            assert rel_fro(r["GR"].M[(i, i)], g["GR"][e][i]) < 1e-14
+            assert rel_fro(1j * r["Gn"].M[(i, i)], g["GL"][e][i]) < 1e-14
+        assert abs(r["T"] - g["T"][e]) < 1e-13
+
+
+# -- C ABI ------------------------------------------------------------------
+
+def _declared_functions():
+    src = open(os.path.join(ROOT, "include", "negf_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\(", src)
+    skip = {"sizeof", "defined"}
+    return sorted({n for n in names if (n.startswith("negf_") or n == "run_bndiag_wrapper") and n not in skip})
+
+
+def test_library_exports_every_declared_symbol():
+    import ctypes
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "libnegf.jl_b200"))
+    from libnegf_b200 import _lib
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    names = _declared_functions()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    # and the Python binding declares a prototype for each of them
+    assert set(names) <= set(_lib.PROTOTYPES), set(names) - set(_lib.PROTOTYPES)
+
+
+def test_library_fails_loudly_without_device():
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "libnegf.jl_b200"))
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    import libnegf_b200
+    lib = libnegf_b200.load()
+    assert lib.negf_version() == 100
+    with pytest.raises(libnegf_b200.NegfError):
+        libnegf_b200._lib.check(lib.negf_probe_fp64_peak(None, None))
