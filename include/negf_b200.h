@@ -201,8 +201,20 @@ int negf_solver_run(negf_solver_t s, void* stream);
 /* Device pointers of the resident outputs (valid until destroy): gr/gl as in
  * negf_solve; t_dev holds 2*nE doubles (re, im of the trace per energy). */
 int negf_solver_outputs(negf_solver_t s, void** gr_dev, void** gl_dev, double** t_dev);
+/* Copy the resident outputs into host buffers (pinned for full speed) on
+ * `stream` and wait: gr/gl as in negf_solve, t as 2*nE doubles (re, im). */
+int negf_solver_download(negf_solver_t s, void* gr_host, void* gl_host, double* t_host, void* stream);
 /* Synchronous check of the zero-pivot flags of the last run. */
 int negf_solver_check(negf_solver_t s);
+/* One pass launch by launch (no graph) with a CUDA event recorded after every
+ * launch on `stream`; per-launch durations accumulate until read. */
+int negf_solver_run_profiled(negf_solver_t s, void* stream);
+/* Kernel kinds: 0 GEMM, 1 inversion panel, 2 inversion un-permute, 3 block
+ * copies, 4 trace, 5 LU panel, 6 LU row swaps, 7 triangular diagonal blocks.
+ * Synchronises and writes, per kind, the summed milliseconds, real flops and
+ * launch counts of the profiled passes since the last reset (reset != 0
+ * starts a new accumulation). */
+int negf_solver_profile_read(negf_solver_t s, double* ms, double* flops, int64_t* launches, int32_t reset);
 /* Real flops of one pass (8mnk per complex GEMM, 8n^3 per inversion),
  * number of kernel launches per pass and workspace bytes. */
 int negf_solver_stats(negf_solver_t s, double* flops, int64_t* launches, int64_t* workspace_bytes);

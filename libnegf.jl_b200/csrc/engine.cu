@@ -307,6 +307,22 @@ double Plan::flops() const {
 
 size_t Plan::num_launches() const { return steps.size(); }
 
+cudaError_t Plan::run_events(cudaStream_t stream, const std::vector<cudaEvent_t>& events) {
+  if (events.size() < steps.size() + 1) return cudaErrorInvalidValue;
+  cudaError_t e = finalize();
+  if (e != cudaSuccess) return e;
+  e = cudaEventRecord(events[0], stream);
+  if (e != cudaSuccess) return e;
+  const unsigned char* base = static_cast<const unsigned char*>(dblob_);
+  for (size_t i = 0; i < steps.size(); ++i) {
+    e = launch_step(steps[i], base, stream);
+    if (e != cudaSuccess) return e;
+    e = cudaEventRecord(events[i + 1], stream);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 cudaError_t Plan::run(cudaStream_t stream, bool use_graph) {
   cudaError_t e = finalize();
   if (e != cudaSuccess) return e;
@@ -317,6 +333,31 @@ cudaError_t Plan::run(cudaStream_t stream, bool use_graph) {
   }
   const unsigned char* base = static_cast<const unsigned char*>(dblob_);
   for (const auto& s : steps) {
+    e = launch_step(s, base, stream);
+    if (e != cudaSuccess) break;
+  }
+  if (use_graph) {
+    cudaGraph_t g = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(stream, &g);
+    if (e != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return e;
+    }
+    if (e2 != cudaSuccess) return e2;
+    if (gexec_) cudaGraphExecDestroy(gexec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    graph_ = g;
+    e = cudaGraphInstantiate(&gexec_, graph_, 0);
+    if (e != cudaSuccess) return e;
+    graph_stream_ = stream;
+    return cudaGraphLaunch(gexec_, stream);
+  }
+  return e;
+}
+
+cudaError_t Plan::launch_step(const Step& s, const unsigned char* base, cudaStream_t stream) {
+  cudaError_t e = cudaSuccess;
+  {
     switch (s.kind) {
       case Step::GEMM:
         e = launch_zgemm_batched(s.opA, s.opB, reinterpret_cast<const ZGemmProblem*>(base + s.off),
@@ -345,23 +386,6 @@ cudaError_t Plan::run(cudaStream_t stream, bool use_graph) {
         e = launch_ztrtri_diag(base + s.off, s.count, s.nb, s.blocked, s.max_n, s.smem, stream);
         break;
     }
-    if (e != cudaSuccess) break;
-  }
-  if (use_graph) {
-    cudaGraph_t g = nullptr;
-    cudaError_t e2 = cudaStreamEndCapture(stream, &g);
-    if (e != cudaSuccess) {
-      if (g) cudaGraphDestroy(g);
-      return e;
-    }
-    if (e2 != cudaSuccess) return e2;
-    if (gexec_) cudaGraphExecDestroy(gexec_);
-    if (graph_) cudaGraphDestroy(graph_);
-    graph_ = g;
-    e = cudaGraphInstantiate(&gexec_, graph_, 0);
-    if (e != cudaSuccess) return e;
-    graph_stream_ = stream;
-    return cudaGraphLaunch(gexec_, stream);
   }
   return e;
 }

@@ -119,6 +119,9 @@ class Plan {
 
   cudaError_t finalize();
   cudaError_t run(cudaStream_t stream, bool use_graph);
+  // Launch-by-launch replay with a CUDA event recorded after every launch
+  // (events[0] before the first); events must hold steps.size() + 1 events.
+  cudaError_t run_events(cudaStream_t stream, const std::vector<cudaEvent_t>& events);
 
   double flops() const;
   size_t num_launches() const;
@@ -126,6 +129,7 @@ class Plan {
   std::vector<Step> steps;
 
  private:
+  cudaError_t launch_step(const Step& s, const unsigned char* base, cudaStream_t stream);
   size_t push_bytes(const void* p, size_t n);
   std::vector<unsigned char> blob_;
   void* dblob_ = nullptr;

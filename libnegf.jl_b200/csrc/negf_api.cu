@@ -128,8 +128,14 @@ struct negf_device_s {
   std::vector<cplx*> Hu;  // H_{i,i+1}
   cplx* gamL = nullptr;
   cplx* gamR = nullptr;
+  cplx* sigL = nullptr;
+  cplx* sigR = nullptr;
+  std::unique_ptr<Plan> assemble;  // Sigma / Gamma assembly launches
+  cudaStream_t stream = nullptr;
   std::vector<void*> owned;
   ~negf_device_s() {
+    assemble.reset();
+    if (stream) cudaStreamDestroy(stream);
     for (void* p : owned) cudaFree(p);
   }
 };
@@ -145,6 +151,12 @@ struct negf_solver_s {
   double* t2 = nullptr;    // 2 * nE (re, im)
   int* info = nullptr;
   size_t per_energy = 0;   // sum b_i^2
+  std::vector<std::vector<cudaEvent_t>> ev_sets;  // one event set per profiled pass
+  size_t ev_used = 0;
+  ~negf_solver_s() {
+    for (auto& v : ev_sets)
+      for (cudaEvent_t e : v) cudaEventDestroy(e);
+  }
 };
 
 namespace {
@@ -213,8 +225,13 @@ int build_solver(negf_solver_s& S) {
         h.u.push_back(plan.alloc_c((size_t)d.b[i] * d.b[i + 1]));
         h.ldu.push_back(d.b[i]);
       }
+      // every pass starts from Sigma^in: zero all diagonal and upper blocks
       for (int i = 0; i < n; ++i) {
         ZBlockOp z{}; z.C = h.d[i]; z.ldc = d.b[i]; z.m = z.n = d.b[i]; z.kind = ZOP_FILL;
+        zero.push_back(z);
+      }
+      for (int i = 0; i + 1 < n; ++i) {
+        ZBlockOp z{}; z.C = h.u[i]; z.ldc = d.b[i]; z.m = d.b[i]; z.n = d.b[i + 1]; z.kind = ZOP_FILL;
         zero.push_back(z);
       }
       ZBlockOp l{}; l.A = d.gamL; l.lda = d.b[0]; l.C = h.d[0]; l.ldc = d.b[0]; l.m = l.n = d.b[0];
@@ -533,9 +550,34 @@ int negf_device_create(int32_t npl, const int32_t* block_sizes, const void* cons
     if (!p) return fail(NEGF_ERR_NOMEM, "device allocation failed");
     d->Hu.push_back(p);
   }
-  d->gamL = dalloc((size_t)d->b[0] * d->b[0]);
-  d->gamR = dalloc((size_t)d->b[npl - 1] * d->b[npl - 1]);
-  if (!d->gamL || !d->gamR) return fail(NEGF_ERR_NOMEM, "device allocation failed");
+  const int b0 = d->b[0], bN = d->b[npl - 1];
+  d->gamL = dalloc((size_t)b0 * b0);
+  d->gamR = dalloc((size_t)bN * bN);
+  d->sigL = dalloc((size_t)b0 * b0);
+  d->sigR = dalloc((size_t)bN * bN);
+  if (!d->gamL || !d->gamR || !d->sigL || !d->sigR) return fail(NEGF_ERR_NOMEM, "device allocation failed");
+  if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(NEGF_ERR_CUDA, "stream creation failed");
+  try {
+    d->assemble.reset(new Plan);
+    auto axpy = [](const cplx* A, cplx* C, int b) {
+      ZBlockOp o{};
+      o.A = A; o.lda = b; o.C = C; o.ldc = b; o.m = o.n = b; o.kind = ZOP_AXPBY;
+      o.alpha = make_double2(1.0, 0.0); o.beta = make_double2(1.0, 0.0);
+      return o;
+    };
+    auto gam = [](const cplx* A, cplx* C, int b) {
+      ZBlockOp o{};
+      o.A = A; o.lda = b; o.C = C; o.ldc = b; o.m = o.n = b; o.kind = ZOP_GAMMA;
+      return o;
+    };
+    // two launches so that npl == 1 (both self-energies on one block) stays race-free
+    d->assemble->blockops({axpy(d->sigL, d->D[0], b0), gam(d->sigL, d->gamL, b0), gam(d->sigR, d->gamR, bN)});
+    d->assemble->blockops({axpy(d->sigR, d->D[npl - 1], bN)});
+    if (d->assemble->finalize() != cudaSuccess) return fail(NEGF_ERR_CUDA, "device assembly plan");
+  } catch (const std::bad_alloc&) {
+    return fail(NEGF_ERR_NOMEM, "device allocation failed");
+  }
   negf_device_t h = d.release();
   return negf_device_upload(h, Hd, Hu, sigL, sigR) == NEGF_SUCCESS ? (*out = h, NEGF_SUCCESS)
                                                                    : (delete h, NEGF_ERR_CUDA);
@@ -545,34 +587,20 @@ int negf_device_upload(negf_device_t d, const void* const* Hd, const void* const
                        const void* sigR) {
   if (!d) return fail(NEGF_ERR_INVALID, "NULL device");
   const int n = d->npl;
-  // host-side assembly of D_0 = H_00 + Sigma_L, D_{N-1} = H + Sigma_R and the Gammas
-  for (int i = 0; i < n; ++i) {
-    size_t cnt = (size_t)d->b[i] * d->b[i];
-    std::vector<cplx> h(cnt);
-    std::memcpy(h.data(), Hd[i], cnt * sizeof(cplx));
-    if (i == 0)
-      for (size_t k = 0; k < cnt; ++k) h[k] = cadd(h[k], static_cast<const cplx*>(sigL)[k]);
-    if (i == n - 1)
-      for (size_t k = 0; k < cnt; ++k) h[k] = cadd(h[k], static_cast<const cplx*>(sigR)[k]);
-    NEGF_TRY_CUDA(cudaMemcpy(d->D[i], h.data(), cnt * sizeof(cplx), cudaMemcpyHostToDevice), "device upload");
-  }
+  // copies straight from the caller's buffers (pinned ones go at full PCIe rate)
+  for (int i = 0; i < n; ++i)
+    NEGF_TRY_CUDA(cudaMemcpyAsync(d->D[i], Hd[i], (size_t)d->b[i] * d->b[i] * sizeof(cplx), cudaMemcpyHostToDevice,
+                                  d->stream), "device upload");
   for (int i = 0; i + 1 < n; ++i)
-    NEGF_TRY_CUDA(cudaMemcpy(d->Hu[i], Hu[i], (size_t)d->b[i] * d->b[i + 1] * sizeof(cplx), cudaMemcpyHostToDevice),
-                  "device upload");
-  auto gamma = [](const cplx* s, int b, std::vector<cplx>& g) {
-    g.resize((size_t)b * b);
-    for (int c = 0; c < b; ++c)
-      for (int r = 0; r < b; ++r) {
-        cplx a = s[r + (size_t)c * b], at = s[c + (size_t)r * b];
-        cplx diff = make_double2(a.x - at.x, a.y + at.y);  // Sigma - Sigma^H
-        g[r + (size_t)c * b] = make_double2(-diff.y, diff.x);  // i * diff
-      }
-  };
-  std::vector<cplx> g;
-  gamma(static_cast<const cplx*>(sigL), d->b[0], g);
-  NEGF_TRY_CUDA(cudaMemcpy(d->gamL, g.data(), g.size() * sizeof(cplx), cudaMemcpyHostToDevice), "device upload");
-  gamma(static_cast<const cplx*>(sigR), d->b[n - 1], g);
-  NEGF_TRY_CUDA(cudaMemcpy(d->gamR, g.data(), g.size() * sizeof(cplx), cudaMemcpyHostToDevice), "device upload");
+    NEGF_TRY_CUDA(cudaMemcpyAsync(d->Hu[i], Hu[i], (size_t)d->b[i] * d->b[i + 1] * sizeof(cplx),
+                                  cudaMemcpyHostToDevice, d->stream), "device upload");
+  NEGF_TRY_CUDA(cudaMemcpyAsync(d->sigL, sigL, (size_t)d->b[0] * d->b[0] * sizeof(cplx), cudaMemcpyHostToDevice,
+                                d->stream), "device upload");
+  NEGF_TRY_CUDA(cudaMemcpyAsync(d->sigR, sigR, (size_t)d->b[n - 1] * d->b[n - 1] * sizeof(cplx),
+                                cudaMemcpyHostToDevice, d->stream), "device upload");
+  // device-side assembly: D_0 += Sigma_L, D_{N-1} += Sigma_R, Gamma = i (Sigma - Sigma^H)
+  NEGF_TRY_CUDA(d->assemble->run(d->stream, false), "device upload");
+  NEGF_TRY_CUDA(cudaStreamSynchronize(d->stream), "device upload");
   return NEGF_SUCCESS;
 }
 
@@ -626,6 +654,59 @@ int negf_solver_run(negf_solver_t s, void* stream) {
   // the legacy NULL stream cannot be captured: replay the launches directly there
   cudaError_t e = s->plan->run(static_cast<cudaStream_t>(stream), stream != nullptr);
   if (e != cudaSuccess) return cuda_fail(e, "negf_solver_run");
+  return NEGF_SUCCESS;
+}
+
+int negf_solver_run_profiled(negf_solver_t s, void* stream) {
+  if (!s) return fail(NEGF_ERR_INVALID, "NULL solver");
+  const size_t need = s->plan->steps.size() + 1;
+  if (s->ev_used == s->ev_sets.size()) {
+    std::vector<cudaEvent_t> v(need);
+    for (auto& e : v) NEGF_TRY_CUDA(cudaEventCreate(&e), "profiled run");
+    s->ev_sets.push_back(std::move(v));
+  }
+  cudaError_t e = s->plan->run_events(static_cast<cudaStream_t>(stream), s->ev_sets[s->ev_used]);
+  if (e != cudaSuccess) return cuda_fail(e, "negf_solver_run_profiled");
+  ++s->ev_used;
+  return NEGF_SUCCESS;
+}
+
+int negf_solver_profile_read(negf_solver_t s, double* ms, double* flops, int64_t* launches, int32_t reset) {
+  if (!s) return fail(NEGF_ERR_INVALID, "NULL solver");
+  const int K = 8;
+  std::vector<double> t(K, 0.0), f(K, 0.0);
+  std::vector<int64_t> n(K, 0);
+  const auto& steps = s->plan->steps;
+  for (size_t p = 0; p < s->ev_used; ++p) {
+    const auto& ev = s->ev_sets[p];
+    NEGF_TRY_CUDA(cudaEventSynchronize(ev.back()), "profile read");
+    for (size_t i = 0; i < steps.size(); ++i) {
+      float x = 0.f;
+      NEGF_TRY_CUDA(cudaEventElapsedTime(&x, ev[i], ev[i + 1]), "profile read");
+      int k = static_cast<int>(steps[i].kind);
+      t[k] += x;
+      f[k] += steps[i].flops;
+      n[k] += 1;
+    }
+  }
+  for (int k = 0; k < K; ++k) {
+    if (ms) ms[k] = t[k];
+    if (flops) flops[k] = f[k];
+    if (launches) launches[k] = n[k];
+  }
+  if (reset) s->ev_used = 0;
+  return NEGF_SUCCESS;
+}
+
+int negf_solver_download(negf_solver_t s, void* gr_host, void* gl_host, double* t_host, void* stream) {
+  if (!s) return fail(NEGF_ERR_INVALID, "NULL solver");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t bytes = (size_t)s->nE * s->per_energy * sizeof(cplx);
+  if (gr_host && s->gr) NEGF_TRY_CUDA(cudaMemcpyAsync(gr_host, s->gr, bytes, cudaMemcpyDeviceToHost, st), "download");
+  if (gl_host && s->gl) NEGF_TRY_CUDA(cudaMemcpyAsync(gl_host, s->gl, bytes, cudaMemcpyDeviceToHost, st), "download");
+  if (t_host && s->t2)
+    NEGF_TRY_CUDA(cudaMemcpyAsync(t_host, s->t2, 2 * sizeof(double) * s->nE, cudaMemcpyDeviceToHost, st), "download");
+  NEGF_TRY_CUDA(cudaStreamSynchronize(st), "download");
   return NEGF_SUCCESS;
 }
 

@@ -94,6 +94,7 @@ enum ZOpKind : int {
   ZOP_FILL = 3,        // C = alpha (every entry)
   ZOP_IDENTITY = 4,    // C = alpha * I
   ZOP_HERM_PART = 5,   // C = (A + A^H)/2
+  ZOP_GAMMA = 6,       // C = i (A - A^H)   (broadening of a self-energy)
 };
 
 struct ZBlockOp {

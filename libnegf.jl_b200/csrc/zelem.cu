@@ -17,7 +17,7 @@ __global__ void zblockop_kernel(const ZBlockOp* __restrict__ ops) {
   const int tilesn = (o.n + EL_TILE - 1) / EL_TILE;
   for (int t = blockIdx.x; t < tilesm * tilesn; t += gridDim.x) {
     const int r0 = (t % tilesm) * EL_TILE, c0 = (t / tilesm) * EL_TILE;
-    if (o.kind == ZOP_CTRANSPOSE || o.kind == ZOP_HERM_PART) {
+    if (o.kind == ZOP_CTRANSPOSE || o.kind == ZOP_HERM_PART || o.kind == ZOP_GAMMA) {
       // A is n x m here (C = A^H is m x n); read A tile (c0.., r0..) coalesced along its rows
       for (int i = threadIdx.y; i < EL_TILE; i += blockDim.y) {
         int ar = c0 + threadIdx.x, ac = r0 + i;  // element A[ar, ac], ar < n, ac < m
@@ -31,6 +31,10 @@ __global__ void zblockop_kernel(const ZBlockOp* __restrict__ ops) {
           if (o.kind == ZOP_HERM_PART) {
             cplx a = o.A[r + (size_t)c * o.lda];
             v = make_double2(0.5 * (a.x + v.x), 0.5 * (a.y + v.y));
+          } else if (o.kind == ZOP_GAMMA) {
+            cplx a = o.A[r + (size_t)c * o.lda];
+            cplx d = make_double2(a.x - v.x, a.y - v.y);  // A - A^H
+            v = make_double2(-d.y, d.x);                  // i * d
           }
           o.C[r + (size_t)c * o.ldc] = v;
         }

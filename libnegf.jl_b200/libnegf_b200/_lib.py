@@ -82,6 +82,11 @@ PROTOTYPES = {
     "negf_solver_outputs": (ctypes.c_int, [ctypes.c_void_p, c_void_pp, c_void_pp,
                                            ctypes.POINTER(ctypes.POINTER(ctypes.c_double))]),
     "negf_solver_check": (ctypes.c_int, [ctypes.c_void_p]),
+    "negf_solver_download": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, c_double_p,
+                                            ctypes.c_void_p]),
+    "negf_solver_run_profiled": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "negf_solver_profile_read": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_double_p,
+                                                ctypes.POINTER(ctypes.c_int64), ctypes.c_int32]),
     "negf_solver_stats": (ctypes.c_int, [ctypes.c_void_p, c_double_p, ctypes.POINTER(ctypes.c_int64),
                                          ctypes.POINTER(ctypes.c_int64)]),
     "run_bndiag_wrapper": (CCscMatrix, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, c_int32_p, c_int32_p,

@@ -126,6 +126,25 @@ class Solver:
     def check(self):
         check(load().negf_solver_check(self._h))
 
+    KINDS = ["gemm", "gj_panel", "gj_unpermute", "blockop", "trace", "lu_panel", "lu_swap", "tri_diag"]
+
+    def run_profiled(self, stream=None):
+        """One pass launch by launch with a CUDA event after each launch."""
+        check(load().negf_solver_run_profiled(self._h, stream))
+
+    def profile_read(self, reset=True):
+        """Per kernel kind: (ms, flops, launches) summed over profiled passes."""
+        ms = (ctypes.c_double * 8)()
+        fl = (ctypes.c_double * 8)()
+        n = (ctypes.c_int64 * 8)()
+        check(load().negf_solver_profile_read(self._h, ms, fl, n, int(reset)))
+        return {k: (ms[i], fl[i], n[i]) for i, k in enumerate(self.KINDS)}
+
+    def download(self, gr_ptr, gl_ptr, t_ptr, stream=None):
+        """Copy the outputs into host memory at the given addresses (None: skip)."""
+        check(load().negf_solver_download(self._h, gr_ptr, gl_ptr,
+                                          ctypes.cast(t_ptr, _lib.c_double_p) if t_ptr else None, stream))
+
     def outputs(self):
         gr = ctypes.c_void_p()
         gl = ctypes.c_void_p()

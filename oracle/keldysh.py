@@ -17,10 +17,11 @@ from .blockmatrix import BlockMatrix
 from .rgf import rgf_upward
 
 
-def keldyshndiag(M, S):
-    """Returns the Hermitian BlockMatrix ``buffS`` (diag + upper blocks)."""
+def keldyshndiag(M, S, upward=None):
+    """Returns the Hermitian BlockMatrix ``buffS`` (diag + upper blocks).
+    ``upward`` reuses a precomputed (lu, R, L) of the RGF upward pass."""
     npl = M.npl
-    lu, R, L = rgf_upward(M)                                     # keldyshndiag.jl:169
+    lu, R, L = upward if upward is not None else rgf_upward(M)   # keldyshndiag.jl:169
     s = {k: v.copy() for k, v in S.M.items()}                    # :178  bm_copy!(buffS, S)
 
     # upward RKD pass (:221-235)
@@ -32,10 +33,13 @@ def keldyshndiag(M, S):
     # central pass (:237-302)
     m2 = {}
     xb = {}
-    m2[(0, 1)] = be_mldivide("N", s[(0, 1)], lu[0])              # :257
-    m2[(1, 0)] = be_ctranspose(m2[(0, 1)])                       # :258
-    xb[(1, 0)] = be_mldivide("N", m2[(1, 0)], lu[1])             # :259
-    s[(0, 1)] = be_ctranspose(xb[(1, 0)])                        # :260
+    if npl > 1:
+        # the reference rescales block (1,2) unconditionally and so needs npl >= 2;
+        # with one layer only the diagonal rescale below applies
+        m2[(0, 1)] = be_mldivide("N", s[(0, 1)], lu[0])          # :257
+        m2[(1, 0)] = be_ctranspose(m2[(0, 1)])                   # :258
+        xb[(1, 0)] = be_mldivide("N", m2[(1, 0)], lu[1])         # :259
+        s[(0, 1)] = be_ctranspose(xb[(1, 0)])                    # :260
     xb[(0, 0)] = np.eye(M.blockSizes[0], dtype=np.complex128)    # :263-268
     for ix in range(1, npl - 1):                                 # :270
         m2[(ix - 1, ix)] = be_gemm("N", "N", 1.0, xb[(ix - 1, ix - 1)], R[ix - 1], 0.0, None)    # :273

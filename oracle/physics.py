@@ -113,12 +113,14 @@ def solve_energy(sysm, E, want_keldysh=True):
     Returns dict with 'GR' (BlockMatrix), 'Gn' (Hermitian BlockMatrix, or None)
     and 'T' (float)."""
     M = sysm.M_of_E(E)
-    GR = _rgf.bndiag_of_inv_rgf_local(M)
+    # one upward pass shared by G^R, G^n and the transmission chain
+    up = _rgf.rgf_upward(M)
+    lu, R, L = up
+    GR = _rgf.bndiag_of_inv_rgf_local(M, upward=up)
     out = {"GR": GR}
     if want_keldysh:
-        out["Gn"] = _keldysh.keldyshndiag(M, sysm.sigma_in(E))
+        out["Gn"] = _keldysh.keldyshndiag(M, sysm.sigma_in(E), upward=up)
     # G^R_{1N} by the row recursion G_{1,j} = -G_{1,j-1} R_{j-1} (rgf.jl:185-199)
-    lu, R, L = _rgf.rgf_upward(M)
     g1 = GR.M[(0, 0)]
     for j in range(1, sysm.npl):
         g1 = be_gemm("N", "N", -1.0, g1, R[j - 1], 0.0, None)

@@ -33,13 +33,14 @@ def rgf_upward(M):
     return lu, R, L
 
 
-def bndiag_of_inv_rgf_local(M, build_full_inv=False):
+def bndiag_of_inv_rgf_local(M, build_full_inv=False, upward=None):
     """Block tridiagonal of M^{-1} (matinvertndiag_rgf.jl:114-200).
 
     Returns a BlockMatrix with blocks (i,i), (i,i+1), (i+1,i); with
-    ``build_full_inv`` every block of the inverse (rgf.jl:185-199)."""
+    ``build_full_inv`` every block of the inverse (rgf.jl:185-199).
+    ``upward`` reuses a precomputed (lu, R, L) of ``rgf_upward``."""
     npl = M.npl
-    lu, R, L = rgf_upward(M)
+    lu, R, L = upward if upward is not None else rgf_upward(M)
     out = BlockMatrix(M.blockSizes, {"in": 3, "out": 3}, False)
     G = out.M
     G[(0, 0)] = be_mldivide("N", be_identity(M.blockSizes[0]), lu[0])   # rgf.jl:169
