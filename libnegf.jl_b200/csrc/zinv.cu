@@ -183,8 +183,16 @@ cudaError_t launch_zgj_panel(const ZInvProblem* probs_dev, int nprob, int k0, in
 }
 
 // Raise the dynamic shared-memory limit of the panel kernel (outside capture).
+// The attribute is process-wide, so it is always set to the device's opt-in
+// maximum: a later, smaller request never lowers the limit another live plan
+// relies on.
 cudaError_t zgj_prepare(size_t smem) {
-  return cudaFuncSetAttribute(zgj_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int dev = 0, mx = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&mx, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  if (smem > (size_t)mx) return cudaErrorInvalidValue;
+  return cudaFuncSetAttribute(zgj_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
 }
 
 cudaError_t launch_zgj_unpermute(const ZInvProblem* probs_dev, int nprob, int max_n, cudaStream_t stream) {

@@ -192,12 +192,17 @@ size_t zgetrf_panel_smem_bytes(int n, int nb) {
 
 size_t ztrtri_smem_bytes(int nb) { return 2 * (size_t)nb * nb * sizeof(cplx); }
 
+// The shared-memory attributes are process-wide: set them to the device's
+// opt-in maximum so that no later plan lowers a limit another one relies on.
 cudaError_t zlu_prepare(size_t panel_smem, size_t tri_smem) {
-  cudaError_t e = cudaSuccess;
-  if (panel_smem)
-    e = cudaFuncSetAttribute(zgetrf_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel_smem);
+  int dev = 0, mx = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&mx, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  if (panel_smem > (size_t)mx || tri_smem > (size_t)mx) return cudaErrorInvalidValue;
+  if (panel_smem) e = cudaFuncSetAttribute(zgetrf_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   if (e == cudaSuccess && tri_smem)
-    e = cudaFuncSetAttribute(ztrtri_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem);
+    e = cudaFuncSetAttribute(ztrtri_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   return e;
 }
 
