@@ -79,6 +79,23 @@ int negf_zcopy_batched(char op, int32_t nprob, const int32_t* m, const int32_t* 
 int negf_zinv_batched(int32_t nprob, const int32_t* n, void* const* A, const int32_t* lda, void* const* Ainv,
                       const int32_t* ldainv, int32_t* info, void* stream);
 
+/* negf_zinv_batched without any device allocation.  This entry point has no
+ * counterpart in the reference.  It is for callers that cannot let the
+ * library call cudaMalloc / cudaFree -- applications whose device memory all
+ * comes from their own pool, or loops that cannot afford the device-wide
+ * synchronisation of cudaFree.  Inputs, outputs and results are those of
+ * negf_zinv_batched; all scratch (block copies, rank-nb update buffers,
+ * pivots, flags, launch descriptors) lives in one fixed 64 MiB __device__
+ * array that every GPU loading the library keeps until the process exits.
+ * A request whose scratch exceeds 64 MiB (about 60 blocks of 256 or 15 of 512
+ * per call) is rejected with NEGF_ERR_INVALID.  The first call on a device
+ * looks up the array's address and sets kernel attributes: make it before
+ * any stream capture.  All calls share the array, so calls that overlap on
+ * the GPU (different streams or threads on one device) race; calls in
+ * sequence on one stream are safe. */
+int negf_zinv_batched_noalloc(int32_t nprob, const int32_t* n, void* const* A, const int32_t* lda,
+                              void* const* Ainv, const int32_t* ldainv, int32_t* info, void* stream);
+
 /* Batched LU with partial pivoting, in place, LAPACK getrf semantics;
  * replaces be_lu! / be_getrf! (src/backend_cpu.jl:147-169, :255-265).
  * ipiv (dptrs, may be NULL entries) receives 1-based LAPACK pivots. */

@@ -50,6 +50,8 @@ PROTOTYPES = {
                                           c_void_pp, c_int32_p, ctypes.c_void_p]),
     "negf_zinv_batched": (ctypes.c_int, [ctypes.c_int32, c_int32_p, c_void_pp, c_int32_p, c_void_pp, c_int32_p,
                                          c_int32_p, ctypes.c_void_p]),
+    "negf_zinv_batched_noalloc": (ctypes.c_int, [ctypes.c_int32, c_int32_p, c_void_pp, c_int32_p, c_void_pp,
+                                                 c_int32_p, c_int32_p, ctypes.c_void_p]),
     "negf_zgetrf_batched": (ctypes.c_int, [ctypes.c_int32, c_int32_p, c_void_pp, c_int32_p, c_void_pp, c_int32_p,
                                            ctypes.c_void_p]),
     "negf_ztrsm_batched": (ctypes.c_int, [ctypes.c_char, ctypes.c_char, ctypes.c_char, ctypes.c_char, c_double_p,
