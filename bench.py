@@ -57,6 +57,23 @@ def parse():
     return ap.parse_args()
 
 
+def shard_energies(ne_per_rank, world, rank, lo=-1.0, hi=1.0):
+    """Weak scaling: the global grid has ne_per_rank * world energies uniform in
+    [lo, hi]; rank r solves the contiguous slice r.  No energy is shared."""
+    grid = np.linspace(lo, hi, ne_per_rank * world)
+    return grid[rank * ne_per_rank:(rank + 1) * ne_per_rank]
+
+
+def max_over_ranks(value, dist=None, device=None):
+    """Max of a float over all ranks (the job time is the slowest rank's)."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def canonical_flops(npl, b):
     """Algorithmic real flops per energy point: the reference's call sequence
     for RKD plus the G^R downward pass sharing its upward pass, and the
@@ -141,9 +158,11 @@ def _cpu_solve_one(args):
 
 
 def cpu_baseline(npl, b, energies, budget_s, seed=0):
-    """Best of (i) one energy at a time with all BLAS threads and (ii) one
-    energy per core with one BLAS thread each (the reference's threading
-    models).  Each mode runs a bounded sample."""
+    """Best of (i) one energy at a time with all BLAS threads (the reference's
+    RGF/RKD benchmarks: one Julia thread, k BLAS threads,
+    benchmrk/runbenchmrks.sh:44-47) and (ii) one energy per core with one BLAS
+    thread each (its DDRGF model: Julia threads x 1 BLAS thread).  Each mode
+    runs a bounded sample."""
     import multiprocessing as mp
     from threadpoolctl import threadpool_limits
     from oracle import physics
@@ -227,8 +246,7 @@ def run_ours(args):
     negf.load()
     # CPU baseline first (spawned pool, before heavy GPU work)
     cpu = None
-    energies_all = np.linspace(-1.0, 1.0, args.ne * world)
-    my_E = energies_all[rank * args.ne:(rank + 1) * args.ne]
+    my_E = shard_energies(args.ne, world, rank)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.npl, args.b, my_E, args.cpu_budget_s)
 
@@ -268,10 +286,7 @@ def run_ours(args):
     ms = ev0.elapsed_time(ev1)
     prof = solver.profile_read(reset=True)
     solver.check()
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist if world > 1 else None, "cuda")
     total_pts = args.ne * args.steps * world
     value = total_pts / (ms / 1000.0)
 
@@ -325,11 +340,7 @@ def run_ours(args):
         t0 = time.perf_counter()
         for _ in range(args.steps):
             e2e_step()
-        el = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([el], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
+        el = max_over_ranks(time.perf_counter() - t0, dist if world > 1 else None, "cuda")
         h2d = sum(h.nbytes for h in sysm.Hd) + sum(h.nbytes for h in sysm.Hu) + 2 * sysm.sigL.nbytes + my_E.nbytes
         e2e = {"value": total_pts / el, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(2 * nbytes + 16 * args.ne), "ms_per_step": 1000 * el / args.steps}

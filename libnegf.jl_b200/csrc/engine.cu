@@ -81,6 +81,7 @@ void Plan::gemm(char opA, char opB, const std::vector<ZGemmProblem>& probs) {
   std::vector<int> starts;
   int total = 0;
   double fl = 0.0;
+  bool pre = true;
   for (const auto& p : probs) {
     int t = zgemm_tiles(p.m, p.n);
     if (t == 0) continue;
@@ -88,12 +89,14 @@ void Plan::gemm(char opA, char opB, const std::vector<ZGemmProblem>& probs) {
     starts.push_back(total);
     total += t;
     fl += 8.0 * p.m * (double)p.n * p.k;
+    pre = pre && zgemm_preload_ok(p);
   }
   if (v.empty()) return;
   Step s;
   s.kind = Step::GEMM;
   s.opA = opA;
   s.opB = opB;
+  s.preload = pre;
   s.off = push_bytes(v.data(), v.size() * sizeof(ZGemmProblem));
   s.tiles_off = push_bytes(starts.data(), starts.size() * sizeof(int));
   s.count = static_cast<int>(v.size());
@@ -360,8 +363,8 @@ cudaError_t Plan::launch_step(const Step& s, const unsigned char* base, cudaStre
   {
     switch (s.kind) {
       case Step::GEMM:
-        e = launch_zgemm_batched(s.opA, s.opB, reinterpret_cast<const ZGemmProblem*>(base + s.off),
-                                 reinterpret_cast<const int*>(base + s.tiles_off), s.count, s.total_tiles, stream);
+        e = launch_zgemm_batched_ex(s.opA, s.opB, s.preload, reinterpret_cast<const ZGemmProblem*>(base + s.off),
+                                    reinterpret_cast<const int*>(base + s.tiles_off), s.count, s.total_tiles, stream);
         break;
       case Step::GJ_PANEL:
         e = launch_zgj_panel(reinterpret_cast<const ZInvProblem*>(base + s.off), s.count, s.k0, s.nb, s.blocked,

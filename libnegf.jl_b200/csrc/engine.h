@@ -20,6 +20,9 @@ namespace negf {
 // launchers (zgemm.cu, zinv.cu, zelem.cu)
 cudaError_t launch_zgemm_batched(char opA, char opB, const ZGemmProblem* probs_dev, const int* tile_start_dev,
                                  int nprob, int total_tiles, cudaStream_t stream);
+cudaError_t launch_zgemm_batched_ex(char opA, char opB, bool preload, const ZGemmProblem* probs_dev,
+                                    const int* tile_start_dev, int nprob, int total_tiles, cudaStream_t stream);
+bool zgemm_preload_ok(const ZGemmProblem& p);
 int zgemm_tiles(int m, int n);
 size_t zgemm_smem_bytes();
 cudaError_t zgemm_prepare(char opA, char opB);
@@ -95,6 +98,7 @@ struct Step {
   size_t tiles_off = 0;  // tile prefix-sum offset (GEMM)
   int count = 0, total_tiles = 0, max_m = 0, max_n = 0;
   int k0 = 0, nb = 0, blocked = 0;
+  bool preload = false;  // GEMM: accumulators start from Cin (all problems alpha, beta = +-1)
   size_t smem = 0;
   double flops = 0.0;    // real flops of the step (8mnk per complex GEMM)
 };

@@ -83,7 +83,7 @@ __device__ __forceinline__ void load_stage(cplx* As, cplx* Bs, const ZGemmProble
   }
 }
 
-template <bool TA, bool CA, bool TB, bool CB>
+template <bool TA, bool CA, bool TB, bool CB, bool PRE>
 __global__ void __launch_bounds__(gemm::THREADS, 2)
     zgemm_batched_kernel(const ZGemmProblem* __restrict__ probs, const int* __restrict__ tile_start, int nprob) {
   using namespace gemm;
@@ -108,13 +108,33 @@ __global__ void __launch_bounds__(gemm::THREADS, 2)
   int g = lane >> 2, tq = lane & 3;
   int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
 
+  // PRE (chosen per launch by the host when every problem has alpha, beta in
+  // {1, -1} and a Cin): in-place updates C = +-A*B +- C, i.e. every Schur
+  // update of the sweeps, start the accumulators from Cin, so the loads are
+  // issued before the main loop and overlap the first operand copies instead
+  // of stalling the epilogue.
+  const bool preload = PRE && p.k > 0 && p.Cin != nullptr;
+  const double pre_sign = p.alpha.x * p.beta.x;  // beta / alpha for alpha, beta in {1, -1}
+
   double acc_re[2][4][4], acc_im[2][4][4];
 #pragma unroll
   for (int a = 0; a < 2; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b)
 #pragma unroll
-      for (int c = 0; c < 4; ++c) { acc_re[a][b][c] = 0.0; acc_im[a][b][c] = 0.0; }
+      for (int c = 0; c < 4; ++c) {
+        acc_re[a][b][c] = 0.0;
+        acc_im[a][b][c] = 0.0;
+        if (preload) {
+          int r = m0 + wm + a * 16 + g + ((c >> 1) << 3);
+          int cc = n0 + wn + b * 8 + 2 * tq + (c & 1);
+          if (r < p.m && cc < p.n) {
+            cplx v = p.Cin[r + (size_t)cc * p.ldcin];
+            acc_re[a][b][c] = pre_sign * v.x;
+            acc_im[a][b][c] = pre_sign * v.y;
+          }
+        }
+      }
 
   int nk = (p.k + BK - 1) / BK;
   // prologue
@@ -171,7 +191,7 @@ __global__ void __launch_bounds__(gemm::THREADS, 2)
 
   // epilogue
   const bool has_ab = p.k > 0;
-  const bool has_cin = (p.beta.x != 0.0 || p.beta.y != 0.0) && p.Cin != nullptr;
+  const bool has_cin = (p.beta.x != 0.0 || p.beta.y != 0.0) && p.Cin != nullptr && !preload;
   const cplx dg = p.diag_ptr ? *p.diag_ptr : p.diag;
 #pragma unroll
   for (int mi = 0; mi < 2; ++mi)
@@ -201,38 +221,61 @@ __global__ void __launch_bounds__(gemm::THREADS, 2)
 
 using ZGemmKernel = void (*)(const ZGemmProblem*, const int*, int);
 
-static ZGemmKernel pick_kernel(char opA, char opB) {
+template <bool PRE>
+static ZGemmKernel pick_kernel_t(int ia, int ib) {
+  switch (ia * 3 + ib) {
+    case 0: return zgemm_batched_kernel<false, false, false, false, PRE>;
+    case 1: return zgemm_batched_kernel<false, false, true, false, PRE>;
+    case 2: return zgemm_batched_kernel<false, false, true, true, PRE>;
+    case 3: return zgemm_batched_kernel<true, false, false, false, PRE>;
+    case 4: return zgemm_batched_kernel<true, false, true, false, PRE>;
+    case 5: return zgemm_batched_kernel<true, false, true, true, PRE>;
+    case 6: return zgemm_batched_kernel<true, true, false, false, PRE>;
+    case 7: return zgemm_batched_kernel<true, true, true, false, PRE>;
+    default: return zgemm_batched_kernel<true, true, true, true, PRE>;
+  }
+}
+
+static ZGemmKernel pick_kernel(char opA, char opB, bool pre) {
   int ia = opA == 'N' ? 0 : (opA == 'T' ? 1 : 2);
   int ib = opB == 'N' ? 0 : (opB == 'T' ? 1 : 2);
-  switch (ia * 3 + ib) {
-    case 0: return zgemm_batched_kernel<false, false, false, false>;
-    case 1: return zgemm_batched_kernel<false, false, true, false>;
-    case 2: return zgemm_batched_kernel<false, false, true, true>;
-    case 3: return zgemm_batched_kernel<true, false, false, false>;
-    case 4: return zgemm_batched_kernel<true, false, true, false>;
-    case 5: return zgemm_batched_kernel<true, false, true, true>;
-    case 6: return zgemm_batched_kernel<true, true, false, false>;
-    case 7: return zgemm_batched_kernel<true, true, true, false>;
-    default: return zgemm_batched_kernel<true, true, true, true>;
-  }
+  return pre ? pick_kernel_t<true>(ia, ib) : pick_kernel_t<false>(ia, ib);
 }
 
 size_t zgemm_smem_bytes() { return gemm::SMEM_BYTES; }
 
-// Raise the dynamic shared-memory limit of one op variant on the current
-// device; done when a plan is finalised, outside any stream capture.
+// Raise the dynamic shared-memory limit of one op variant (both accumulator
+// initialisations) on the current device; done when a plan is finalised,
+// outside any stream capture.
 cudaError_t zgemm_prepare(char opA, char opB) {
-  return cudaFuncSetAttribute(pick_kernel(opA, opB), cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(pick_kernel(opA, opB, false), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)gemm::SMEM_BYTES);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(pick_kernel(opA, opB, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)gemm::SMEM_BYTES);
 }
 
-// Host launcher.  probs_dev / tile_start_dev are device arrays prepared by the
-// caller (tile_start has nprob entries, exclusive prefix sum of tile counts).
+// True when the problem qualifies for the accumulator preload variant.
+bool zgemm_preload_ok(const ZGemmProblem& p) {
+  return p.k > 0 && p.Cin != nullptr && p.alpha.y == 0.0 && p.beta.y == 0.0 &&
+         (p.alpha.x == 1.0 || p.alpha.x == -1.0) && (p.beta.x == 1.0 || p.beta.x == -1.0);
+}
+
+// Host launchers.  probs_dev / tile_start_dev are device arrays prepared by
+// the caller (tile_start has nprob entries, exclusive prefix sum of tile
+// counts).  preload may only be set when zgemm_preload_ok holds for every
+// problem of the launch.
+cudaError_t launch_zgemm_batched_ex(char opA, char opB, bool preload, const ZGemmProblem* probs_dev,
+                                    const int* tile_start_dev, int nprob, int total_tiles, cudaStream_t stream) {
+  if (nprob <= 0 || total_tiles <= 0) return cudaSuccess;
+  pick_kernel(opA, opB, preload)<<<total_tiles, gemm::THREADS, gemm::SMEM_BYTES, stream>>>(probs_dev, tile_start_dev,
+                                                                                            nprob);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_zgemm_batched(char opA, char opB, const ZGemmProblem* probs_dev, const int* tile_start_dev,
                                  int nprob, int total_tiles, cudaStream_t stream) {
-  if (nprob <= 0 || total_tiles <= 0) return cudaSuccess;
-  pick_kernel(opA, opB)<<<total_tiles, gemm::THREADS, gemm::SMEM_BYTES, stream>>>(probs_dev, tile_start_dev, nprob);
-  return cudaGetLastError();
+  return launch_zgemm_batched_ex(opA, opB, false, probs_dev, tile_start_dev, nprob, total_tiles, stream);
 }
 
 int zgemm_tiles(int m, int n) {

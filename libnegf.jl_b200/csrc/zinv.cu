@@ -46,71 +46,66 @@ __global__ void __launch_bounds__(GJ_THREADS)
   const int k0 = args.k0;
   if (n <= 0 || k0 >= n) return;
   const int w = min(args.nb, n - k0);
+  constexpr int NW = GJ_THREADS / 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx* S = reinterpret_cast<cplx*>(smem_raw);  // n x w, column-major
   cplx* colbuf = S + (size_t)n * w;               // n
   cplx* rowbuf = colbuf + n;                       // w
-  double* redv = reinterpret_cast<double*>(rowbuf + w);  // GJ_THREADS/32
-  int* redr = reinterpret_cast<int*>(redv + GJ_THREADS / 32);
-  int* sh_piv = redr + GJ_THREADS / 32;            // w
+  double* redv = reinterpret_cast<double*>(rowbuf + w);  // NW (pivot value of the column, as complex below)
+  int* redr = reinterpret_cast<int*>(redv + NW);   // NW
+  int* sh_piv = redr + NW;                          // w
   uint8_t* used = reinterpret_cast<uint8_t*>(sh_piv + w);  // n
+  cplx* sh_pv = reinterpret_cast<cplx*>(redv);      // reuses redv[0..1]: the scaled pivot inverse
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int idx = tid; idx < n * w; idx += GJ_THREADS) {
-    int c = idx / n, r = idx - c * n;
-    S[idx] = p.W[r + (size_t)(k0 + c) * p.ld];
-  }
+  // column-per-warp, row-per-lane loops (no integer division)
+  for (int j = warp; j < w; j += NW)
+    for (int r = lane; r < n; r += 32) S[(size_t)j * n + r] = p.W[r + (size_t)(k0 + j) * p.ld];
   for (int r = tid; r < n; r += GJ_THREADS) used[r] = (k0 == 0) ? 0 : p.used[r];
   __syncthreads();
 
   for (int c = 0; c < w; ++c) {
-    // pivot search over unused rows
-    double bv = -1.0;
-    int br = -1;
-    for (int r = tid; r < n; r += GJ_THREADS)
-      if (!used[r]) argmax_merge(bv, br, cabs1(S[(size_t)c * n + r]), r);
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      double v2 = __shfl_down_sync(0xffffffffu, bv, off);
-      int r2 = __shfl_down_sync(0xffffffffu, br, off);
-      argmax_merge(bv, br, v2, r2);
-    }
-    if (lane == 0) { redv[warp] = bv; redr[warp] = br; }
-    __syncthreads();
     if (warp == 0) {
-      bv = lane < GJ_THREADS / 32 ? redv[lane] : -1.0;
-      br = lane < GJ_THREADS / 32 ? redr[lane] : -1;
+      // pivot search over unused rows, then stage column c and the scaled pivot row
+      double bv = -1.0;
+      int br = -1;
+      for (int r = lane; r < n; r += 32)
+        if (!used[r]) argmax_merge(bv, br, cabs1(S[(size_t)c * n + r]), r);
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) {
-        double v2 = __shfl_down_sync(0xffffffffu, bv, off);
-        int r2 = __shfl_down_sync(0xffffffffu, br, off);
+        double v2 = __shfl_xor_sync(0xffffffffu, bv, off);
+        int r2 = __shfl_xor_sync(0xffffffffu, br, off);
         argmax_merge(bv, br, v2, r2);
       }
+      const int pr = br;  // identical in every lane after the xor reduction
       if (lane == 0) {
-        sh_piv[c] = br;
-        if (br < 0 || bv == 0.0) {
+        sh_piv[c] = pr;
+        if (pr < 0 || bv == 0.0) {
           if (p.info) atomicCAS(p.info, 0, k0 + c + 1);
         }
+        if (pr >= 0) used[pr] = 1;
+      }
+      if (pr >= 0) {
+        cplx pivv = S[(size_t)c * n + pr];
+        cplx pv = (pivv.x == 0.0 && pivv.y == 0.0) ? make_double2(0.0, 0.0) : cinv(pivv);
+        for (int r = lane; r < n; r += 32) colbuf[r] = S[(size_t)c * n + r];
+        for (int j = lane; j < w; j += 32) rowbuf[j] = (j == c) ? pv : cmul(S[(size_t)j * n + pr], pv);
+        if (lane == 0) *sh_pv = pv;
       }
     }
     __syncthreads();
     const int pr = sh_piv[c];
     if (pr < 0) break;  // no candidate row: the host reports the info code
-    cplx pivv = S[(size_t)c * n + pr];
-    cplx pv = (pivv.x == 0.0 && pivv.y == 0.0) ? make_double2(0.0, 0.0) : cinv(pivv);
-    // stage column c and the scaled pivot row
-    for (int r = tid; r < n; r += GJ_THREADS) colbuf[r] = S[(size_t)c * n + r];
-    for (int j = tid; j < w; j += GJ_THREADS) rowbuf[j] = (j == c) ? pv : cmul(S[(size_t)j * n + pr], pv);
-    __syncthreads();
-    for (int idx = tid; idx < n * w; idx += GJ_THREADS) {
-      int j = idx / n, r = idx - j * n;
-      cplx v;
-      if (r == pr) v = rowbuf[j];
-      else if (j == c) v = cneg(cmul(colbuf[r], pv));
-      else v = cfms(S[idx], colbuf[r], rowbuf[j]);
-      S[idx] = v;
+    const cplx pv = *sh_pv;
+    for (int j = warp; j < w; j += NW) {
+      const cplx rj = rowbuf[j];
+      cplx* Sj = S + (size_t)j * n;
+      if (j == c) {
+        for (int r = lane; r < n; r += 32) Sj[r] = (r == pr) ? rj : cneg(cmul(colbuf[r], pv));
+      } else {
+        for (int r = lane; r < n; r += 32) Sj[r] = (r == pr) ? rj : cfms(Sj[r], colbuf[r], rj);
+      }
     }
-    if (tid == 0) used[pr] = 1;
     __syncthreads();
   }
 
@@ -120,35 +115,35 @@ __global__ void __launch_bounds__(GJ_THREADS)
     bool ok = true;
     for (int c = 0; c < w; ++c) ok = ok && sh_piv[c] >= 0;
     if (!ok) return;  // singular: info is set, out is left untouched
-    for (int idx = tid; idx < n * n; idx += GJ_THREADS) {
-      int c = idx / n, r = idx - c * n;
-      p.out[r + (size_t)sh_piv[c] * p.ldo] = S[(size_t)c * n + sh_piv[r]];
+    for (int c = warp; c < n; c += NW) {
+      cplx* o = p.out + (size_t)sh_piv[c] * p.ldo;
+      const cplx* Sc = S + (size_t)c * n;
+      for (int r = lane; r < n; r += 32) o[r] = Sc[sh_piv[r]];
     }
     return;
   }
   // write back slab, pivots and used flags
-  for (int idx = tid; idx < n * w; idx += GJ_THREADS) {
-    int c = idx / n, r = idx - c * n;
-    p.W[r + (size_t)(k0 + c) * p.ld] = S[idx];
-  }
+  for (int j = warp; j < w; j += NW)
+    for (int r = lane; r < n; r += 32) p.W[r + (size_t)(k0 + j) * p.ld] = S[(size_t)j * n + r];
   for (int c = tid; c < w; c += GJ_THREADS) p.piv[k0 + c] = sh_piv[c];
-  {
-    for (int r = tid; r < n; r += GJ_THREADS) p.used[r] = used[r];
-    // F = slab - E_P  (n x w, ld n)
-    for (int idx = tid; idx < n * w; idx += GJ_THREADS) {
-      int c = idx / n, r = idx - c * n;
-      cplx v = S[idx];
-      if (r == sh_piv[c]) v.x -= 1.0;
-      p.F[idx] = v;
+  for (int r = tid; r < n; r += GJ_THREADS) p.used[r] = used[r];
+  // F = slab - E_P  (n x w, ld n)
+  for (int j = warp; j < w; j += NW) {
+    const int pj = sh_piv[j];
+    for (int r = lane; r < n; r += 32) {
+      cplx v = S[(size_t)j * n + r];
+      if (r == pj) v.x -= 1.0;
+      p.F[r + (size_t)j * n] = v;
     }
-    // Bbuf = W[P, :] with panel columns zeroed  (w x n, ld w); the non-panel
-    // columns of W are not modified by this kernel, so these are old values
-    for (int idx = tid; idx < n * w; idx += GJ_THREADS) {
-      int j = idx / w, c = idx - j * w;
-      int pr = sh_piv[c];
+  }
+  // Bbuf = W[P, :] with panel columns zeroed  (w x n, ld w); the non-panel
+  // columns of W are not modified by this kernel, so these are old values
+  for (int j = warp; j < n; j += NW) {
+    const bool inK = (j >= k0 && j < k0 + w);
+    for (int c = lane; c < w; c += 32) {
       cplx v = make_double2(0.0, 0.0);
-      if ((j < k0 || j >= k0 + w) && pr >= 0) v = p.W[pr + (size_t)j * p.ld];
-      p.Bbuf[idx] = v;
+      if (!inK) v = p.W[sh_piv[c] + (size_t)j * p.ld];
+      p.Bbuf[c + (size_t)j * w] = v;
     }
   }
 }
