@@ -19,6 +19,8 @@
 //  * epilogue: C = alpha*acc + beta*Cin + diag*I, bounds-checked.
 #include "negf_common.cuh"
 
+#include <cstdlib>
+
 namespace negf {
 
 namespace gemm {
@@ -219,27 +221,178 @@ __global__ void __launch_bounds__(gemm::THREADS, 2)
       }
 }
 
-using ZGemmKernel = void (*)(const ZGemmProblem*, const int*, int);
-
-template <bool PRE>
-static ZGemmKernel pick_kernel_t(int ia, int ib) {
-  switch (ia * 3 + ib) {
-    case 0: return zgemm_batched_kernel<false, false, false, false, PRE>;
-    case 1: return zgemm_batched_kernel<false, false, true, false, PRE>;
-    case 2: return zgemm_batched_kernel<false, false, true, true, PRE>;
-    case 3: return zgemm_batched_kernel<true, false, false, false, PRE>;
-    case 4: return zgemm_batched_kernel<true, false, true, false, PRE>;
-    case 5: return zgemm_batched_kernel<true, false, true, true, PRE>;
-    case 6: return zgemm_batched_kernel<true, true, false, false, PRE>;
-    case 7: return zgemm_batched_kernel<true, true, true, false, PRE>;
-    default: return zgemm_batched_kernel<true, true, true, true, PRE>;
-  }
+// ---------------------------------------------------------------------------
+// 3M variant (Gauss's complex product): three real DMMA products per complex
+// product instead of four,
+//   P1 = Ar Br,  P2 = Ai Bi,  P3 = (Ar + Ai)(Br + Bi),
+//   Re C = P1 - P2,  Im C = P3 - P1 - P2,
+// the scheme of zgemm3m (normwise stable; the imaginary part carries an
+// absolute error of a few ulps of |A||B| instead of |Im C|).  Same 64x64
+// tile and staging as the 4M kernel; 8 warps of 32x16 so that the three
+// accumulator sets fit the register file.
+namespace gemm3m {
+constexpr int THREADS = 256;
 }
 
-static ZGemmKernel pick_kernel(char opA, char opB, bool pre) {
+template <bool TA, bool CA, bool TB, bool CB, bool PRE>
+__global__ void __launch_bounds__(gemm3m::THREADS, 1)
+    zgemm3m_batched_kernel(const ZGemmProblem* __restrict__ probs, const int* __restrict__ tile_start, int nprob) {
+  using namespace gemm;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx* smem = reinterpret_cast<cplx*>(smem_raw);
+  int bid = blockIdx.x;
+  int lo = 0, hi = nprob - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (tile_start[mid] <= bid) lo = mid; else hi = mid - 1;
+  }
+  const ZGemmProblem p = probs[lo];
+  const int t = bid - tile_start[lo];
+  const int tiles_m = (p.m + BM - 1) / BM;
+  const int m0 = (t % tiles_m) * BM;
+  const int n0 = (t / tiles_m) * BN;
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, tq = lane & 3;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
+
+  const bool preload = PRE && p.k > 0 && p.Cin != nullptr;
+  const double pre_sign = p.alpha.x * p.beta.x;
+  double P1[2][2][4], P2[2][2][4], P3[2][2][4];
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        P1[a][b][c] = 0.0; P2[a][b][c] = 0.0; P3[a][b][c] = 0.0;
+        if (preload) {
+          // Re = P1 - P2 = s Cr,  Im = P3 - P1 - P2 = s Ci
+          int r = m0 + wm + a * 16 + g + ((c >> 1) << 3);
+          int cc = n0 + wn + b * 8 + 2 * tq + (c & 1);
+          if (r < p.m && cc < p.n) {
+            cplx v = p.Cin[r + (size_t)cc * p.ldcin];
+            P1[a][b][c] = pre_sign * v.x;
+            P3[a][b][c] = pre_sign * v.x + pre_sign * v.y;
+          }
+        }
+      }
+
+  const int nk = (p.k + BK - 1) / BK;
+  // the loader is written for 128 threads: the first four warps stage each slab
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < nk && tid < THREADS)
+      load_stage<TA, TB>(smem + s * STAGE_SIZE, smem + s * STAGE_SIZE + AS_SIZE, p, m0, n0, s * BK, tid);
+    cp_async_commit();
+  }
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    int kn = kt + STAGES - 1;
+    if (kn < nk && tid < THREADS) {
+      int s = kn % STAGES;
+      load_stage<TA, TB>(smem + s * STAGE_SIZE, smem + s * STAGE_SIZE + AS_SIZE, p, m0, n0, kn * BK, tid);
+    }
+    cp_async_commit();
+    const cplx* As = smem + (kt % STAGES) * STAGE_SIZE;
+    const cplx* Bs = As + AS_SIZE;
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 4) {
+      double ar[2][2], ai[2][2], as[2][2], br[2], bi[2], bs[2];
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi) {
+        cplx x0 = As[(kk + tq) * AS_LD + wm + mi * 16 + g];
+        cplx x1 = As[(kk + tq) * AS_LD + wm + mi * 16 + g + 8];
+        ar[mi][0] = x0.x; ai[mi][0] = CA ? -x0.y : x0.y; as[mi][0] = ar[mi][0] + ai[mi][0];
+        ar[mi][1] = x1.x; ai[mi][1] = CA ? -x1.y : x1.y; as[mi][1] = ar[mi][1] + ai[mi][1];
+      }
+#pragma unroll
+      for (int ni = 0; ni < 2; ++ni) {
+        cplx y = Bs[(wn + ni * 8 + g) * BS_LD + kk + tq];
+        br[ni] = y.x;
+        bi[ni] = CB ? -y.y : y.y;
+        bs[ni] = br[ni] + bi[ni];
+      }
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 2; ++ni) {
+          double* p1 = P1[mi][ni];
+          double* p2 = P2[mi][ni];
+          double* p3 = P3[mi][ni];
+          dmma16x8x4(p1[0], p1[1], p1[2], p1[3], ar[mi][0], ar[mi][1], br[ni]);
+          dmma16x8x4(p2[0], p2[1], p2[2], p2[3], ai[mi][0], ai[mi][1], bi[ni]);
+          dmma16x8x4(p3[0], p3[1], p3[2], p3[3], as[mi][0], as[mi][1], bs[ni]);
+        }
+    }
+  }
+  cp_async_wait<0>();
+
+  const bool has_ab = p.k > 0;
+  const bool has_cin = (p.beta.x != 0.0 || p.beta.y != 0.0) && p.Cin != nullptr && !preload;
+  const cplx dg = p.diag_ptr ? *p.diag_ptr : p.diag;
+#pragma unroll
+  for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        int r = m0 + wm + mi * 16 + g + ((e >> 1) << 3);
+        int c = n0 + wn + ni * 8 + 2 * tq + (e & 1);
+        if (r < p.m && c < p.n) {
+          cplx v = make_double2(0.0, 0.0);
+          if (has_ab) {
+            double xr = P1[mi][ni][e] - P2[mi][ni][e];
+            double xi = P3[mi][ni][e] - P1[mi][ni][e] - P2[mi][ni][e];
+            v.x = p.alpha.x * xr - p.alpha.y * xi;
+            v.y = p.alpha.x * xi + p.alpha.y * xr;
+          }
+          if (has_cin) {
+            cplx ci = p.Cin[r + (size_t)c * p.ldcin];
+            v.x += p.beta.x * ci.x - p.beta.y * ci.y;
+            v.y += p.beta.x * ci.y + p.beta.y * ci.x;
+          }
+          if (r == c) { v.x += dg.x; v.y += dg.y; }
+          p.C[r + (size_t)c * p.ldc] = v;
+        }
+      }
+}
+
+using ZGemmKernel = void (*)(const ZGemmProblem*, const int*, int);
+
+template <bool PRE, bool G3M>
+static ZGemmKernel pick_kernel_t(int ia, int ib) {
+#define NEGF_K(TA, CA, TB, CB) \
+  (G3M ? zgemm3m_batched_kernel<TA, CA, TB, CB, PRE> : zgemm_batched_kernel<TA, CA, TB, CB, PRE>)
+  switch (ia * 3 + ib) {
+    case 0: return NEGF_K(false, false, false, false);
+    case 1: return NEGF_K(false, false, true, false);
+    case 2: return NEGF_K(false, false, true, true);
+    case 3: return NEGF_K(true, false, false, false);
+    case 4: return NEGF_K(true, false, true, false);
+    case 5: return NEGF_K(true, false, true, true);
+    case 6: return NEGF_K(true, true, false, false);
+    case 7: return NEGF_K(true, true, true, false);
+    default: return NEGF_K(true, true, true, true);
+  }
+#undef NEGF_K
+}
+
+// The 3M kernel is the default; NEGF_ZGEMM=4m selects the four-product kernel.
+static bool use_3m() {
+  static const bool v = [] {
+    const char* e = std::getenv("NEGF_ZGEMM");
+    return !(e && (e[0] == '4'));
+  }();
+  return v;
+}
+
+static ZGemmKernel pick_kernel(char opA, char opB, bool pre, bool g3m) {
   int ia = opA == 'N' ? 0 : (opA == 'T' ? 1 : 2);
   int ib = opB == 'N' ? 0 : (opB == 'T' ? 1 : 2);
-  return pre ? pick_kernel_t<true>(ia, ib) : pick_kernel_t<false>(ia, ib);
+  if (g3m) return pre ? pick_kernel_t<true, true>(ia, ib) : pick_kernel_t<false, true>(ia, ib);
+  return pre ? pick_kernel_t<true, false>(ia, ib) : pick_kernel_t<false, false>(ia, ib);
 }
 
 size_t zgemm_smem_bytes() { return gemm::SMEM_BYTES; }
@@ -248,11 +401,12 @@ size_t zgemm_smem_bytes() { return gemm::SMEM_BYTES; }
 // initialisations) on the current device; done when a plan is finalised,
 // outside any stream capture.
 cudaError_t zgemm_prepare(char opA, char opB) {
-  cudaError_t e = cudaFuncSetAttribute(pick_kernel(opA, opB, false), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)gemm::SMEM_BYTES);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(pick_kernel(opA, opB, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)gemm::SMEM_BYTES);
+  for (int v = 0; v < 4; ++v) {
+    cudaError_t e = cudaFuncSetAttribute(pick_kernel(opA, opB, v & 1, v & 2), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)gemm::SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 // True when the problem qualifies for the accumulator preload variant.
@@ -268,14 +422,19 @@ bool zgemm_preload_ok(const ZGemmProblem& p) {
 cudaError_t launch_zgemm_batched_ex(char opA, char opB, bool preload, const ZGemmProblem* probs_dev,
                                     const int* tile_start_dev, int nprob, int total_tiles, cudaStream_t stream) {
   if (nprob <= 0 || total_tiles <= 0) return cudaSuccess;
-  pick_kernel(opA, opB, preload)<<<total_tiles, gemm::THREADS, gemm::SMEM_BYTES, stream>>>(probs_dev, tile_start_dev,
-                                                                                            nprob);
+  const bool g3m = use_3m();
+  pick_kernel(opA, opB, preload, g3m)<<<total_tiles, g3m ? gemm3m::THREADS : gemm::THREADS, gemm::SMEM_BYTES,
+                                        stream>>>(probs_dev, tile_start_dev, nprob);
   return cudaGetLastError();
 }
 
+// The four-product kernel without accumulator preload.
 cudaError_t launch_zgemm_batched(char opA, char opB, const ZGemmProblem* probs_dev, const int* tile_start_dev,
                                  int nprob, int total_tiles, cudaStream_t stream) {
-  return launch_zgemm_batched_ex(opA, opB, false, probs_dev, tile_start_dev, nprob, total_tiles, stream);
+  if (nprob <= 0 || total_tiles <= 0) return cudaSuccess;
+  pick_kernel(opA, opB, false, false)<<<total_tiles, gemm::THREADS, gemm::SMEM_BYTES, stream>>>(
+      probs_dev, tile_start_dev, nprob);
+  return cudaGetLastError();
 }
 
 int zgemm_tiles(int m, int n) {
