@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--cpu-budget-s", type=float, default=12.0, help="time budget of each CPU baseline mode")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
     return ap.parse_args()
 
 
@@ -62,6 +63,18 @@ def shard_energies(ne_per_rank, world, rank, lo=-1.0, hi=1.0):
     [lo, hi]; rank r solves the contiguous slice r.  No energy is shared."""
     grid = np.linspace(lo, hi, ne_per_rank * world)
     return grid[rank * ne_per_rank:(rank + 1) * ne_per_rank]
+
+
+class _DevicePtr:
+    """A device address seen as a flat float64 array (CUDA array interface)."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False), "version": 3,
+                                         "strides": None}
+
+
+def _device_doubles(ptr, n):
+    return torch.as_tensor(_DevicePtr(ptr, n), device="cuda")
 
 
 def max_over_ranks(value, dist=None, device=None):
@@ -345,6 +358,70 @@ def run_ours(args):
         e2e = {"value": total_pts / el, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(2 * nbytes + 16 * args.ne), "ms_per_step": 1000 * el / args.steps}
 
+    # mixed precision: the same workload with the Schur products on the INT8
+    # tensor cores (FP64-accurate digit splitting); compared block by block
+    # with the FP64 outputs of a sample of energies
+    mixed = None
+    if not args.no_mixed:
+        per = sum(b * b for b in dev.sizes)
+        checked = list(range(0, args.ne, max(1, args.ne // 32)))
+        stream.synchronize()
+        outs = solver.outputs()
+        refs = [_device_doubles(outs[w], 2 * args.ne * per).view(args.ne, 2 * per)[checked].clone()
+                for w in range(2)]
+        t_ref = _device_doubles(outs[2], 2 * args.ne)[0::2].clone()
+        solver.close()
+        msolver = negf.Solver(dev, args.ne, eta=sysm.eta, precision="mixed")
+        mstats = msolver.stats()
+        msolver.set_energies(my_E, sh)
+        for _ in range(args.warmup):
+            msolver.run_profiled(sh)
+        stream.synchronize()
+        msolver.profile_read(reset=True)
+        msolver.check()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            msolver.run_profiled(sh)
+        ev1.record(stream)
+        ev1.synchronize()
+        mms = max_over_ranks(ev0.elapsed_time(ev1), dist if world > 1 else None, "cuda")
+        mprof = msolver.profile_read(reset=True)
+        msolver.check()
+        outs = msolver.outputs()
+        errs = [0.0, 0.0]
+        for w in range(2):
+            got = _device_doubles(outs[w], 2 * args.ne * per).view(args.ne, 2 * per)[checked]
+            o = 0
+            for bsz in dev.sizes:
+                sl_ = slice(2 * o, 2 * (o + bsz * bsz))
+                num = torch.linalg.vector_norm(got[:, sl_] - refs[w][:, sl_], dim=1)
+                den = torch.linalg.vector_norm(refs[w][:, sl_], dim=1)
+                errs[w] = max(errs[w], float((num / den).max()))
+                o += bsz * bsz
+        t_mix = _device_doubles(outs[2], 2 * args.ne)[0::2]
+        t_err = float(((t_mix - t_ref).abs() / t_ref.abs().clamp(min=1.0)).max())
+        mval = total_pts / (mms / 1000.0)
+        tot_ms = sum(v[0] for v in mprof.values())
+        mixed = {"value": mval, "unit": UNIT, "ms_per_step": mms / args.steps, "speedup_vs_fp64": mval / value,
+                 "max_block_rel_err_vs_fp64": {"GR": errs[0], "GL": errs[1], "energies_checked": len(checked)},
+                 "max_T_err_vs_fp64": t_err,
+                 "kernels": {k: {"ms": v[0] / args.steps, "launches": v[2] // args.steps,
+                                 "share": v[0] / tot_ms if tot_ms else None}
+                             for k, v in mprof.items() if v[2]},
+                 "gpu_launches": int(mstats["launches"]) * args.steps,
+                 "algorithmic_tflops": step_flops / ((mms / args.steps) / 1000.0) / 1e12,
+                 "method": "3M complex products of 7-digit int8 splits (28 digit pairs per real product) on "
+                           "tcgen05.mma kind::i8 with exact int32 TMEM accumulation; FP64 Gauss-Jordan inversions"}
+        if "oz_mma" in mprof and mprof["oz_mma"][2]:
+            k = mprof["oz_mma"]
+            mixed["int8_mma"] = {"complex_flops_per_s": k[1] / (k[0] / 1000.0),
+                                 "int8_ops_per_s": k[1] / (k[0] / 1000.0) * 28 * 3 / 4}
+        del refs, t_ref
+        solver = msolver
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -356,7 +433,7 @@ def run_ours(args):
                                  (stats["workspace_bytes"] / 1e9)},
                 "roofline": roof, "kernels": breakdown, "whole_step": whole, "clocks": clk.summary(),
                 "gpu_launches": int(stats["launches"]) * args.steps,
-                "e2e": e2e, "cpu_baseline": cpu}
+                "e2e": e2e, "cpu_baseline": cpu, "mixed": mixed}
         print(json.dumps(line), flush=True)
     solver.close()
     dev.close()

@@ -65,6 +65,11 @@ typedef struct {
  * opA, opB in {'N','T','C'}.  One launch on the FP64 tensor path. */
 int negf_zgemm_batched(char opA, char opB, int32_t nprob, const negf_zgemm_problem* probs, void* stream);
 
+/* negf_zgemm_batched in the MIXED precision mode (INT8 tensor cores with
+ * digit splitting; see NEGF_PREC_MIXED).  Same problems and results within
+ * ~1e-13 relative to |op(A)| |op(B)|; k <= 1024. */
+int negf_zgemm_batched_mixed(char opA, char opB, int32_t nprob, const negf_zgemm_problem* probs, void* stream);
+
 /* Batched be_copy_in_hw! / be_ctranspose! (src/backend_cpu.jl:42-68):
  * C[i] = op(A[i]) with op 'N' (copy) or 'C' (conjugate transpose); C[i] is
  * m[i] x n[i] (A[i] is n[i] x m[i] for 'C'). */
@@ -197,7 +202,16 @@ typedef struct {
   int32_t want_t;    /* transmission */
   int32_t max_chunk; /* energies per device-resident batch (0: by HBM budget) */
   double hbm_budget_gb; /* 0: 80% of free device memory */
+  int32_t precision; /* NEGF_PREC_FP64 or NEGF_PREC_MIXED */
 } negf_solve_opts;
+
+/* Precision modes.  FP64: every product in FP64 on the DMMA tensor path.
+ * MIXED: the Schur-complement products run on the INT8 tensor cores
+ * (tcgen05) with FP64-accurate digit splitting (7 digits of 7 bits per
+ * operand, exact int32 accumulation, ~1e-13 relative per product); the
+ * diagonal-block inversions stay in FP64. */
+#define NEGF_PREC_FP64 0
+#define NEGF_PREC_MIXED 1
 
 /* Solve nE energy points (energies: host array).  gr_out / gl_out receive
  * nE * sum_i b_i^2 complex128 values (energy-major, then layer, column-major
@@ -227,10 +241,13 @@ int negf_solver_check(negf_solver_t s);
  * launch on `stream`; per-launch durations accumulate until read. */
 int negf_solver_run_profiled(negf_solver_t s, void* stream);
 /* Kernel kinds: 0 GEMM, 1 inversion panel, 2 inversion un-permute, 3 block
- * copies, 4 trace, 5 LU panel, 6 LU row swaps, 7 triangular diagonal blocks.
- * Synchronises and writes, per kind, the summed milliseconds, real flops and
- * launch counts of the profiled passes since the last reset (reset != 0
- * starts a new accumulation). */
+ * copies, 4 trace, 5 LU panel, 6 LU row swaps, 7 triangular diagonal blocks,
+ * 8 INT8 digit split, 9 INT8 tensor-core product (mixed precision); the
+ * arrays hold NEGF_PROFILE_KINDS entries. Synchronises and writes, per
+ * kind, the summed milliseconds, real flops and launch counts of the
+ * profiled passes since the last reset (reset != 0 starts a new
+ * accumulation). */
+#define NEGF_PROFILE_KINDS 10
 int negf_solver_profile_read(negf_solver_t s, double* ms, double* flops, int64_t* launches, int32_t reset);
 /* Real flops of one pass (8mnk per complex GEMM, 8n^3 per inversion),
  * number of kernel launches per pass and workspace bytes. */

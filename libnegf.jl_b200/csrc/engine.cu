@@ -4,7 +4,9 @@
 
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <set>
+#include <tuple>
 
 namespace negf {
 
@@ -77,6 +79,121 @@ size_t Plan::push_bytes(const void* p, size_t n) {
 }
 
 void Plan::gemm(char opA, char opB, const std::vector<ZGemmProblem>& probs) {
+  if (!mixed_) {
+    gemm_fp64(opA, opB, probs);
+    return;
+  }
+  std::vector<ZGemmProblem> dbl, mix;
+  for (const auto& p : probs) (p.k > 0 ? mix : dbl).push_back(p);
+  gemm_fp64(opA, opB, dbl);
+  gemm_mixed(opA, opB, mix);
+}
+
+namespace {
+// views of the operands as R x K real-and-imaginary matrices (K = contraction)
+struct OzKey {
+  const cplx* X;
+  long long sr, sk;
+  int rows, cols, conj, side;
+  bool operator<(const OzKey& o) const {
+    return std::tie(X, sr, sk, rows, cols, conj, side) < std::tie(o.X, o.sr, o.sk, o.rows, o.cols, o.conj, o.side);
+  }
+};
+inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
+}  // namespace
+
+void Plan::gemm_mixed(char opA, char opB, const std::vector<ZGemmProblem>& probs) {
+  if (probs.empty()) return;
+  if (!err_) err_ = static_cast<int*>(alloc(sizeof(int)));
+  std::map<OzKey, int> index;
+  std::vector<OzKey> keys;
+  std::vector<std::pair<int, int>> which(probs.size());
+  auto key_of = [&](const ZGemmProblem& p, bool A) {
+    OzKey k;
+    if (A) {  // Y = op(A): m x k
+      k.X = p.A; k.rows = p.m; k.cols = p.k; k.side = 0;
+      if (opA == 'N') { k.sr = 1; k.sk = p.lda; k.conj = 0; }
+      else { k.sr = p.lda; k.sk = 1; k.conj = opA == 'C'; }
+    } else {  // Y = op(B)^T: n x k
+      k.X = p.B; k.rows = p.n; k.cols = p.k; k.side = 1;
+      if (opB == 'N') { k.sr = p.ldb; k.sk = 1; k.conj = 0; }
+      else { k.sr = 1; k.sk = p.ldb; k.conj = opB == 'C'; }
+    }
+    return k;
+  };
+  auto get = [&](const OzKey& k) {
+    auto it = index.find(k);
+    if (it != index.end()) return it->second;
+    int id = (int)keys.size();
+    index[k] = id;
+    keys.push_back(k);
+    return id;
+  };
+  for (size_t i = 0; i < probs.size(); ++i) which[i] = {get(key_of(probs[i], true)), get(key_of(probs[i], false))};
+  // scratch layout of this step's digit slices (shared pool, grown as needed)
+  std::vector<size_t> off_s(keys.size()), off_e(keys.size());
+  std::vector<int> rpad(keys.size()), kpad(keys.size());
+  size_t need = 0;
+  for (size_t i = 0; i < keys.size(); ++i) {
+    rpad[i] = round_up(std::max(keys[i].rows, 1), keys[i].side == 0 ? 128 : 64);
+    kpad[i] = round_up(std::max(keys[i].cols, 1), 32);
+    off_s[i] = need;
+    need += (size_t)21 * rpad[i] * kpad[i];
+    need = (need + 255) & ~size_t(255);
+    off_e[i] = need;
+    need += sizeof(int) * (size_t)rpad[i];
+    need = (need + 255) & ~size_t(255);
+  }
+  if (need > oz_pool_bytes_) {
+    oz_pool_ = static_cast<unsigned char*>(alloc(need));
+    oz_pool_bytes_ = need;
+  }
+  std::vector<OzSplitProblem> sp(keys.size());
+  int max_rows = 0;
+  for (size_t i = 0; i < keys.size(); ++i) {
+    OzSplitProblem& s = sp[i];
+    s.X = keys[i].X; s.sr = keys[i].sr; s.sk = keys[i].sk;
+    s.rows = keys[i].rows; s.cols = keys[i].cols; s.rows_pad = rpad[i]; s.k_pad = kpad[i];
+    s.conj = keys[i].conj; s.pad_ = 0;
+    s.slices = reinterpret_cast<int8_t*>(oz_pool_ + off_s[i]);
+    s.exps = reinterpret_cast<int*>(oz_pool_ + off_e[i]);
+    max_rows = std::max(max_rows, rpad[i]);
+  }
+  Step s1;
+  s1.kind = Step::OZ_SPLIT;
+  s1.off = push_bytes(sp.data(), sp.size() * sizeof(OzSplitProblem));
+  s1.count = (int)sp.size();
+  s1.max_m = max_rows;
+  steps.push_back(s1);
+  std::vector<OzMmaProblem> mp;
+  std::vector<int> starts;
+  int total = 0;
+  double fl = 0.0;
+  for (size_t i = 0; i < probs.size(); ++i) {
+    const ZGemmProblem& p = probs[i];
+    const int a = which[i].first, b = which[i].second;
+    OzMmaProblem q;
+    q.SA = sp[a].slices; q.eA = sp[a].exps; q.SB = sp[b].slices; q.eB = sp[b].exps;
+    q.C = p.C; q.Cin = p.Cin; q.diag_ptr = p.diag_ptr;
+    q.m = p.m; q.n = p.n; q.m_pad = rpad[a]; q.n_pad = rpad[b]; q.k_pad = kpad[a];
+    q.ldc = p.ldc; q.ldcin = p.ldcin; q.pad_ = 0;
+    q.alpha = p.alpha; q.beta = p.beta; q.diag = p.diag;
+    starts.push_back(total);
+    total += (q.m_pad / 128) * (q.n_pad / 64);
+    fl += 8.0 * p.m * (double)p.n * p.k;
+    mp.push_back(q);
+  }
+  Step s2;
+  s2.kind = Step::OZ_MMA;
+  s2.off = push_bytes(mp.data(), mp.size() * sizeof(OzMmaProblem));
+  s2.tiles_off = push_bytes(starts.data(), starts.size() * sizeof(int));
+  s2.count = (int)mp.size();
+  s2.total_tiles = total;
+  s2.flops = fl;
+  steps.push_back(s2);
+}
+
+void Plan::gemm_fp64(char opA, char opB, const std::vector<ZGemmProblem>& probs) {
   std::vector<ZGemmProblem> v;
   std::vector<int> starts;
   int total = 0;
@@ -145,7 +262,7 @@ void Plan::inv(const std::vector<InvSpec>& specs) {
       int w = std::min(nb, p.n - k0);
       g.push_back(gp(p.F, p.n, p.Bbuf, w, p.W, p.ld, p.n, p.n, w, ONE, p.W, p.ld, ONE));
     }
-    gemm('N', 'N', g);
+    gemm_fp64('N', 'N', g);  // the diagonal-block inversion stays in FP64
   }
   // the GEMM updates carry their own flop count; the panel work is the rest
   Step u;
@@ -198,8 +315,8 @@ void Plan::getrf(const std::vector<LuSpec>& specs) {
       cplx* A22 = p.A + (k0 + wd) + (size_t)(k0 + wd) * p.ld;
       g2.push_back(gp(A21, p.ld, A12, p.ld, A22, p.ld, rest, rest, wd, MONE, A22, p.ld, ONE));
     }
-    gemm('N', 'N', g1);
-    gemm('N', 'N', g2);
+    gemm_fp64('N', 'N', g1);  // factorisations stay in FP64
+    gemm_fp64('N', 'N', g2);
   }
 }
 
@@ -246,8 +363,8 @@ void Plan::trtri(const std::vector<TriSpec>& specs, bool upper) {
         g2.push_back(gp(p.X + j0 + (size_t)j0 * p.ldx, p.ldx, sp.T, nb, p.X + j0, p.ldx, wj, j0, wj, MONE));
       }
     }
-    gemm('N', 'N', g1);
-    gemm('N', 'N', g2);
+    gemm_fp64('N', 'N', g1);
+    gemm_fp64('N', 'N', g2);
   }
 }
 
@@ -290,6 +407,12 @@ cudaError_t Plan::finalize() {
     cudaError_t e = zlu_prepare(lu_smem, tri_smem);
     if (e != cudaSuccess) return e;
   }
+  for (const auto& s : steps)
+    if (s.kind == Step::OZ_MMA) {
+      cudaError_t e = ozaki_prepare();
+      if (e != cudaSuccess) return e;
+      break;
+    }
   for (auto& o : ops) {
     cudaError_t e = zgemm_prepare(o.first, o.second);
     if (e != cudaSuccess) return e;
@@ -387,6 +510,13 @@ cudaError_t Plan::launch_step(const Step& s, const unsigned char* base, cudaStre
         break;
       case Step::TRI_DIAG:
         e = launch_ztrtri_diag(base + s.off, s.count, s.nb, s.blocked, s.max_n, s.smem, stream);
+        break;
+      case Step::OZ_SPLIT:
+        e = launch_ozaki_split(base + s.off, s.count, s.max_m, stream);
+        break;
+      case Step::OZ_MMA:
+        e = launch_ozaki_mma(base + s.off, reinterpret_cast<const int*>(base + s.tiles_off), s.count, s.total_tiles,
+                             err_, stream);
         break;
     }
   }

@@ -40,6 +40,15 @@ cudaError_t launch_zlaswp_copy(const void* probs, int nprob, int k0, int nb, int
 cudaError_t launch_ztrtri_diag(const void* probs, int nprob, int nb, int upper, int max_n, size_t smem,
                                cudaStream_t st);
 
+// mixed-precision (Ozaki / INT8 tcgen05) complex GEMM, zgemm_ozaki.cu
+struct OzSplitProblem;
+struct OzMmaProblem;
+size_t ozaki_mma_smem_bytes();
+cudaError_t ozaki_prepare();
+cudaError_t launch_ozaki_split(const void* probs, int nprob, int max_rows_pad, cudaStream_t st);
+cudaError_t launch_ozaki_mma(const void* probs, const int* tile_start, int nprob, int total_tiles, int* err,
+                             cudaStream_t st);
+
 // LU request (LAPACK getrf semantics, in place).  ipiv receives 0-based
 // global pivot rows; ipiv_lapack (optional, device int32) 1-based ones.
 struct LuSpec {
@@ -91,7 +100,8 @@ struct InvSpec {
 
 struct Step {
   enum Kind {
-    GEMM = 0, GJ_PANEL = 1, GJ_UNPERMUTE = 2, BLOCKOP = 3, TRACE = 4, LU_PANEL = 5, LU_SWAP = 6, TRI_DIAG = 7
+    GEMM = 0, GJ_PANEL = 1, GJ_UNPERMUTE = 2, BLOCKOP = 3, TRACE = 4, LU_PANEL = 5, LU_SWAP = 6, TRI_DIAG = 7,
+    OZ_SPLIT = 8, OZ_MMA = 9
   } kind;
   char opA = 'N', opB = 'N';
   size_t off = 0;        // descriptor offset in the blob
@@ -114,7 +124,15 @@ class Plan {
   void* alloc(size_t bytes);
   cplx* alloc_c(size_t n) { return static_cast<cplx*>(alloc(n * sizeof(cplx))); }
 
+  // Complex GEMM step; with set_mixed(true) the products (k > 0) run on the
+  // INT8 tensor cores with FP64-accurate Ozaki splitting.  Products issued by
+  // inv() (the Gauss-Jordan updates) always stay in FP64.
   void gemm(char opA, char opB, const std::vector<ZGemmProblem>& probs);
+  void gemm_fp64(char opA, char opB, const std::vector<ZGemmProblem>& probs);
+  void gemm_mixed(char opA, char opB, const std::vector<ZGemmProblem>& probs);
+  void set_mixed(bool on) { mixed_ = on; }
+  bool mixed() const { return mixed_; }
+  int* error_flag() const { return err_; }
   void inv(const std::vector<InvSpec>& specs);
   void blockops(const std::vector<ZBlockOp>& ops);
   void trace(const std::vector<ZTraceProblemHost>& probs);
@@ -143,6 +161,10 @@ class Plan {
   cudaGraph_t graph_ = nullptr;
   cudaGraphExec_t gexec_ = nullptr;
   cudaStream_t graph_stream_ = nullptr;
+  bool mixed_ = false;
+  int* err_ = nullptr;            // tensor-core wait time-out flag (device int)
+  unsigned char* oz_pool_ = nullptr;  // digit-slice scratch shared by all mixed steps
+  size_t oz_pool_bytes_ = 0;
 };
 
 // ---------------------------------------------------------------------------

@@ -187,6 +187,12 @@ int build_solver(negf_solver_s& S) {
   if (S.opts.want_t) S.t2 = static_cast<double*>(plan.alloc(sizeof(double) * 2 * nE));
   const cplx i_unit = make_double2(0.0, 1.0);
   NEGF_TRY_CUDA(cudaMemcpy(S.params + 3 * nE, &i_unit, sizeof(cplx), cudaMemcpyHostToDevice), "solver params");
+  if (S.opts.precision != NEGF_PREC_FP64 && S.opts.precision != NEGF_PREC_MIXED)
+    return fail(NEGF_ERR_INVALID, "precision must be NEGF_PREC_FP64 or NEGF_PREC_MIXED");
+  for (int x : d.b)
+    if (S.opts.precision == NEGF_PREC_MIXED && x > 1024)
+      return fail(NEGF_ERR_INVALID, "the mixed precision mode supports blocks up to 1024");
+  plan.set_mixed(S.opts.precision == NEGF_PREC_MIXED);
 
   std::vector<TriSystem> sys(nE);
   std::vector<RgfWork> work(nE);
@@ -358,6 +364,43 @@ int negf_zgemm_batched(char opA, char opB, int32_t nprob, const negf_zgemm_probl
     }
     plan.gemm(opA, opB, v);
     return run_plan_sync(plan, static_cast<cudaStream_t>(stream), nullptr, 0, "negf_zgemm_batched");
+  } catch (const std::bad_alloc&) {
+    return fail(NEGF_ERR_NOMEM, "device allocation failed");
+  }
+}
+
+int negf_zgemm_batched_mixed(char opA, char opB, int32_t nprob, const negf_zgemm_problem* probs, void* stream) {
+  if (int r = check_device()) return r;
+  if (nprob < 0 || (nprob > 0 && !probs)) return fail(NEGF_ERR_INVALID, "bad problem list");
+  auto okop = [](char c) { return c == 'N' || c == 'T' || c == 'C'; };
+  if (!okop(opA) || !okop(opB)) return fail(NEGF_ERR_INVALID, "op must be N, T or C");
+  try {
+    Plan plan;
+    plan.set_mixed(true);
+    std::vector<ZGemmProblem> v(nprob);
+    for (int i = 0; i < nprob; ++i) {
+      const negf_zgemm_problem& q = probs[i];
+      if (q.m < 0 || q.n < 0 || q.k < 0 || q.k > 1024)
+        return fail(NEGF_ERR_INVALID, "dimensions must be >= 0 and k <= 1024");
+      ZGemmProblem& p = v[i];
+      p.A = static_cast<const cplx*>(q.A); p.B = static_cast<const cplx*>(q.B);
+      p.Cin = static_cast<const cplx*>(q.Cin); p.C = static_cast<cplx*>(q.C); p.diag_ptr = nullptr;
+      p.m = q.m; p.n = q.n; p.k = q.k;
+      p.lda = std::max(1, q.lda); p.ldb = std::max(1, q.ldb); p.ldc = std::max(1, q.ldc);
+      p.ldcin = std::max(1, q.ldcin); p.pad_ = 0;
+      p.alpha = c2(q.alpha); p.beta = c2(q.beta); p.diag = c2(q.diag);
+      if (p.m > 0 && p.n > 0 && !p.C) return fail(NEGF_ERR_INVALID, "NULL C");
+      if (p.k > 0 && (!p.A || !p.B)) return fail(NEGF_ERR_INVALID, "NULL A or B");
+    }
+    plan.gemm(opA, opB, v);
+    int rc = run_plan_sync(plan, static_cast<cudaStream_t>(stream), nullptr, 0, "negf_zgemm_batched_mixed");
+    if (rc) return rc;
+    if (plan.error_flag()) {
+      int h = 0;
+      NEGF_TRY_CUDA(cudaMemcpy(&h, plan.error_flag(), sizeof(int), cudaMemcpyDeviceToHost), "mixed gemm");
+      if (h) return fail(NEGF_ERR_CUDA, "negf_zgemm_batched_mixed: tensor-core completion wait timed out");
+    }
+    return NEGF_SUCCESS;
   } catch (const std::bad_alloc&) {
     return fail(NEGF_ERR_NOMEM, "device allocation failed");
   }
@@ -673,7 +716,7 @@ int negf_solver_run_profiled(negf_solver_t s, void* stream) {
 
 int negf_solver_profile_read(negf_solver_t s, double* ms, double* flops, int64_t* launches, int32_t reset) {
   if (!s) return fail(NEGF_ERR_INVALID, "NULL solver");
-  const int K = 8;
+  const int K = NEGF_PROFILE_KINDS;
   std::vector<double> t(K, 0.0), f(K, 0.0);
   std::vector<int64_t> n(K, 0);
   const auto& steps = s->plan->steps;
@@ -730,6 +773,11 @@ int negf_solver_check(negf_solver_t s) {
   if (!s) return fail(NEGF_ERR_INVALID, "NULL solver");
   std::vector<int> h(s->nE);
   NEGF_TRY_CUDA(cudaMemcpy(h.data(), s->info, sizeof(int) * s->nE, cudaMemcpyDeviceToHost), "solver check");
+  if (s->plan->error_flag()) {
+    int fl = 0;
+    NEGF_TRY_CUDA(cudaMemcpy(&fl, s->plan->error_flag(), sizeof(int), cudaMemcpyDeviceToHost), "solver check");
+    if (fl) return fail(NEGF_ERR_CUDA, "tensor-core completion wait timed out in the mixed-precision products");
+  }
   for (int e = 0; e < s->nE; ++e)
     if (h[e]) {
       char buf[128];

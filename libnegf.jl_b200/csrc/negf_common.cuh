@@ -86,6 +86,31 @@ struct ZTriProblem {
   int n, lda, ldx, pad_;
 };
 
+// Digit split of one real-and-imaginary operand view for the Ozaki GEMM
+// (zgemm_ozaki.cu): Y[r][k] = X[r*sr + k*sk] (conjugated when conj), R x K.
+struct OzSplitProblem {
+  const cplx* X;
+  long long sr, sk;
+  int rows, cols, rows_pad, k_pad;
+  int conj, pad_;
+  int8_t* slices;  // [3][7][rows_pad][k_pad] int8 digits, K-major rows
+  int* exps;       // [rows_pad] power-of-two row scales
+};
+
+// One complex product of the Ozaki GEMM: C = alpha A B + beta Cin + diag I
+// from the digit slices of A (m x k) and of B^T (n x k).
+struct OzMmaProblem {
+  const int8_t* SA;
+  const int* eA;
+  const int8_t* SB;
+  const int* eB;
+  cplx* C;
+  const cplx* Cin;
+  const cplx* diag_ptr;
+  int m, n, m_pad, n_pad, k_pad, ldc, ldcin, pad_;
+  cplx alpha, beta, diag;
+};
+
 // Elementwise block operations (ZBlockOp::kind).
 enum ZOpKind : int {
   ZOP_COPY = 0,        // C = A

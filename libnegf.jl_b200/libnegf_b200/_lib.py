@@ -32,7 +32,12 @@ class ZGemmProblem(ctypes.Structure):
 class SolveOpts(ctypes.Structure):
     _fields_ = [("eta", ctypes.c_double), ("mu_l", ctypes.c_double), ("mu_r", ctypes.c_double),
                 ("kT", ctypes.c_double), ("want_gr", ctypes.c_int32), ("want_gl", ctypes.c_int32),
-                ("want_t", ctypes.c_int32), ("max_chunk", ctypes.c_int32), ("hbm_budget_gb", ctypes.c_double)]
+                ("want_t", ctypes.c_int32), ("max_chunk", ctypes.c_int32), ("hbm_budget_gb", ctypes.c_double),
+                ("precision", ctypes.c_int32)]
+
+
+NEGF_PREC_FP64 = 0
+NEGF_PREC_MIXED = 1
 
 
 class CCscMatrix(ctypes.Structure):
@@ -46,6 +51,8 @@ PROTOTYPES = {
     "negf_version": (ctypes.c_int, []),
     "negf_zgemm_batched": (ctypes.c_int, [ctypes.c_char, ctypes.c_char, ctypes.c_int32,
                                           ctypes.POINTER(ZGemmProblem), ctypes.c_void_p]),
+    "negf_zgemm_batched_mixed": (ctypes.c_int, [ctypes.c_char, ctypes.c_char, ctypes.c_int32,
+                                                ctypes.POINTER(ZGemmProblem), ctypes.c_void_p]),
     "negf_zcopy_batched": (ctypes.c_int, [ctypes.c_char, ctypes.c_int32, c_int32_p, c_int32_p, c_void_pp, c_int32_p,
                                           c_void_pp, c_int32_p, ctypes.c_void_p]),
     "negf_zinv_batched": (ctypes.c_int, [ctypes.c_int32, c_int32_p, c_void_pp, c_int32_p, c_void_pp, c_int32_p,

@@ -183,13 +183,15 @@ def be_gemm_(tA, tB, alpha, A, B, beta, C, td=None, cd=None):
     check(load().negf_zgemm_batched(tA.encode(), tB.encode(), 1, arr, stream_handle()))
 
 
-def be_gemm_batched_(tA, tB, items):
+def be_gemm_batched_(tA, tB, items, precision="fp64"):
     """Many be_gemm! calls with the same ops in one launch: items are tuples
-    (alpha, A, B, beta, C)."""
+    (alpha, A, B, beta, C).  precision "mixed" runs the products on the INT8
+    tensor cores with FP64-accurate digit splitting."""
     if not items:
         return
     arr = (_lib.ZGemmProblem * len(items))(*[_gemm_problem(tA, tB, *it) for it in items])
-    check(load().negf_zgemm_batched(tA.encode(), tB.encode(), len(items), arr, stream_handle()))
+    fn = load().negf_zgemm_batched_mixed if precision == "mixed" else load().negf_zgemm_batched
+    check(fn(tA.encode(), tB.encode(), len(items), arr, stream_handle()))
 
 
 def be_ctranspose_(out, inp, td=None, cd=None):

@@ -26,12 +26,15 @@ def _host_blocks(blocks):
 
 
 def make_opts(eta=1e-6, mu_l=0.1, mu_r=-0.1, kT=0.025, want_gr=True, want_gl=True, want_t=True, max_chunk=0,
-              hbm_budget_gb=0.0):
+              hbm_budget_gb=0.0, precision="fp64"):
+    """precision: "fp64" (every product in FP64) or "mixed" (Schur products on
+    the INT8 tensor cores with FP64-accurate digit splitting)."""
     o = _lib.SolveOpts()
     o.eta, o.mu_l, o.mu_r, o.kT = eta, mu_l, mu_r, kT
     o.want_gr, o.want_gl, o.want_t = int(want_gr), int(want_gl), int(want_t)
     o.max_chunk = int(max_chunk)
     o.hbm_budget_gb = float(hbm_budget_gb)
+    o.precision = {"fp64": _lib.NEGF_PREC_FP64, "mixed": _lib.NEGF_PREC_MIXED}[precision]
     return o
 
 
@@ -72,7 +75,7 @@ class Device:
             pass
 
     def solve(self, energies, eta=1e-6, mu_l=0.1, mu_r=-0.1, kT=0.025, want_gr=True, want_gl=True, want_t=True,
-              max_chunk=0):
+              max_chunk=0, precision="fp64"):
         """G^R / G^< diagonal blocks and T(E) for every energy (host arrays).
 
         Returns (gr, gl, t): gr/gl are lists (per energy) of lists (per layer)
@@ -83,7 +86,7 @@ class Device:
         gr = np.empty(nE * per, dtype=np.complex128) if want_gr else None
         gl = np.empty(nE * per, dtype=np.complex128) if want_gl else None
         t = np.empty(nE, dtype=np.float64) if want_t else None
-        o = make_opts(eta, mu_l, mu_r, kT, want_gr, want_gl, want_t, max_chunk)
+        o = make_opts(eta, mu_l, mu_r, kT, want_gr, want_gl, want_t, max_chunk, precision=precision)
         check(load().negf_solve(self._handle, nE, E.ctypes.data_as(_lib.c_double_p), ctypes.byref(o),
                                 gr.ctypes.data if gr is not None else None,
                                 gl.ctypes.data if gl is not None else None,
@@ -126,7 +129,8 @@ class Solver:
     def check(self):
         check(load().negf_solver_check(self._h))
 
-    KINDS = ["gemm", "gj_panel", "gj_unpermute", "blockop", "trace", "lu_panel", "lu_swap", "tri_diag"]
+    KINDS = ["gemm", "gj_panel", "gj_unpermute", "blockop", "trace", "lu_panel", "lu_swap", "tri_diag",
+             "oz_split", "oz_mma"]
 
     def run_profiled(self, stream=None):
         """One pass launch by launch with a CUDA event after each launch."""
@@ -134,9 +138,10 @@ class Solver:
 
     def profile_read(self, reset=True):
         """Per kernel kind: (ms, flops, launches) summed over profiled passes."""
-        ms = (ctypes.c_double * 8)()
-        fl = (ctypes.c_double * 8)()
-        n = (ctypes.c_int64 * 8)()
+        K = len(self.KINDS)
+        ms = (ctypes.c_double * K)()
+        fl = (ctypes.c_double * K)()
+        n = (ctypes.c_int64 * K)()
         check(load().negf_solver_profile_read(self._h, ms, fl, n, int(reset)))
         return {k: (ms[i], fl[i], n[i]) for i, k in enumerate(self.KINDS)}
 

