@@ -74,6 +74,7 @@ class _DevicePtr:
 
 
 def _device_doubles(ptr, n):
+    import torch
     return torch.as_tensor(_DevicePtr(ptr, n), device="cuda")
 
 

@@ -28,3 +28,11 @@ def rel_fro(a, b):
     import numpy as np
     nb = np.linalg.norm(b)
     return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+def kappa_tol(cond, tol=1e-12):
+    """Parity bound between two FP64 inversions of the same matrix: each is
+    backward stable with a normwise forward error near u * kappa (u = 2^-53),
+    so they may differ by 2 u kappa. The 1e-12 bar stands up to kappa ~ 4.5e3;
+    the stress generators also draw worse-conditioned matrices."""
+    return max(tol, 2.0 * 2.0 ** -53 * float(cond))

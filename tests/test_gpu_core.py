@@ -9,7 +9,7 @@ products.
 import numpy as np
 import pytest
 
-from conftest import rel_fro
+from conftest import kappa_tol, rel_fro
 from oracle import rgf as o_rgf, keldysh as o_keldysh, physics as o_phys
 from oracle.blockmatrix import bm_convert_dense, band_of_dense
 from oracle.generators import bm_create_synthetic_random, hermitian_random_like
@@ -20,10 +20,9 @@ TOL = 1e-12
 
 
 def tol_ref(M):
-    """The reference's ComplexF64 tolerance (1e-12) holds for kappa(M) <= 1e4;
-    its uniform-[0,1) generator also draws worse-conditioned matrices, where any
-    two FP64 implementations (the oracle included) differ by ~kappa * eps."""
-    return TOL * max(1.0, np.linalg.cond(bm_convert_dense(M)) / 1e4)
+    """The reference's ComplexF64 tolerance (1e-12), widened to 2 u kappa(M)
+    for the worse-conditioned stress matrices."""
+    return kappa_tol(np.linalg.cond(bm_convert_dense(M)), TOL)
 
 
 def _rand(rng, m, n):

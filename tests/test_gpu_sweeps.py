@@ -13,7 +13,7 @@ import ctypes
 import numpy as np
 import pytest
 
-from conftest import rel_fro
+from conftest import kappa_tol, rel_fro
 from oracle import rgf as o_rgf, general_rgf as o_grgf, selected_inverse as o_si, ddrgf as o_dd
 from oracle.blockmatrix import bm_convert_dense, band_of_dense, bm_fuse_to_tridiagonal as o_fuse
 from oracle.generators import bm_create_synthetic_random, set_sparse_block, full_of_blocks
@@ -37,11 +37,10 @@ def test_general_rgf(negf, npl, b, nd):
     out = negf.BlockMatrix(M.blockSizes)
     negf.bndiag_of_inv_general_rgf_(out, dM, negf.allocate_aux_data_general_RGF(dM))
     G = negf.bm_to_dense(out)
-    # the reference's 1e-12 (roundoffs[ComplexF64] * 1e3) holds for kappa(M) <= 1e4; the
-    # uniform-[0,1) generator also draws worse-conditioned matrices, where any two FP64
-    # implementations (the oracle included) differ by ~kappa * eps: scale with kappa
+    # the reference's 1e-12 (roundoffs[ComplexF64] * 1e3), widened to 2 u kappa for
+    # the worse-conditioned draws of the uniform-[0,1) generator
     D = bm_convert_dense(M)
-    tol = 1e-12 * max(1.0, np.linalg.cond(D) / 1e4)
+    tol = kappa_tol(np.linalg.cond(D))
     assert rel_fro(G, ref) < tol
     exact = band_of_dense(np.linalg.inv(D), M.blockSizes, {"in": nd, "out": nd})
     assert rel_fro(G, exact) < tol
@@ -61,7 +60,7 @@ def test_general_rgf_vs_fused(negf):
     fout = negf.BlockMatrix(fused.blockSizes)
     negf.bndiag_of_inv_rgf_local_(fout, fused)
     aligned = band_of_dense(negf.bm_to_dense(fout), M.blockSizes, {"in": 5, "out": 5})
-    assert rel_fro(negf.bm_to_dense(gen), aligned) < 1e-12
+    assert rel_fro(negf.bm_to_dense(gen), aligned) < kappa_tol(np.linalg.cond(bm_convert_dense(M)))
 
 
 RIND = [1, 1, 1, 2, 3, 3, 3, 4, 5]
