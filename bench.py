@@ -414,12 +414,13 @@ def run_ours(args):
                              for k, v in mprof.items() if v[2]},
                  "gpu_launches": int(mstats["launches"]) * args.steps,
                  "algorithmic_tflops": step_flops / ((mms / args.steps) / 1000.0) / 1e12,
-                 "method": "3M complex products of 7-digit int8 splits (28 digit pairs per real product) on "
-                           "tcgen05.mma kind::i8 with exact int32 TMEM accumulation; FP64 Gauss-Jordan inversions"}
+                 "method": "3M complex products of 7-digit base-256 int8 splits of 54-bit fixed-point rows "
+                           "(34 digit pairs per real product) on tcgen05.mma kind::i8 with exact int32 TMEM "
+                           "accumulation; FP64 Gauss-Jordan inversions"}
         if "oz_mma" in mprof and mprof["oz_mma"][2]:
             k = mprof["oz_mma"]
             mixed["int8_mma"] = {"complex_flops_per_s": k[1] / (k[0] / 1000.0),
-                                 "int8_ops_per_s": k[1] / (k[0] / 1000.0) * 28 * 3 / 4}
+                                 "int8_ops_per_s": k[1] / (k[0] / 1000.0) * 34 * 3 / 4}
         del refs, t_ref
         solver = msolver
 

@@ -138,7 +138,7 @@ void Plan::gemm_mixed(char opA, char opB, const std::vector<ZGemmProblem>& probs
     rpad[i] = round_up(std::max(keys[i].rows, 1), keys[i].side == 0 ? 128 : 64);
     kpad[i] = round_up(std::max(keys[i].cols, 1), 32);
     off_s[i] = need;
-    need += (size_t)21 * rpad[i] * kpad[i];
+    need += (size_t)21 * rpad[i] * kpad[i];  // 3 real operands x 7 digit slices
     need = (need + 255) & ~size_t(255);
     off_e[i] = need;
     need += sizeof(int) * (size_t)rpad[i];
@@ -154,7 +154,7 @@ void Plan::gemm_mixed(char opA, char opB, const std::vector<ZGemmProblem>& probs
     OzSplitProblem& s = sp[i];
     s.X = keys[i].X; s.sr = keys[i].sr; s.sk = keys[i].sk;
     s.rows = keys[i].rows; s.cols = keys[i].cols; s.rows_pad = rpad[i]; s.k_pad = kpad[i];
-    s.conj = keys[i].conj; s.pad_ = 0;
+    s.conj = keys[i].conj; s.tile_rows = keys[i].side == 0 ? 128 : 64;
     s.slices = reinterpret_cast<int8_t*>(oz_pool_ + off_s[i]);
     s.exps = reinterpret_cast<int*>(oz_pool_ + off_e[i]);
     max_rows = std::max(max_rows, rpad[i]);
@@ -166,7 +166,7 @@ void Plan::gemm_mixed(char opA, char opB, const std::vector<ZGemmProblem>& probs
   s1.max_m = max_rows;
   steps.push_back(s1);
   std::vector<OzMmaProblem> mp;
-  std::vector<int> starts;
+  std::vector<int> tmap;  // 4 ints per output tile, see launch_ozaki_mma
   int total = 0;
   double fl = 0.0;
   for (size_t i = 0; i < probs.size(); ++i) {
@@ -178,15 +178,21 @@ void Plan::gemm_mixed(char opA, char opB, const std::vector<ZGemmProblem>& probs
     q.m = p.m; q.n = p.n; q.m_pad = rpad[a]; q.n_pad = rpad[b]; q.k_pad = kpad[a];
     q.ldc = p.ldc; q.ldcin = p.ldcin; q.pad_ = 0;
     q.alpha = p.alpha; q.beta = p.beta; q.diag = p.diag;
-    starts.push_back(total);
-    total += (q.m_pad / 128) * (q.n_pad / 64);
+    const int tm = q.m_pad / 128, tn = q.n_pad / 64, kc = q.k_pad / 32;
+    for (int t = 0; t < tm * tn; ++t) {
+      tmap.push_back((int)i);
+      tmap.push_back((t / tn) | ((t % tn) << 16));
+      tmap.push_back(kc | (tm << 16));
+      tmap.push_back(tn);
+    }
+    total += tm * tn;
     fl += 8.0 * p.m * (double)p.n * p.k;
     mp.push_back(q);
   }
   Step s2;
   s2.kind = Step::OZ_MMA;
   s2.off = push_bytes(mp.data(), mp.size() * sizeof(OzMmaProblem));
-  s2.tiles_off = push_bytes(starts.data(), starts.size() * sizeof(int));
+  s2.tiles_off = push_bytes(tmap.data(), tmap.size() * sizeof(int));
   s2.count = (int)mp.size();
   s2.total_tiles = total;
   s2.flops = fl;
@@ -515,8 +521,7 @@ cudaError_t Plan::launch_step(const Step& s, const unsigned char* base, cudaStre
         e = launch_ozaki_split(base + s.off, s.count, s.max_m, stream);
         break;
       case Step::OZ_MMA:
-        e = launch_ozaki_mma(base + s.off, reinterpret_cast<const int*>(base + s.tiles_off), s.count, s.total_tiles,
-                             err_, stream);
+        e = launch_ozaki_mma(base + s.off, base + s.tiles_off, s.total_tiles, err_, stream);
         break;
     }
   }

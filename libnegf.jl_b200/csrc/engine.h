@@ -46,8 +46,9 @@ struct OzMmaProblem;
 size_t ozaki_mma_smem_bytes();
 cudaError_t ozaki_prepare();
 cudaError_t launch_ozaki_split(const void* probs, int nprob, int max_rows_pad, cudaStream_t st);
-cudaError_t launch_ozaki_mma(const void* probs, const int* tile_start, int nprob, int total_tiles, int* err,
-                             cudaStream_t st);
+// tile_map: per output tile an int4 (problem, m tile | n tile << 16,
+// K chunks | m tiles << 16, n tiles)
+cudaError_t launch_ozaki_mma(const void* probs, const void* tile_map, int total_tiles, int* err, cudaStream_t st);
 
 // LU request (LAPACK getrf semantics, in place).  ipiv receives 0-based
 // global pivot rows; ipiv_lapack (optional, device int32) 1-based ones.

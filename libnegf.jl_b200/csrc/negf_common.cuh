@@ -88,13 +88,20 @@ struct ZTriProblem {
 
 // Digit split of one real-and-imaginary operand view for the Ozaki GEMM
 // (zgemm_ozaki.cu): Y[r][k] = X[r*sr + k*sk] (conjugated when conj), R x K.
+// The digits are stored pre-tiled for the tensor cores: for every real
+// operand p (re, im, re + im), row tile t (tile_rows rows) and 32-wide K chunk
+// c one contiguous block of 7 digit slices in the canonical K-major
+// core-matrix order (r, k) -> (k / 16) * R * 16 + (r / 8) * 128 + (r % 8) * 16
+// + k % 16; blocks ordered [p][t][c]. Left operand (tile_rows 128): each slice
+// is its own R = 128 matrix. Right operand (tile_rows 64): the seven slices
+// form one R = 448 matrix (row 64 i + r for slice i).
 struct OzSplitProblem {
   const cplx* X;
   long long sr, sk;
   int rows, cols, rows_pad, k_pad;
-  int conj, pad_;
-  int8_t* slices;  // [3][7][rows_pad][k_pad] int8 digits, K-major rows
-  int* exps;       // [rows_pad] power-of-two row scales
+  int conj, tile_rows;  // tile_rows: 128 (left operand) or 64 (right operand)
+  int8_t* slices;       // 3 * 7 * rows_pad * k_pad int8 digits
+  int* exps;            // [rows_pad] power-of-two row scales
 };
 
 // One complex product of the Ozaki GEMM: C = alpha A B + beta Cin + diag I

@@ -6,25 +6,37 @@
 // multiplication unit", 2024).
 //
 //   * split: every row r of a real operand Y (R x K) gets a power-of-two scale
-//     2^e_r > max_k |Y[r,k]|; Y[r,k] = 2^e_r * sum_{s=1..7} d_s 2^(-7 s) with
-//     signed digits |d_s| <= 127 (int8), so seven digits carry 49 bits;
-//   * product: sum_k A[r,k] B[c,k] = 2^(eA_r + eB_c) sum_d 2^(-7 d) acc_d with
-//     acc_d = sum_{s+t=d} sum_k dA_s dB_t; every acc_d is an exact int32 sum
-//     (|acc_d| <= 7 * K * 127^2 < 2^31 for K <= 1024); only pairs with
-//     s + t <= 8 are formed (28 of 49), which bounds the error near 2^-49
-//     relative to |A||B| (measured ~1e-13 per complex product);
+//     2^e_r > max_k |Y[r,k]|; x = rint(Y[r,k] 2^(54 - e_r)) is a 54-bit
+//     integer, written as seven balanced base-256 digits x = sum_i s_i
+//     256^(6 - i) (top digit |s_0| <= 64, lower digits in [-128, 127]); the
+//     digits are the bytes of x + C6 (lower ones minus 128), so the split is a
+//     conversion, an add and byte permutes per element (representation error
+//     <= 2^(e_r - 55));
+//   * product: sum_k A[r,k] B[c,k] = 2^(eA_r + eB_c) sum_{D=0..7} 2^(-12 - 8D)
+//     acc_D, acc_D = sum_{i+j=D} sum_k sA_i sB_j; each acc_D is an exact int32
+//     sum (|acc_D| <= 7 * K * 2^14 < 2^31 for K < 18000); the 34 digit pairs
+//     with i + j <= 7 are formed; the dropped ones sum to below
+//     2^(eA_r + eB_c - 59) K, so a product is as accurate as an FP64 one;
 //   * complex: 3M (Gauss) -- P1 = Ar Br, P2 = Ai Bi, P3 = (Ar+Ai)(Br+Bi),
 //     Re = P1 - P2, Im = P3 - P1 - P2 -- the three real operands of a side
-//     share one scale per row;
-//   * the MMA kernel: one CTA per 128 x 64 output tile; 2-stage cp.async
-//     staging of the seven digit slices of A and B per 32-byte K chunk into
-//     the canonical K-major (no swizzle) UMMA layout; one thread issues the
-//     28 MMAs of a chunk into seven TMEM accumulators (one per digit
-//     diagonal d = 2..8, 7 x 64 columns) and commits them to an mbarrier;
-//     after each real product the eight warps drain the accumulators into FP64
-//     registers (warp w reads TMEM lanes 32(w%4).., columns 32(w/4)..).
-// All mbarrier waits are bounded: on time-out the kernel records an error
-// code, waits (bounded) for its MMAs in flight, releases its TMEM and returns.
+//     share one scale per row and xr + xi is formed exactly in integers;
+//   * storage: the split writes, per (real operand, row tile, 32-byte K chunk),
+//     one contiguous block of the seven digit slices already in the canonical
+//     K-major core-matrix layout of the tensor-core shared-memory descriptors,
+//     so that the product kernel moves a whole stage with two bulk copies; the
+//     right operand's seven slices form one 448-row matrix, so that one MMA
+//     multiplies a left digit slice by several right digit slices at once;
+//   * the product kernel (persistent, one CTA per SM, 128 x 64 output tiles,
+//     256 threads): one thread streams stages with cp.async.bulk into a 5-deep
+//     mbarrier ring and issues the 12 MMAs (N = 64..256) of each stage into
+//     eight TMEM accumulators (one per digit diagonal, 8 x 64 columns); after
+//     each real product the eight warps drain the accumulators into FP64
+//     registers, and at the end of a tile they write
+//     C = alpha A B + beta Cin + diag I while the next tile's first product is
+//     already on the tensor cores.
+// Every mbarrier wait is bounded: a role that times out records an error code
+// and raises an abort flag that ends the other roles' waits; the CTA then
+// waits (bounded) for its copies and MMAs in flight, releases TMEM and returns.
 #include "negf_common.cuh"
 
 #include <cstdint>
@@ -32,88 +44,169 @@
 namespace negf {
 
 namespace oz {
-constexpr int S = 7;            // digits per operand
-constexpr int NP = 3;           // real products (3M)
+constexpr int S = 7;             // base-256 digits per operand
+constexpr int NP = 3;            // real products (3M)
+constexpr int ND = 8;            // digit diagonals D = i + j = 0..7 (34 digit pairs)
 constexpr int TM = 128, TN = 64, KC = 32;
-constexpr int THREADS = 256;
-constexpr int A_SLICE = TM * KC;  // bytes of one digit slice of the A tile
-constexpr int B_SLICE = TN * KC;
-constexpr int STAGE = S * (A_SLICE + B_SLICE);
-constexpr int STAGES = 2;
-constexpr int TMEM_COLS = 512;  // 7 x 64 used
+constexpr int A_SLICE = TM * KC;        // 4096 bytes
+constexpr int B_SLICE = TN * KC;        // 2048 bytes
+constexpr int A_BLOCK = S * A_SLICE;    // 28 KiB: one stage of the left operand
+constexpr int B_BLOCK = S * B_SLICE;    // 14 KiB
+constexpr int STAGE = A_BLOCK + B_BLOCK;
+constexpr int STAGES = 5;
+constexpr int THREADS = 256;            // 8 warps drain; lane 0 of warp 0 also loads and issues MMAs
+constexpr int DRAIN_WARPS = 8;
+constexpr int TMEM_COLS = 512;          // ND x TN
 constexpr long long WAIT_CYCLES = 2000000000LL;  // ~1 s at 1.9 GHz per wait
+constexpr int SPLIT_ROWS = 64;          // rows per split CTA
+// offset that turns the six lower bytes of x + C6 into digits + 128:
+// C6 = 128 (256^6 - 1) / 255
+constexpr long long C6 = 128LL * ((1LL << 48) - 1) / 255;
 }  // namespace oz
+
+// weight 2^(-12 - 8D) of digit diagonal D = 0..7
+__device__ constexpr double kDiagWeight[oz::ND] = {0x1p-12, 0x1p-20, 0x1p-28, 0x1p-36,
+                                                   0x1p-44, 0x1p-52, 0x1p-60, 0x1p-68};
 
 // ---------------------------------------------------------------------------
 // split
 
-__global__ void __launch_bounds__(256) ozaki_split_kernel(const OzSplitProblem* __restrict__ probs) {
+// gather byte `bb` of four words into one word (element j -> byte j)
+__device__ __forceinline__ uint32_t oz_gather(uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3, uint32_t bb) {
+  const uint32_t sel = bb | ((bb + 4u) << 4);
+  return __byte_perm(__byte_perm(w0, w1, sel), __byte_perm(w2, w3, sel), 0x5410);
+}
+
+__global__ void __launch_bounds__(256, 3) ozaki_split_kernel(const OzSplitProblem* __restrict__ probs) {
   const OzSplitProblem q = probs[blockIdx.y];
-  const int r0 = blockIdx.x * 32;
+  const int r0 = blockIdx.x * oz::SPLIT_ROWS;
   if (r0 >= q.rows_pad) return;
-  const int rr = threadIdx.x & 31, kg = threadIdx.x >> 5;  // 32 rows x 8 K groups
-  const int r = r0 + rr;
-  const bool live = r < q.rows;
-  __shared__ double red[8][33];
-  __shared__ int sh_e[32];
-  // pass 1: max over k of |re| + |im| (bounds |re|, |im| and |re + im|)
-  double mx = 0.0;
-  if (live)
-    for (int k = kg; k < q.cols; k += 8) {
-      cplx v = q.X[r * q.sr + k * q.sk];
-      mx = fmax(mx, fabs(v.x) + fabs(v.y));
+  __shared__ cplx tile[oz::SPLIT_ROWS][33];
+  __shared__ double red[4][oz::SPLIT_ROWS];
+  __shared__ int sh_e[oz::SPLIT_ROWS];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const bool rows_contig = q.sr == 1;
+  const int kch = q.k_pad / oz::KC;
+
+  // pass 1: row maxima of |re| + |im| (bounds |re|, |im| and |re + im|),
+  // streamed along whichever index is contiguous in memory
+  if (rows_contig) {
+    const int r = tid & 63, gr = r0 + r;
+    double mx = 0.0;
+    if (gr < q.rows)
+      for (int k = tid >> 6; k < q.cols; k += 4) {
+        const cplx v = q.X[(long long)gr + (long long)k * q.sk];
+        mx = fmax(mx, fabs(v.x) + fabs(v.y));
+      }
+    red[tid >> 6][r] = mx;
+    __syncthreads();
+    if (tid < oz::SPLIT_ROWS) {
+      const double m = fmax(fmax(red[0][tid], red[1][tid]), fmax(red[2][tid], red[3][tid]));
+      int e = 0;
+      if (m > 0.0) frexp(m, &e);  // m < 2^e
+      sh_e[tid] = e;
+      q.exps[r0 + tid] = e;
     }
-  red[kg][rr] = mx;
-  __syncthreads();
-  if (kg == 0) {
-    double m = red[0][rr];
-    for (int j = 1; j < 8; ++j) m = fmax(m, red[j][rr]);
-    int e = 0;
-    if (m > 0.0) frexp(m, &e);  // m < 2^e
-    sh_e[rr] = e;
-    if (r < q.rows_pad) q.exps[r] = e;
+  } else {
+    for (int j = 0; j < 8; ++j) {
+      const int r = warp + 8 * j, gr = r0 + r;
+      double mx = 0.0;
+      if (gr < q.rows)
+        for (int k = lane; k < q.cols; k += 32) {
+          const cplx v = q.X[(long long)gr * q.sr + k];
+          mx = fmax(mx, fabs(v.x) + fabs(v.y));
+        }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      if (lane == 0) {
+        int e = 0;
+        if (mx > 0.0) frexp(mx, &e);
+        sh_e[r] = e;
+        q.exps[r0 + r] = e;
+      }
+    }
   }
   __syncthreads();
-  const int e = sh_e[rr];
-  const size_t plane = (size_t)q.rows_pad * q.k_pad;
-  // pass 2: digits, 16 consecutive k per store
-  for (int kc = kg; kc * 16 < q.k_pad; kc += 8) {
-    int8_t dig[3][oz::S][16];
-#pragma unroll 1
-    for (int j = 0; j < 16; ++j) {
-      const int k = kc * 16 + j;
-      double comp[3] = {0.0, 0.0, 0.0};
-      if (live && k < q.cols) {
-        cplx v = q.X[r * q.sr + k * q.sk];
-        double re = v.x, im = q.conj ? -v.y : v.y;
-        comp[0] = re; comp[1] = im; comp[2] = re + im;
+
+  // pass 2: a warp owns 8 rows; lane = (row % 8) * 4 + k quad, so one warp
+  // store covers a 128-byte core matrix of one digit slice
+  const int rl = warp * 8 + (lane >> 2);
+  const int kq = lane & 3;
+  const int e = sh_e[rl];
+  // x = rint(v 2^(54 - e)), |x| <= 2^54, scaled in two exact power-of-two factors
+  const int sh = 54 - e;
+  const double f1 = ldexp(1.0, sh / 2), f2 = ldexp(1.0, sh - sh / 2);
+  const double fi = q.conj ? -f1 : f1;
+  const int TR = q.tile_rows;
+  const int grow = r0 + rl;
+  const int t = grow / TR, rt = grow % TR;
+  // left operand (128-row tiles): slice i at i * 4096, K halves 2048 apart;
+  // right operand (64-row tiles): the seven slices form one 448-row K-major
+  // matrix (row = 64 i + r), so slice i starts at i * 1024, K halves 7168 apart
+  const size_t slice = TR == oz::TM ? (size_t)TR * oz::KC : (size_t)TR * 16;
+  const size_t half = TR == oz::TM ? (size_t)TR * 16 : (size_t)oz::S * TR * 16;
+  const size_t block = (size_t)oz::S * TR * oz::KC;
+  const int ntiles = q.rows_pad / TR;
+  for (int c = 0; c < kch; ++c) {
+    // stage rows r0..r0+63, k = 32c..32c+31 (zeros outside)
+    const int kbase = c * oz::KC;
+    if (rows_contig) {
+      const int r = tid & 63, gr = r0 + r;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int kk = (tid >> 6) + 4 * j, gk = kbase + kk;
+        cplx v = make_double2(0.0, 0.0);
+        if (gr < q.rows && gk < q.cols) v = q.X[(long long)gr + (long long)gk * q.sk];
+        tile[r][kk] = v;
       }
+    } else {
+      const int kk = tid & 31, gk = kbase + kk;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int r = (tid >> 5) + 8 * j, gr = r0 + r;
+        cplx v = make_double2(0.0, 0.0);
+        if (gr < q.rows && gk < q.cols) v = q.X[(long long)gr * q.sr + gk];
+        tile[r][kk] = v;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      // offset fixed-point values x + C6 of re, im and re + im of 4 consecutive
+      // k: byte 6 is the top digit, bytes 5..0 are the lower digits + 128
+      uint32_t lo[3][4], hi[3][4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const cplx v = tile[rl][16 * h + 4 * kq + j];
+        const long long xr = __double2ll_rn(v.x * f1 * f2);
+        const long long xi = __double2ll_rn(v.y * fi * f2);
+        const long long x3[3] = {xr + oz::C6, xi + oz::C6, xr + xi + oz::C6};
+#pragma unroll
+        for (int p = 0; p < 3; ++p) {
+          lo[p][j] = (uint32_t)x3[p];
+          hi[p][j] = (uint32_t)((unsigned long long)x3[p] >> 32);
+        }
+      }
+      const size_t inrow = (size_t)h * half + (size_t)(rt >> 3) * 128 + (rt & 7) * 16 + 4 * kq;
 #pragma unroll
       for (int p = 0; p < 3; ++p) {
-        double y = ldexp(comp[p], 7 - e);  // |y| < 128
+        uint8_t* base = reinterpret_cast<uint8_t*>(q.slices) + ((size_t)(p * ntiles + t) * kch + c) * block + inrow;
 #pragma unroll
-        for (int s = 0; s < oz::S; ++s) {
-          double d = trunc(y);
-          dig[p][s][j] = static_cast<int8_t>(d);
-          y = (y - d) * 128.0;
+        for (int i = 0; i < oz::S; ++i) {
+          const int bi = oz::S - 1 - i;  // byte of digit slice i
+          uint32_t w = bi < 4 ? oz_gather(lo[p][0], lo[p][1], lo[p][2], lo[p][3], bi)
+                              : oz_gather(hi[p][0], hi[p][1], hi[p][2], hi[p][3], bi - 4);
+          if (i > 0) w ^= 0x80808080u;  // lower digits: byte - 128
+          *reinterpret_cast<uint32_t*>(base + i * slice) = w;
         }
       }
     }
-#pragma unroll
-    for (int p = 0; p < 3; ++p)
-#pragma unroll
-      for (int s = 0; s < oz::S; ++s) {
-        int4 pack;
-        int8_t* b = reinterpret_cast<int8_t*>(&pack);
-#pragma unroll
-        for (int j = 0; j < 16; ++j) b[j] = dig[p][s][j];
-        *reinterpret_cast<int4*>(q.slices + (size_t)(p * oz::S + s) * plane + (size_t)r * q.k_pad + kc * 16) = pack;
-      }
+    __syncthreads();
   }
 }
 
 // ---------------------------------------------------------------------------
-// MMA
+// product
 
 __device__ __forceinline__ uint32_t oz_smem(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -126,157 +219,244 @@ __device__ __forceinline__ uint64_t oz_desc(uint32_t saddr, uint32_t lbo, uint32
   return d;                // base offset 0, no swizzle
 }
 
-__device__ __forceinline__ void oz_cp16(uint32_t dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src));
+__device__ __forceinline__ bool oz_try(uint32_t mbar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\tselp.b32 %0, 1, 0, P1;\n\t}\n"
+      : "=r"(done)
+      : "r"(mbar), "r"(parity)
+      : "memory");
+  return done != 0;
 }
 
-// bounded wait for completion number `target` (1-based) of an mbarrier whose
-// completions we have seen `seen` of; returns false on time-out
-__device__ __forceinline__ bool oz_wait(uint32_t mbar, uint32_t& seen, uint32_t target) {
-  while (seen < target) {
-    uint32_t done = 0;
-    const long long t0 = clock64();
-    while (!done && clock64() - t0 < oz::WAIT_CYCLES) {
-      asm volatile(
-          "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\tselp.b32 %0, 1, 0, P1;\n\t}\n"
-          : "=r"(done)
-          : "r"(mbar), "r"(seen & 1u));
+// Bounded wait for the completion of the mbarrier phase of the given parity.
+// Returns false when another role raised the abort flag (watch) or after
+// WAIT_CYCLES, in which case it raises the flag and records the error.
+__device__ __forceinline__ bool oz_wait(uint32_t mbar, uint32_t parity, volatile int* abort_flag, int* err,
+                                        bool watch) {
+  const long long t0 = clock64();
+  while (!oz_try(mbar, parity)) {
+    if (watch && *abort_flag) return false;
+    if (clock64() - t0 > oz::WAIT_CYCLES) {
+      *abort_flag = 1;
+      atomicExch(err, 1);
+      return false;
     }
-    if (!done) return false;
-    ++seen;
   }
   return true;
 }
 
+__device__ __forceinline__ void oz_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
+}
+
+struct OzTile {
+  int prob, mt, nt, tiles_m, tiles_n, kch;
+};
+
+// tile t of a batched launch from the host-built map: x = problem, y = m tile
+// | n tile << 16, z = K chunks | m tiles << 16, w = n tiles (n fastest, so
+// that consecutive tiles share the left operand)
+__device__ __forceinline__ OzTile oz_tile(const int4* __restrict__ tile_map, int t) {
+  const int4 v = tile_map[t];
+  OzTile r;
+  r.prob = v.x;
+  r.mt = v.y & 0xFFFF;
+  r.nt = v.y >> 16;
+  r.kch = v.z & 0xFFFF;
+  r.tiles_m = v.z >> 16;
+  r.tiles_n = v.w;
+  return r;
+}
+
+// The MMAs of one stage: A digit slice i times the contiguous B digit slices
+// j0 .. j0 + nj - 1 (one N = 64 nj product) into the accumulators of the
+// diagonals D = i + j0 .. i + j0 + nj - 1. The listed order makes every
+// accumulator's first write one whose columns are all first writes ("init").
+struct OzMmaOp {
+  int i, j0, nj, init;
+};
+__device__ constexpr OzMmaOp kOzOps[12] = {{0, 0, 4, 1}, {0, 4, 3, 1}, {1, 0, 4, 0}, {1, 4, 2, 0},
+                                           {1, 6, 1, 1}, {2, 0, 4, 0}, {2, 4, 2, 0}, {3, 0, 4, 0},
+                                           {3, 4, 1, 0}, {4, 0, 4, 0}, {5, 0, 3, 0}, {6, 0, 2, 0}};
+
+// Persistent: CTA b computes tiles b, b + G, b + 2G, ... (G = gridDim.x); the
+// stage ring streams across tile boundaries, and the first product of the next
+// tile is issued before the epilogue of the current one.
 __global__ void __launch_bounds__(oz::THREADS, 1)
-    ozaki_mma_kernel(const OzMmaProblem* __restrict__ probs, const int* __restrict__ tile_start, int nprob,
+    ozaki_mma_kernel(const OzMmaProblem* __restrict__ probs, const int4* __restrict__ tile_map, int total_tiles,
                      int* __restrict__ err) {
   using namespace oz;
   extern __shared__ __align__(1024) unsigned char smem[];
-  __shared__ __align__(8) uint64_t mbar[STAGES];
-  __shared__ uint32_t tmem_base_sh;
-  __shared__ int eA_sh[TM], eB_sh[TN];
+  __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES], accf_bar, acce_bar, done_bar;
+  __shared__ uint32_t tmem_sh;
+  __shared__ int abort_sh;
+  volatile int* abort_flag = &abort_sh;
 
-  int bid = blockIdx.x;
-  int lo = 0, hi = nprob - 1;
-  while (lo < hi) {
-    int mid = (lo + hi + 1) >> 1;
-    if (tile_start[mid] <= bid) lo = mid; else hi = mid - 1;
-  }
-  const OzMmaProblem q = probs[lo];
-  const int t = bid - tile_start[lo];
-  const int tiles_m = q.m_pad / TM;
-  const int m0 = (t % tiles_m) * TM, n0 = (t / tiles_m) * TN;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int G = gridDim.x;
+  const int my_tiles = (int)blockIdx.x < total_tiles ? (total_tiles - (int)blockIdx.x + G - 1) / G : 0;
+  const long long my_products = (long long)my_tiles * NP;
 
   if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(oz_smem(&tmem_base_sh)),
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(oz_smem(&tmem_sh)),
                  "r"(TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
   }
   if (tid == 0) {
-    for (int s = 0; s < STAGES; ++s) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(oz_smem(&mbar[s])));
-    asm volatile("fence.mbarrier_init.release.cluster;" ::);
+    for (int s = 0; s < STAGES; ++s) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(oz_smem(&full_bar[s])));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(oz_smem(&empty_bar[s])));
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(oz_smem(&accf_bar)));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(oz_smem(&acce_bar)), "r"(DRAIN_WARPS));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(oz_smem(&done_bar)));
+    abort_sh = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  for (int i = tid; i < TM; i += THREADS) eA_sh[i] = q.eA[m0 + i];
-  for (int i = tid; i < TN; i += THREADS) eB_sh[i] = q.eB[n0 + i];
   asm volatile("tcgen05.fence::before_thread_sync;" ::);
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::);
-  const uint32_t tmem = tmem_base_sh;
-
-  const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
-  const int kch = q.k_pad / KC;
-  const int total = NP * kch;
-  const size_t planeA = (size_t)q.m_pad * q.k_pad, planeB = (size_t)q.n_pad * q.k_pad;
+  const uint32_t tmem = tmem_sh;
   const uint32_t sbase = oz_smem(smem);
-  uint32_t seen[STAGES] = {0, 0}, uses[STAGES] = {0, 0};
-  bool ok = true;
+  const bool leader = tid == 0;
 
-  // copy the seven A and B digit slices of iteration `it` into stage `st`
-  auto load = [&](int it, int st) {
-    const int p = it / kch, kc = it % kch;
-    const uint32_t sA = sbase + st * STAGE, sB = sA + S * A_SLICE;
-    for (int idx = tid; idx < S * TM * 2; idx += THREADS) {  // (slice, row, 16-byte half)
-      int s = idx / (TM * 2), rem = idx % (TM * 2), r = rem >> 1, h = rem & 1;
-      const int8_t* src = q.SA + (size_t)(p * S + s) * planeA + (size_t)(m0 + r) * q.k_pad + kc * KC + h * 16;
-      oz_cp16(sA + s * A_SLICE + h * (TM * 16) + (r >> 3) * 128 + (r & 7) * 16, src);
+  // ---- leader state: the load cursor (tile lq, product lp, chunk lc; global
+  // load count gl) runs up to STAGES loads ahead of the MMA cursor gm
+  int lq = 0, lp = 0, lc = 0;
+  long long gl = 0, gm = 0;
+  bool lvalid = my_tiles > 0;
+  OzTile lt = oz_tile(tile_map, lvalid ? (int)blockIdx.x : 0);
+  int last_use[STAGES];
+#pragma unroll
+  for (int s = 0; s < STAGES; ++s) last_use[s] = -1;
+  bool mma_ok = true;
+  long long next_issue = 0;  // first product whose MMAs are not issued yet
+
+  auto issue_load = [&]() {
+    const OzMmaProblem& q = probs[lt.prob];
+    const int st = (int)(gl % STAGES);
+    const int8_t* srcA = q.SA + ((size_t)(lp * lt.tiles_m + lt.mt) * lt.kch + lc) * A_BLOCK;
+    const int8_t* srcB = q.SB + ((size_t)(lp * lt.tiles_n + lt.nt) * lt.kch + lc) * B_BLOCK;
+    const uint32_t fb = oz_smem(&full_bar[st]);
+    const uint32_t dA = sbase + st * STAGE, dB = dA + A_BLOCK;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb), "r"(STAGE) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dA),
+                 "l"(srcA), "r"(A_BLOCK), "r"(fb)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dB),
+                 "l"(srcB), "r"(B_BLOCK), "r"(fb)
+                 : "memory");
+    last_use[st] = (int)(gl / STAGES);
+    ++gl;
+    if (++lc == lt.kch) {
+      lc = 0;
+      if (++lp == NP) {
+        lp = 0;
+        if (++lq == my_tiles) lvalid = false;
+        else lt = oz_tile(tile_map, (int)blockIdx.x + lq * G);
+      }
     }
-    for (int idx = tid; idx < S * TN * 2; idx += THREADS) {
-      int s = idx / (TN * 2), rem = idx % (TN * 2), r = rem >> 1, h = rem & 1;
-      const int8_t* src = q.SB + (size_t)(p * S + s) * planeB + (size_t)(n0 + r) * q.k_pad + kc * KC + h * 16;
-      oz_cp16(sB + s * B_SLICE + h * (TN * 16) + (r >> 3) * 128 + (r & 7) * 16, src);
-    }
-    asm volatile("cp.async.commit_group;\n" ::);
   };
 
-  // FP64 accumulators of this thread: tile row 32*(warp%4)+lane, columns 32*(warp/4) + j
-  double cr[32], ci[32];
-#pragma unroll
-  for (int j = 0; j < 32; ++j) { cr[j] = 0.0; ci[j] = 0.0; }
-  const int qd = warp & 3, half = warp >> 2;
-
-  if (total > 0) load(0, 0);
-  for (int it = 0; it < total && ok; ++it) {
-    const int st = it & 1;
-    if (it + 1 < total) {
-      const int ns = (it + 1) & 1;
-      // MMAs of it-1 done (the decision is made CTA-uniform before anyone leaves the loop)
-      ok = __syncthreads_and(oz_wait(oz_smem(&mbar[ns]), seen[ns], uses[ns]) ? 1 : 0) != 0;
-      if (!ok) break;
-      load(it + 1, ns);
-      asm volatile("cp.async.wait_group 1;\n" ::);
-    } else {
-      asm volatile("cp.async.wait_group 0;\n" ::);
+  // issue every stage of global product P (tile P / NP, real product P % NP)
+  auto issue_product = [&](long long P) {
+    if (P > 0 && !oz_wait(oz_smem(&acce_bar), (uint32_t)((P - 1) & 1), abort_flag, err, true)) {
+      mma_ok = false;
+      return;
     }
-    asm volatile("fence.proxy.async.shared::cta;" ::);
-    __syncthreads();
-    const int p = it / kch, kc = it % kch;
-    if (tid == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::);
-      const uint32_t sA = sbase + st * STAGE, sB = sA + S * A_SLICE;
-      for (int d = 2; d <= S + 1; ++d) {
-        bool first = true;
-        for (int s = 1; s <= S; ++s) {
-          const int tt = d - s;
-          if (tt < 1 || tt > S) continue;
-          uint64_t da = oz_desc(sA + (s - 1) * A_SLICE, TM * 16, 128);
-          uint64_t db = oz_desc(sB + (tt - 1) * B_SLICE, TN * 16, 128);
-          uint32_t acc = (kc == 0 && first) ? 0u : 1u;
-          first = false;
-          asm volatile(
-              "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-              "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
-                  tmem + (uint32_t)((d - 2) * TN)),
-              "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
-        }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::);
+    const OzTile mtl = oz_tile(tile_map, (int)blockIdx.x + (int)(P / NP) * G);
+    for (int c = 0; c < mtl.kch; ++c) {
+      const int st = (int)(gm % STAGES);
+      const uint32_t n = (uint32_t)(gm / STAGES);
+      if (!oz_wait(oz_smem(&full_bar[st]), n & 1, abort_flag, err, true)) {
+        mma_ok = false;
+        return;
       }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-          oz_smem(&mbar[st])));
+      asm volatile("tcgen05.fence::after_thread_sync;" ::);
+      const uint32_t sA = sbase + st * STAGE, sB = sA + A_BLOCK;
+      const uint64_t dA0 = oz_desc(sA, TM * 16, 128), dB0 = oz_desc(sB, S * TN * 16, 128);
+#pragma unroll
+      for (int o = 0; o < 12; ++o) {
+        const OzMmaOp op = kOzOps[o];
+        const uint32_t idesc =
+            (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(op.nj * TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+        // the start-address field of a descriptor is addr >> 4
+        const uint64_t da = dA0 + (uint64_t)(op.i * (A_SLICE >> 4));
+        const uint64_t db = dB0 + (uint64_t)(op.j0 * (TN * 16 >> 4));
+        const uint32_t acc = (c == 0 && op.init) ? 0u : 1u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+                tmem + (uint32_t)((op.i + op.j0) * TN)),
+            "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+      }
+      oz_commit(oz_smem(&empty_bar[st]));
+      if (c == mtl.kch - 1) oz_commit(oz_smem(&accf_bar));
+      // refill the stage of gm - 1 once its MMAs are done
+      if (gm >= 1 && lvalid) {
+        const long long pg = gm - 1;
+        if (!oz_wait(oz_smem(&empty_bar[pg % STAGES]), (uint32_t)((pg / STAGES) & 1), abort_flag, err, true)) {
+          mma_ok = false;
+          return;
+        }
+        issue_load();
+      }
+      ++gm;
     }
-    uses[st] += 1;
-    if (kc == kch - 1) {
-      // product p finished: drain the seven accumulators into FP64
-      ok = __syncthreads_and(oz_wait(oz_smem(&mbar[st]), seen[st], uses[st]) ? 1 : 0) != 0;
-      if (!ok) break;
+  };
+
+  if (leader)
+    while (lvalid && gl < STAGES) issue_load();
+
+  // ---- all eight warps: drain each product, then the tile epilogue; warp w
+  // reads TMEM lanes 32 (w % 4).. and columns 32 (w / 4)..
+  const int qd = warp & 3, hh = warp >> 2;
+  bool ok = true;
+  for (int q = 0; q < my_tiles && ok; ++q) {
+    double cr[32], ci[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) { cr[j] = 0.0; ci[j] = 0.0; }
+    for (int p = 0; p < NP; ++p) {
+      const long long P = (long long)q * NP + p;
+      if (leader && mma_ok && next_issue == P) {
+        issue_product(P);
+        ++next_issue;
+      }
+      __syncwarp();
+      const bool got = oz_wait(oz_smem(&accf_bar), (uint32_t)(P & 1), abort_flag, err, true);
+      if (!__all_sync(0xffffffffu, got)) {
+        ok = false;
+        break;
+      }
       asm volatile("tcgen05.fence::after_thread_sync;" ::);
       const double sr = (p == 2) ? 0.0 : (p == 0 ? 1.0 : -1.0);  // P1 -> +Re, P2 -> -Re
       const double si = (p == 2) ? 1.0 : -1.0;                   // P3 -> +Im, P1, P2 -> -Im
 #pragma unroll
       for (int c8 = 0; c8 < 4; ++c8) {
-        double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        double v[8];
 #pragma unroll
-        for (int d = 0; d < S; ++d) {
-          uint32_t x[8];
-          uint32_t addr = tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(d * TN + half * 32 + c8 * 8);
-          asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                       : "=r"(x[0]), "=r"(x[1]), "=r"(x[2]), "=r"(x[3]), "=r"(x[4]), "=r"(x[5]), "=r"(x[6]),
-                         "=r"(x[7])
-                       : "r"(addr));
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::);
-          const double w = ldexp(1.0, -7 * (d + 2));
+        for (int j = 0; j < 8; ++j) v[j] = 0.0;
 #pragma unroll
-          for (int j = 0; j < 8; ++j) v[j] = fma((double)(int32_t)x[j], w, v[j]);
+        for (int g = 0; g < 2; ++g) {  // four diagonals per TMEM round trip
+          uint32_t x[4][8];
+#pragma unroll
+          for (int dd = 0; dd < 4; ++dd) {
+            const int d = 4 * g + dd;
+            const uint32_t addr = tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(d * TN + hh * 32 + c8 * 8);
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                         : "=r"(x[dd][0]), "=r"(x[dd][1]), "=r"(x[dd][2]), "=r"(x[dd][3]), "=r"(x[dd][4]),
+                           "=r"(x[dd][5]), "=r"(x[dd][6]), "=r"(x[dd][7])
+                         : "r"(addr));
+          }
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+          for (int dd = 0; dd < 4; ++dd) {
+            const double w = kDiagWeight[4 * g + dd];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) v[j] = fma((double)(int32_t)x[dd][j], w, v[j]);
+          }
         }
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
@@ -285,53 +465,73 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
         }
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::);
-      __syncthreads();  // accumulators free for the next product
+      __syncwarp();
+      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(oz_smem(&acce_bar)) : "memory");
     }
-  }
-
-  if (!ok) {
-    if (tid == 0) atomicExch(err, 1);
-    // bounded wait for the MMAs this CTA issued, then release TMEM
-    for (int s = 0; s < STAGES; ++s) oz_wait(oz_smem(&mbar[s]), seen[s], uses[s]);
-  } else {
+    if (!ok) break;
+    // the next tile's first product goes to the tensor cores before this epilogue
+    if (leader && mma_ok && next_issue < my_products) {
+      issue_product(next_issue);
+      ++next_issue;
+    }
+    __syncwarp();
     // C = alpha * 2^(eA + eB) (Re, Im) + beta * Cin + diag * I
+    const OzTile tl = oz_tile(tile_map, (int)blockIdx.x + q * G);
+    const OzMmaProblem& pq = probs[tl.prob];
     const int row = qd * 32 + lane;
-    const int r = m0 + row;
-    const cplx dg = q.diag_ptr ? *q.diag_ptr : q.diag;
-    const bool has_cin = q.Cin && (q.beta.x != 0.0 || q.beta.y != 0.0);
-    if (r < q.m) {
+    const int r = tl.mt * TM + row;
+    if (r < pq.m) {
+      const cplx dg = pq.diag_ptr ? *pq.diag_ptr : pq.diag;
+      const bool has_cin = pq.Cin && (pq.beta.x != 0.0 || pq.beta.y != 0.0);
+      const int er = pq.eA[r];
 #pragma unroll
       for (int j = 0; j < 32; ++j) {
-        const int cl = half * 32 + j;
-        const int c = n0 + cl;
-        if (c >= q.n) continue;
-        const int e = eA_sh[row] + eB_sh[cl];
-        const double xr = ldexp(cr[j], e), xi = ldexp(ci[j], e);
-        cplx v;
-        v.x = q.alpha.x * xr - q.alpha.y * xi;
-        v.y = q.alpha.x * xi + q.alpha.y * xr;
-        if (has_cin) {
-          cplx b = q.Cin[r + (size_t)c * q.ldcin];
-          v.x += q.beta.x * b.x - q.beta.y * b.y;
-          v.y += q.beta.x * b.y + q.beta.y * b.x;
+        const int c = tl.nt * TN + hh * 32 + j;
+        if (c >= pq.n) continue;
+        const int e = er + pq.eB[c];
+        double xr, xi;
+        if (e >= -1022 && e <= 1023) {  // 2^e as a normal double
+          const double sc = __longlong_as_double((long long)(e + 1023) << 52);
+          xr = cr[j] * sc;
+          xi = ci[j] * sc;
+        } else {
+          xr = ldexp(cr[j], e);
+          xi = ldexp(ci[j], e);
         }
-        if (r == c) { v.x += dg.x; v.y += dg.y; }
-        q.C[r + (size_t)c * q.ldc] = v;
+        cplx v;
+        v.x = pq.alpha.x * xr - pq.alpha.y * xi;
+        v.y = pq.alpha.x * xi + pq.alpha.y * xr;
+        if (has_cin) {
+          const cplx b = pq.Cin[r + (size_t)c * pq.ldcin];
+          v.x += pq.beta.x * b.x - pq.beta.y * b.y;
+          v.y += pq.beta.x * b.y + pq.beta.y * b.x;
+        }
+        if (r == c) {
+          v.x += dg.x;
+          v.y += dg.y;
+        }
+        pq.C[r + (size_t)c * pq.ldc] = v;
       }
     }
   }
+  if (leader) {
+    // all MMAs of this CTA complete, and every issued copy has landed, before
+    // TMEM is released and the CTA exits
+    oz_commit(oz_smem(&done_bar));
+    oz_wait(oz_smem(&done_bar), 0, abort_flag, err, false);
+    for (int s = 0; s < STAGES; ++s)
+      if (last_use[s] >= 0) oz_wait(oz_smem(&full_bar[s]), (uint32_t)(last_use[s] & 1), abort_flag, err, false);
+  }
+  __syncwarp();
   asm volatile("tcgen05.fence::before_thread_sync;" ::);
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::);
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+  }
 }
 
-// 86 KB of stages; the request is raised to 120 KB so that one CTA (and its
-// 512 TMEM columns) owns an SM at a time instead of a second CTA blocking in
-// tcgen05.alloc.
-size_t ozaki_mma_smem_bytes() {
-  size_t need = (size_t)oz::STAGES * oz::STAGE;
-  return need < 120 * 1024 ? 120 * 1024 : need;
-}
+size_t ozaki_mma_smem_bytes() { return (size_t)oz::STAGES * oz::STAGE; }
 
 cudaError_t ozaki_prepare() {
   return cudaFuncSetAttribute(ozaki_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -340,16 +540,23 @@ cudaError_t ozaki_prepare() {
 
 cudaError_t launch_ozaki_split(const void* probs, int nprob, int max_rows_pad, cudaStream_t st) {
   if (nprob <= 0) return cudaSuccess;
-  dim3 grid((max_rows_pad + 31) / 32, nprob);
+  dim3 grid((max_rows_pad + oz::SPLIT_ROWS - 1) / oz::SPLIT_ROWS, nprob);
   ozaki_split_kernel<<<grid, 256, 0, st>>>(static_cast<const OzSplitProblem*>(probs));
   return cudaGetLastError();
 }
 
-cudaError_t launch_ozaki_mma(const void* probs, const int* tile_start, int nprob, int total_tiles, int* err,
-                             cudaStream_t st) {
-  if (nprob <= 0 || total_tiles <= 0) return cudaSuccess;
-  ozaki_mma_kernel<<<total_tiles, oz::THREADS, ozaki_mma_smem_bytes(), st>>>(
-      static_cast<const OzMmaProblem*>(probs), tile_start, nprob, err);
+cudaError_t launch_ozaki_mma(const void* probs, const void* tile_map, int total_tiles, int* err, cudaStream_t st) {
+  if (total_tiles <= 0) return cudaSuccess;
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+  }
+  const int grid = total_tiles < sms ? total_tiles : sms;
+  ozaki_mma_kernel<<<grid, oz::THREADS, ozaki_mma_smem_bytes(), st>>>(
+      static_cast<const OzMmaProblem*>(probs), static_cast<const int4*>(tile_map), total_tiles, err);
   return cudaGetLastError();
 }
 
