@@ -28,8 +28,9 @@
 //     multiplies a left digit slice by several right digit slices at once;
 //   * the product kernel (persistent, one CTA per SM, 128 x 64 output tiles,
 //     256 threads): one thread streams stages with cp.async.bulk into a 5-deep
-//     mbarrier ring and issues the 12 MMAs (N = 64..256) of each stage into
-//     eight TMEM accumulators (one per digit diagonal, 8 x 64 columns); after
+//     mbarrier ring, refilling each slot as its MMAs retire; another issues the
+//     12 MMAs (N = 64..256) of each stage into eight TMEM accumulators (one per
+//     digit diagonal, 8 x 64 columns); after
 //     each real product the eight warps drain the accumulators into FP64
 //     registers, and at the end of a tile they write
 //     C = alpha A B + beta Cin + diag I while the next tile's first product is
@@ -54,7 +55,7 @@ constexpr int A_BLOCK = S * A_SLICE;    // 28 KiB: one stage of the left operand
 constexpr int B_BLOCK = S * B_SLICE;    // 14 KiB
 constexpr int STAGE = A_BLOCK + B_BLOCK;
 constexpr int STAGES = 5;
-constexpr int THREADS = 256;            // 8 warps drain; lane 0 of warp 0 also loads and issues MMAs
+constexpr int THREADS = 256;            // 8 warps drain; lane 0 of warps 0 / 1 also issue MMAs / loads
 constexpr int DRAIN_WARPS = 8;
 constexpr int TMEM_COLS = 512;          // ND x TN
 constexpr long long WAIT_CYCLES = 2000000000LL;  // ~1 s at 1.9 GHz per wait
@@ -64,9 +65,18 @@ constexpr int SPLIT_ROWS = 64;          // rows per split CTA
 constexpr long long C6 = 128LL * ((1LL << 48) - 1) / 255;
 }  // namespace oz
 
-// weight 2^(-12 - 8D) of digit diagonal D = 0..7
-__device__ constexpr double kDiagWeight[oz::ND] = {0x1p-12, 0x1p-20, 0x1p-28, 0x1p-36,
-                                                   0x1p-44, 0x1p-52, 0x1p-60, 0x1p-68};
+// weight 2^(-12 - 8D) of digit diagonal D = 0..7 (a compile-time constant)
+__host__ __device__ constexpr double oz_diag_weight(int D) {
+  double w = 0x1p-12;
+  for (int d = 0; d < D; ++d) w *= 0x1p-8;
+  return w;
+}
+
+// exact int32 -> double on the FP64 pipe: the bits 0x43300000:(x ^ 2^31) are
+// 2^52 + 2^31 + x, from which one exact subtraction leaves x
+__device__ __forceinline__ double oz_i2d(uint32_t x) {
+  return __hiloint2double(0x43300000, (int)(x ^ 0x80000000u)) - 4503601774854144.0;
+}
 
 // ---------------------------------------------------------------------------
 // split
@@ -234,6 +244,7 @@ __device__ __forceinline__ bool oz_try(uint32_t mbar, uint32_t parity) {
 // WAIT_CYCLES, in which case it raises the flag and records the error.
 __device__ __forceinline__ bool oz_wait(uint32_t mbar, uint32_t parity, volatile int* abort_flag, int* err,
                                         bool watch) {
+  if (oz_try(mbar, parity)) return true;
   const long long t0 = clock64();
   while (!oz_try(mbar, parity)) {
     if (watch && *abort_flag) return false;
@@ -244,6 +255,30 @@ __device__ __forceinline__ bool oz_wait(uint32_t mbar, uint32_t parity, volatile
     }
   }
   return true;
+}
+
+// The same wait for a whole warp that has nothing else to do: lane 0 polls
+// with a back-off, so that idle warps leave the issue slots to the thread that
+// feeds the tensor cores; the result is uniform across the warp.
+__device__ __forceinline__ bool oz_wait_warp(uint32_t mbar, uint32_t parity, volatile int* abort_flag, int* err) {
+  int ok = 0;
+  if ((threadIdx.x & 31) == 0) {
+    const long long t0 = clock64();
+    while (true) {
+      if (oz_try(mbar, parity)) {
+        ok = 1;
+        break;
+      }
+      if (*abort_flag) break;
+      if (clock64() - t0 > oz::WAIT_CYCLES) {
+        *abort_flag = 1;
+        atomicExch(err, 1);
+        break;
+      }
+      __nanosleep(256);
+    }
+  }
+  return __shfl_sync(0xffffffffu, ok, 0) != 0;
 }
 
 __device__ __forceinline__ void oz_commit(uint32_t mbar) {
@@ -269,16 +304,42 @@ __device__ __forceinline__ OzTile oz_tile(const int4* __restrict__ tile_map, int
   return r;
 }
 
-// The MMAs of one stage: A digit slice i times the contiguous B digit slices
-// j0 .. j0 + nj - 1 (one N = 64 nj product) into the accumulators of the
-// diagonals D = i + j0 .. i + j0 + nj - 1. The listed order makes every
-// accumulator's first write one whose columns are all first writes ("init").
-struct OzMmaOp {
-  int i, j0, nj, init;
-};
-__device__ constexpr OzMmaOp kOzOps[12] = {{0, 0, 4, 1}, {0, 4, 3, 1}, {1, 0, 4, 0}, {1, 4, 2, 0},
-                                           {1, 6, 1, 1}, {2, 0, 4, 0}, {2, 4, 2, 0}, {3, 0, 4, 0},
-                                           {3, 4, 1, 0}, {4, 0, 4, 0}, {5, 0, 3, 0}, {6, 0, 2, 0}};
+// One MMA of a stage: A digit slice I times the contiguous B digit slices
+// J0 .. J0 + NJ - 1 (one N = 64 NJ product) into the accumulators of the
+// diagonals D = I + J0 .. I + J0 + NJ - 1. INIT marks the MMAs that write
+// accumulators first (all of whose columns are first writes); compile-time
+// operands keep the issuing thread at one instruction sequence per MMA.
+template <int I, int J0, int NJ, int INIT>
+__device__ __forceinline__ void oz_mma(uint32_t tmem, uint64_t dA0, uint64_t dB0, bool first_chunk) {
+  constexpr uint32_t idesc =
+      (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NJ * oz::TN >> 3) << 17) | ((uint32_t)(oz::TM >> 4) << 24);
+  // the start-address field of a descriptor is addr >> 4
+  const uint64_t da = dA0 + (uint64_t)(I * (oz::A_SLICE >> 4));
+  const uint64_t db = dB0 + (uint64_t)(J0 * (oz::TN * 16 >> 4));
+  const uint32_t acc = (INIT && first_chunk) ? 0u : 1u;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+          tmem + (uint32_t)((I + J0) * oz::TN)),
+      "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+// The 34 digit pairs (i + j <= 7) of a stage as 12 MMAs; the order makes every
+// accumulator's first write an INIT one.
+__device__ __forceinline__ void oz_stage_mmas(uint32_t tmem, uint64_t dA0, uint64_t dB0, bool first_chunk) {
+  oz_mma<0, 0, 4, 1>(tmem, dA0, dB0, first_chunk);
+  oz_mma<0, 4, 3, 1>(tmem, dA0, dB0, first_chunk);
+  oz_mma<1, 0, 4, 0>(tmem, dA0, dB0, first_chunk);
+  oz_mma<1, 4, 2, 0>(tmem, dA0, dB0, first_chunk);
+  oz_mma<1, 6, 1, 1>(tmem, dA0, dB0, first_chunk);
+  oz_mma<2, 0, 4, 0>(tmem, dA0, dB0, first_chunk);
+  oz_mma<2, 4, 2, 0>(tmem, dA0, dB0, first_chunk);
+  oz_mma<3, 0, 4, 0>(tmem, dA0, dB0, first_chunk);
+  oz_mma<3, 4, 1, 0>(tmem, dA0, dB0, first_chunk);
+  oz_mma<4, 0, 4, 0>(tmem, dA0, dB0, first_chunk);
+  oz_mma<5, 0, 3, 0>(tmem, dA0, dB0, first_chunk);
+  oz_mma<6, 0, 2, 0>(tmem, dA0, dB0, first_chunk);
+}
 
 // Persistent: CTA b computes tiles b, b + G, b + 2G, ... (G = gridDim.x); the
 // stage ring streams across tile boundaries, and the first product of the next
@@ -319,96 +380,109 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
   asm volatile("tcgen05.fence::after_thread_sync;" ::);
   const uint32_t tmem = tmem_sh;
   const uint32_t sbase = oz_smem(smem);
-  const bool leader = tid == 0;
+  // Lane 0 of warp 0 issues the MMAs; lane 0 of warp 1 streams the stages.
+  const bool mma_thread = tid == 0, load_thread = tid == 32;
 
-  // ---- leader state: the load cursor (tile lq, product lp, chunk lc; global
-  // load count gl) runs up to STAGES loads ahead of the MMA cursor gm
-  int lq = 0, lp = 0, lc = 0;
-  long long gl = 0, gm = 0;
+  // ---- load thread. Load cursor: tile lq, product lp, chunk lc, ring slot
+  // ls; refill cursor: the slot rs (phase rph) whose MMAs retire next. All
+  // counters are small ints (no division on the issue paths).
+  const uint32_t full0 = oz_smem(&full_bar[0]), empty0 = oz_smem(&empty_bar[0]);
+  int lq = 0, lp = 0, lc = 0, ls = 0, rs = 0;
+  uint32_t rph = 0;
+  uint32_t used = 0, last_ph = 0;  // per slot: ever loaded, phase parity of its last load
   bool lvalid = my_tiles > 0;
   OzTile lt = oz_tile(tile_map, lvalid ? (int)blockIdx.x : 0);
-  int last_use[STAGES];
-#pragma unroll
-  for (int s = 0; s < STAGES; ++s) last_use[s] = -1;
-  bool mma_ok = true;
-  long long next_issue = 0;  // first product whose MMAs are not issued yet
+  const int8_t* la = nullptr;  // next A / B stage source of the load cursor
+  const int8_t* lb = nullptr;
+  auto load_product_base = [&]() {
+    const OzMmaProblem& q = probs[lt.prob];
+    la = q.SA + (size_t)(lp * lt.tiles_m + lt.mt) * lt.kch * A_BLOCK;
+    lb = q.SB + (size_t)(lp * lt.tiles_n + lt.nt) * lt.kch * B_BLOCK;
+  };
+  if (load_thread && lvalid) load_product_base();
+  bool load_ok = true, mma_ok = true;
+  long long next_issue = 0, next_refill = 0;  // first product not issued / not refilled yet
 
   auto issue_load = [&]() {
-    const OzMmaProblem& q = probs[lt.prob];
-    const int st = (int)(gl % STAGES);
-    const int8_t* srcA = q.SA + ((size_t)(lp * lt.tiles_m + lt.mt) * lt.kch + lc) * A_BLOCK;
-    const int8_t* srcB = q.SB + ((size_t)(lp * lt.tiles_n + lt.nt) * lt.kch + lc) * B_BLOCK;
-    const uint32_t fb = oz_smem(&full_bar[st]);
-    const uint32_t dA = sbase + st * STAGE, dB = dA + A_BLOCK;
+    const uint32_t fb = full0 + ls * 8;
+    const uint32_t dA = sbase + ls * STAGE, dB = dA + A_BLOCK;
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb), "r"(STAGE) : "memory");
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dA),
-                 "l"(srcA), "r"(A_BLOCK), "r"(fb)
+                 "l"(la), "r"(A_BLOCK), "r"(fb)
                  : "memory");
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dB),
-                 "l"(srcB), "r"(B_BLOCK), "r"(fb)
+                 "l"(lb), "r"(B_BLOCK), "r"(fb)
                  : "memory");
-    last_use[st] = (int)(gl / STAGES);
-    ++gl;
+    // phase parity of this load of slot ls: flips on every reuse of the slot
+    const uint32_t bit = 1u << ls;
+    last_ph = (used & bit) ? (last_ph ^ bit) : (last_ph & ~bit);
+    used |= bit;
+    ls = ls + 1 == STAGES ? 0 : ls + 1;
+    la += A_BLOCK;
+    lb += B_BLOCK;
     if (++lc == lt.kch) {
       lc = 0;
       if (++lp == NP) {
         lp = 0;
-        if (++lq == my_tiles) lvalid = false;
-        else lt = oz_tile(tile_map, (int)blockIdx.x + lq * G);
+        if (++lq == my_tiles) {
+          lvalid = false;
+          return;
+        }
+        lt = oz_tile(tile_map, (int)blockIdx.x + lq * G);
       }
+      load_product_base();
     }
   };
 
-  // issue every stage of global product P (tile P / NP, real product P % NP)
+  // refill, stage by stage as the MMAs of global product P retire, the slots
+  // with the next stages of the load cursor
+  int rkch = 0;
+  auto refill_product = [&](long long P) {
+    if (P % NP == 0) rkch = oz_tile(tile_map, (int)blockIdx.x + (int)(P / NP) * G).kch;
+    for (int c = 0; c < rkch; ++c) {
+      if (!oz_wait(empty0 + rs * 8, rph, abort_flag, err, true)) {
+        load_ok = false;
+        return;
+      }
+      if (++rs == STAGES) {
+        rs = 0;
+        rph ^= 1u;
+      }
+      if (lvalid) issue_load();
+    }
+  };
+
+  // ---- MMA thread: every stage of global product P (tile P / NP, real product
+  // P % NP); ring slot ms with its full-barrier phase mph
+  const uint64_t descA0 = oz_desc(sbase, TM * 16, 128), descB0 = oz_desc(sbase + A_BLOCK, S * TN * 16, 128);
+  int ms = 0, mkch = 0;
+  uint32_t mph = 0;
   auto issue_product = [&](long long P) {
     if (P > 0 && !oz_wait(oz_smem(&acce_bar), (uint32_t)((P - 1) & 1), abort_flag, err, true)) {
       mma_ok = false;
       return;
     }
     asm volatile("tcgen05.fence::after_thread_sync;" ::);
-    const OzTile mtl = oz_tile(tile_map, (int)blockIdx.x + (int)(P / NP) * G);
-    for (int c = 0; c < mtl.kch; ++c) {
-      const int st = (int)(gm % STAGES);
-      const uint32_t n = (uint32_t)(gm / STAGES);
-      if (!oz_wait(oz_smem(&full_bar[st]), n & 1, abort_flag, err, true)) {
+    if (P % NP == 0) mkch = oz_tile(tile_map, (int)blockIdx.x + (int)(P / NP) * G).kch;
+    for (int c = 0; c < mkch; ++c) {
+      if (!oz_wait(full0 + ms * 8, mph, abort_flag, err, true)) {
         mma_ok = false;
         return;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::);
-      const uint32_t sA = sbase + st * STAGE, sB = sA + A_BLOCK;
-      const uint64_t dA0 = oz_desc(sA, TM * 16, 128), dB0 = oz_desc(sB, S * TN * 16, 128);
-#pragma unroll
-      for (int o = 0; o < 12; ++o) {
-        const OzMmaOp op = kOzOps[o];
-        const uint32_t idesc =
-            (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(op.nj * TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
-        // the start-address field of a descriptor is addr >> 4
-        const uint64_t da = dA0 + (uint64_t)(op.i * (A_SLICE >> 4));
-        const uint64_t db = dB0 + (uint64_t)(op.j0 * (TN * 16 >> 4));
-        const uint32_t acc = (c == 0 && op.init) ? 0u : 1u;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
-                tmem + (uint32_t)((op.i + op.j0) * TN)),
-            "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+      const uint64_t soff = (uint64_t)(ms * (STAGE >> 4));
+      oz_stage_mmas(tmem, descA0 + soff, descB0 + soff, c == 0);
+      oz_commit(empty0 + ms * 8);
+      if (c == mkch - 1) oz_commit(oz_smem(&accf_bar));
+      if (++ms == STAGES) {
+        ms = 0;
+        mph ^= 1u;
       }
-      oz_commit(oz_smem(&empty_bar[st]));
-      if (c == mtl.kch - 1) oz_commit(oz_smem(&accf_bar));
-      // refill the stage of gm - 1 once its MMAs are done
-      if (gm >= 1 && lvalid) {
-        const long long pg = gm - 1;
-        if (!oz_wait(oz_smem(&empty_bar[pg % STAGES]), (uint32_t)((pg / STAGES) & 1), abort_flag, err, true)) {
-          mma_ok = false;
-          return;
-        }
-        issue_load();
-      }
-      ++gm;
     }
   };
 
-  if (leader)
-    while (lvalid && gl < STAGES) issue_load();
+  if (load_thread)
+    for (int i = 0; i < STAGES && lvalid; ++i) issue_load();
 
   // ---- all eight warps: drain each product, then the tile epilogue; warp w
   // reads TMEM lanes 32 (w % 4).. and columns 32 (w / 4)..
@@ -420,13 +494,16 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
     for (int j = 0; j < 32; ++j) { cr[j] = 0.0; ci[j] = 0.0; }
     for (int p = 0; p < NP; ++p) {
       const long long P = (long long)q * NP + p;
-      if (leader && mma_ok && next_issue == P) {
+      if (mma_thread && mma_ok && next_issue == P) {
         issue_product(P);
         ++next_issue;
       }
+      if (load_thread && load_ok && next_refill == P) {
+        refill_product(P);
+        ++next_refill;
+      }
       __syncwarp();
-      const bool got = oz_wait(oz_smem(&accf_bar), (uint32_t)(P & 1), abort_flag, err, true);
-      if (!__all_sync(0xffffffffu, got)) {
+      if (!oz_wait_warp(oz_smem(&accf_bar), (uint32_t)(P & 1), abort_flag, err)) {
         ok = false;
         break;
       }
@@ -439,7 +516,7 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
 #pragma unroll
         for (int j = 0; j < 8; ++j) v[j] = 0.0;
 #pragma unroll
-        for (int g = 0; g < 2; ++g) {  // four diagonals per TMEM round trip
+        for (int g = 0; g < ND / 4; ++g) {  // four diagonals per TMEM round trip
           uint32_t x[4][8];
 #pragma unroll
           for (int dd = 0; dd < 4; ++dd) {
@@ -453,9 +530,9 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
           asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
           for (int dd = 0; dd < 4; ++dd) {
-            const double w = kDiagWeight[4 * g + dd];
+            const double w = oz_diag_weight(4 * g + dd);
 #pragma unroll
-            for (int j = 0; j < 8; ++j) v[j] = fma((double)(int32_t)x[dd][j], w, v[j]);
+            for (int j = 0; j < 8; ++j) v[j] = fma(oz_i2d(x[dd][j]), w, v[j]);
           }
         }
 #pragma unroll
@@ -469,59 +546,79 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
       if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(oz_smem(&acce_bar)) : "memory");
     }
     if (!ok) break;
-    // the next tile's first product goes to the tensor cores before this epilogue
-    if (leader && mma_ok && next_issue < my_products) {
+    // the next tile's first product goes to the tensor cores before this
+    // epilogue (its first STAGES stages are loaded already; the load thread
+    // refills after its own epilogue)
+    if (mma_thread && mma_ok && next_issue < my_products) {
       issue_product(next_issue);
       ++next_issue;
     }
     __syncwarp();
-    // C = alpha * 2^(eA + eB) (Re, Im) + beta * Cin + diag * I
+    // C = alpha * 2^(eA + eB) (Re, Im) + beta * Cin + diag * I. The problem's
+    // fields go to registers first and every group of eight columns loads
+    // its inputs before its stores, so that no load waits behind a store
+    // that might alias it.
     const OzTile tl = oz_tile(tile_map, (int)blockIdx.x + q * G);
-    const OzMmaProblem& pq = probs[tl.prob];
+    const OzMmaProblem* pp = probs + tl.prob;
+    const int pm = pp->m, pn = pp->n, ldc = pp->ldc, ldcin = pp->ldcin;
+    const cplx alpha = pp->alpha, beta = pp->beta;
+    cplx* const Cout = pp->C;
+    const cplx* const Cin = pp->Cin;
+    const int* const eBp = pp->eB;
     const int row = qd * 32 + lane;
     const int r = tl.mt * TM + row;
-    if (r < pq.m) {
-      const cplx dg = pq.diag_ptr ? *pq.diag_ptr : pq.diag;
-      const bool has_cin = pq.Cin && (pq.beta.x != 0.0 || pq.beta.y != 0.0);
-      const int er = pq.eA[r];
+    if (r < pm) {
+      const cplx dg = pp->diag_ptr ? *pp->diag_ptr : pp->diag;
+      const bool has_cin = Cin && (beta.x != 0.0 || beta.y != 0.0);
+      const int er = pp->eA[r];
+      const int c0 = tl.nt * TN + hh * 32;
 #pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        const int c = tl.nt * TN + hh * 32 + j;
-        if (c >= pq.n) continue;
-        const int e = er + pq.eB[c];
-        double xr, xi;
-        if (e >= -1022 && e <= 1023) {  // 2^e as a normal double
-          const double sc = __longlong_as_double((long long)(e + 1023) << 52);
-          xr = cr[j] * sc;
-          xi = ci[j] * sc;
-        } else {
-          xr = ldexp(cr[j], e);
-          xi = ldexp(ci[j], e);
+      for (int g8 = 0; g8 < 4; ++g8) {
+        int ec[8];
+        cplx cb[8];
+#pragma unroll
+        for (int jj = 0; jj < 8; ++jj) {
+          const int c = c0 + g8 * 8 + jj;
+          const bool in = c < pn;
+          ec[jj] = in ? eBp[c] : 0;
+          cb[jj] = (in && has_cin) ? Cin[r + (size_t)c * ldcin] : make_double2(0.0, 0.0);
         }
-        cplx v;
-        v.x = pq.alpha.x * xr - pq.alpha.y * xi;
-        v.y = pq.alpha.x * xi + pq.alpha.y * xr;
-        if (has_cin) {
-          const cplx b = pq.Cin[r + (size_t)c * pq.ldcin];
-          v.x += pq.beta.x * b.x - pq.beta.y * b.y;
-          v.y += pq.beta.x * b.y + pq.beta.y * b.x;
+#pragma unroll
+        for (int jj = 0; jj < 8; ++jj) {
+          const int j = g8 * 8 + jj;
+          const int c = c0 + j;
+          if (c >= pn) continue;
+          const int e = er + ec[jj];
+          double xr, xi;
+          if (e >= -1022 && e <= 1023) {  // 2^e as a normal double
+            const double sc = __longlong_as_double((long long)(e + 1023) << 52);
+            xr = cr[j] * sc;
+            xi = ci[j] * sc;
+          } else {
+            xr = ldexp(cr[j], e);
+            xi = ldexp(ci[j], e);
+          }
+          cplx v;
+          v.x = alpha.x * xr - alpha.y * xi + (beta.x * cb[jj].x - beta.y * cb[jj].y);
+          v.y = alpha.x * xi + alpha.y * xr + (beta.x * cb[jj].y + beta.y * cb[jj].x);
+          if (r == c) {
+            v.x += dg.x;
+            v.y += dg.y;
+          }
+          Cout[r + (size_t)c * ldc] = v;
         }
-        if (r == c) {
-          v.x += dg.x;
-          v.y += dg.y;
-        }
-        pq.C[r + (size_t)c * pq.ldc] = v;
       }
     }
   }
-  if (leader) {
-    // all MMAs of this CTA complete, and every issued copy has landed, before
-    // TMEM is released and the CTA exits
+  // all MMAs of this CTA complete, and every issued copy has landed, before
+  // TMEM is released and the CTA exits
+  if (mma_thread) {
     oz_commit(oz_smem(&done_bar));
     oz_wait(oz_smem(&done_bar), 0, abort_flag, err, false);
-    for (int s = 0; s < STAGES; ++s)
-      if (last_use[s] >= 0) oz_wait(oz_smem(&full_bar[s]), (uint32_t)(last_use[s] & 1), abort_flag, err, false);
   }
+  if (load_thread)
+    for (int s = 0; s < STAGES; ++s)
+      if (used & (1u << s)) oz_wait(full0 + s * 8, (last_ph >> s) & 1u, abort_flag, err, false);
   __syncwarp();
   asm volatile("tcgen05.fence::before_thread_sync;" ::);
   __syncthreads();
