@@ -352,6 +352,11 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
   __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES], accf_bar, acce_bar, done_bar;
   __shared__ uint32_t tmem_sh;
   __shared__ int abort_sh;
+  // per (tile parity, warp): a copy of the tile's problem descriptor and the
+  // warp's 32 column scales, staged at the start of a tile for its epilogue
+  constexpr int PROB_WORDS = (int)(sizeof(OzMmaProblem) / 4);
+  static_assert(sizeof(OzMmaProblem) % 16 == 0 && PROB_WORDS <= 40, "epilogue staging layout");
+  __shared__ __align__(16) int ep_sh[2][DRAIN_WARPS][72];
   volatile int* abort_flag = &abort_sh;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -401,7 +406,7 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
   };
   if (load_thread && lvalid) load_product_base();
   bool load_ok = true, mma_ok = true;
-  long long next_issue = 0, next_refill = 0;  // first product not issued / not refilled yet
+  long long next_refill = 0;  // first product not refilled yet
 
   auto issue_load = [&]() {
     const uint32_t fb = full0 + ls * 8;
@@ -452,19 +457,27 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
     }
   };
 
-  // ---- MMA thread: every stage of global product P (tile P / NP, real product
-  // P % NP); ring slot ms with its full-barrier phase mph
+  // ---- MMA thread: the stages of global product P (tile P / NP, real product
+  // P % NP) up to chunk cend; product cur_P has its chunks [0, cur_c) issued.
+  // Ring slot ms with its full-barrier phase mph.
   const uint64_t descA0 = oz_desc(sbase, TM * 16, 128), descB0 = oz_desc(sbase + A_BLOCK, S * TN * 16, 128);
-  int ms = 0, mkch = 0;
+  int ms = 0, mkch = 0, cur_c = 0;
+  long long cur_P = -1;
   uint32_t mph = 0;
-  auto issue_product = [&](long long P) {
-    if (P > 0 && !oz_wait(oz_smem(&acce_bar), (uint32_t)((P - 1) & 1), abort_flag, err, true)) {
-      mma_ok = false;
-      return;
+  auto issue_upto = [&](long long P, int cend) {
+    if (cur_P != P) {
+      if (P > 0 && !oz_wait(oz_smem(&acce_bar), (uint32_t)((P - 1) & 1), abort_flag, err, true)) {
+        mma_ok = false;
+        return;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::);
+      if (P % NP == 0) mkch = oz_tile(tile_map, (int)blockIdx.x + (int)(P / NP) * G).kch;
+      cur_P = P;
+      cur_c = 0;
     }
-    asm volatile("tcgen05.fence::after_thread_sync;" ::);
-    if (P % NP == 0) mkch = oz_tile(tile_map, (int)blockIdx.x + (int)(P / NP) * G).kch;
-    for (int c = 0; c < mkch; ++c) {
+    const int c1 = cend < mkch ? cend : mkch;
+    for (; cur_c < c1; ++cur_c) {
+      const int c = cur_c;
       if (!oz_wait(full0 + ms * 8, mph, abort_flag, err, true)) {
         mma_ok = false;
         return;
@@ -488,21 +501,31 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
   // reads TMEM lanes 32 (w % 4).. and columns 32 (w / 4)..
   const int qd = warp & 3, hh = warp >> 2;
   bool ok = true;
+  constexpr int mkch_all = 1 << 30;
+  int my_eA = 0;
   for (int q = 0; q < my_tiles && ok; ++q) {
+    const OzTile tq = oz_tile(tile_map, (int)blockIdx.x + q * G);
     double cr[32], ci[32];
 #pragma unroll
     for (int j = 0; j < 32; ++j) { cr[j] = 0.0; ci[j] = 0.0; }
     for (int p = 0; p < NP; ++p) {
       const long long P = (long long)q * NP + p;
-      if (mma_thread && mma_ok && next_issue == P) {
-        issue_product(P);
-        ++next_issue;
-      }
+      if (mma_thread && mma_ok) issue_upto(P, mkch_all);
       if (load_thread && load_ok && next_refill == P) {
         refill_product(P);
         ++next_refill;
       }
       __syncwarp();
+      if (p == 0) {
+        // stage this tile's epilogue inputs while its first product runs
+        const int* src = reinterpret_cast<const int*>(probs + tq.prob);
+        int* eps = ep_sh[q & 1][warp];
+        for (int w = lane; w < PROB_WORDS; w += 32) eps[w] = src[w];
+        const OzMmaProblem* pp = probs + tq.prob;
+        eps[40 + lane] = pp->eB[tq.nt * TN + hh * 32 + lane];
+        my_eA = pp->eA[tq.mt * TM + qd * 32 + lane];
+        __syncwarp();
+      }
       if (!oz_wait_warp(oz_smem(&accf_bar), (uint32_t)(P & 1), abort_flag, err)) {
         ok = false;
         break;
@@ -547,48 +570,46 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
     }
     if (!ok) break;
     // the next tile's first product goes to the tensor cores before this
-    // epilogue (its first STAGES stages are loaded already; the load thread
-    // refills after its own epilogue)
-    if (mma_thread && mma_ok && next_issue < my_products) {
-      issue_product(next_issue);
-      ++next_issue;
-    }
+    // epilogue, as far as its stages are loaded already (STAGES of them); the
+    // rest follows after the epilogue, as does the load thread's refill
+    if (mma_thread && mma_ok && (long long)(q + 1) * NP < my_products) issue_upto((long long)(q + 1) * NP, STAGES);
     __syncwarp();
-    // C = alpha * 2^(eA + eB) (Re, Im) + beta * Cin + diag * I. The problem's
-    // fields go to registers first and every group of eight columns loads
-    // its inputs before its stores, so that no load waits behind a store
-    // that might alias it.
-    const OzTile tl = oz_tile(tile_map, (int)blockIdx.x + q * G);
-    const OzMmaProblem* pp = probs + tl.prob;
-    const int pm = pp->m, pn = pp->n, ldc = pp->ldc, ldcin = pp->ldcin;
-    const cplx alpha = pp->alpha, beta = pp->beta;
-    cplx* const Cout = pp->C;
-    const cplx* const Cin = pp->Cin;
-    const int* const eBp = pp->eB;
-    const int row = qd * 32 + lane;
-    const int r = tl.mt * TM + row;
-    if (r < pm) {
-      const cplx dg = pp->diag_ptr ? *pp->diag_ptr : pp->diag;
+    // C = alpha * 2^(eA + eB) (Re, Im) + beta * Cin + diag * I, from the
+    // staged descriptor and scales; Cin is read one group of columns ahead of
+    // the stores
+    const int* eps = ep_sh[q & 1][warp];
+    const OzMmaProblem& ps = *reinterpret_cast<const OzMmaProblem*>(eps);
+    const int r = tq.mt * TM + qd * 32 + lane;
+    if (r < ps.m) {
+      const int pn = ps.n, ldc = ps.ldc, ldcin = ps.ldcin;
+      const cplx alpha = ps.alpha, beta = ps.beta;
+      cplx* const Cout = ps.C;
+      const cplx* const Cin = ps.Cin;
+      const cplx dg = ps.diag_ptr ? *ps.diag_ptr : ps.diag;
       const bool has_cin = Cin && (beta.x != 0.0 || beta.y != 0.0);
-      const int er = pp->eA[r];
-      const int c0 = tl.nt * TN + hh * 32;
+      const int c0 = tq.nt * TN + hh * 32;
+      constexpr int GW = 4;  // columns per group
+      cplx cb[GW], cn[GW];
 #pragma unroll
-      for (int g8 = 0; g8 < 4; ++g8) {
-        int ec[8];
-        cplx cb[8];
+      for (int jj = 0; jj < GW; ++jj)
+        cn[jj] = (has_cin && c0 + jj < pn) ? Cin[r + (size_t)(c0 + jj) * ldcin] : make_double2(0.0, 0.0);
 #pragma unroll
-        for (int jj = 0; jj < 8; ++jj) {
-          const int c = c0 + g8 * 8 + jj;
-          const bool in = c < pn;
-          ec[jj] = in ? eBp[c] : 0;
-          cb[jj] = (in && has_cin) ? Cin[r + (size_t)c * ldcin] : make_double2(0.0, 0.0);
+      for (int g8 = 0; g8 < 32 / GW; ++g8) {
+#pragma unroll
+        for (int jj = 0; jj < GW; ++jj) cb[jj] = cn[jj];
+        if (g8 < 32 / GW - 1) {
+#pragma unroll
+          for (int jj = 0; jj < GW; ++jj) {
+            const int c = c0 + (g8 + 1) * GW + jj;
+            cn[jj] = (has_cin && c < pn) ? Cin[r + (size_t)c * ldcin] : make_double2(0.0, 0.0);
+          }
         }
 #pragma unroll
-        for (int jj = 0; jj < 8; ++jj) {
-          const int j = g8 * 8 + jj;
+        for (int jj = 0; jj < GW; ++jj) {
+          const int j = g8 * GW + jj;
           const int c = c0 + j;
           if (c >= pn) continue;
-          const int e = er + ec[jj];
+          const int e = my_eA + eps[40 + j];
           double xr, xi;
           if (e >= -1022 && e <= 1023) {  // 2^e as a normal double
             const double sc = __longlong_as_double((long long)(e + 1023) << 52);
