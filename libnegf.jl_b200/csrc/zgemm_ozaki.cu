@@ -10,8 +10,8 @@
 //     integer, written as seven balanced base-256 digits x = sum_i s_i
 //     256^(6 - i) (top digit |s_0| <= 64, lower digits in [-128, 127]); the
 //     digits are the bytes of x + C6 (lower ones minus 128), so the split is a
-//     conversion, an add and byte permutes per element (representation error
-//     <= 2^(e_r - 55));
+//     rounding (FP64 adds), an add and byte permutes per element
+//     (representation error <= 2^(e_r - 55));
 //   * product: sum_k A[r,k] B[c,k] = 2^(eA_r + eB_c) sum_{D=0..7} 2^(-12 - 8D)
 //     acc_D, acc_D = sum_{i+j=D} sum_k sA_i sB_j; each acc_D is an exact int32
 //     sum (|acc_D| <= 7 * K * 2^14 < 2^31 for K < 18000); the 34 digit pairs
@@ -72,6 +72,12 @@ __host__ __device__ constexpr double oz_diag_weight(int D) {
   return w;
 }
 
+// 2^e as a double for |e| <= 500, else 0 (callers then take an ldexp path);
+// the limit keeps products of two such factors and an accumulator in range
+__device__ __forceinline__ double oz_pow2(int e) {
+  return (e >= -500 && e <= 500) ? __longlong_as_double((long long)(e + 1023) << 52) : 0.0;
+}
+
 // exact int32 -> double on the FP64 pipe: the bits 0x43300000:(x ^ 2^31) are
 // 2^52 + 2^31 + x, from which one exact subtraction leaves x
 __device__ __forceinline__ double oz_i2d(uint32_t x) {
@@ -80,6 +86,21 @@ __device__ __forceinline__ double oz_i2d(uint32_t x) {
 
 // ---------------------------------------------------------------------------
 // split
+
+__device__ __forceinline__ uint32_t oz_smem(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// rint(y) for |y| < 2^54 as an int64, on the FP64 add pipe: with M = 2^52 +
+// 2^51, the low word of t + M is rint(t) for |t| < 2^31; y is taken in two
+// 27-bit halves (both steps exact but the final rounding of the low half)
+__device__ __forceinline__ long long oz_rint54(double y) {
+  constexpr double M = 6755399441055744.0;  // 2^52 + 2^51
+  const double t = y * 0x1p-27;
+  const double th = (t + M) - M;            // rint(t), |th| <= 2^27
+  const int hi = __double2loint(t + M);
+  const double yl = fma(-th, 0x1p27, y);    // exact, |yl| <= 2^26
+  const int lo = __double2loint(yl + M);
+  return ((long long)hi << 27) + lo;
+}
 
 // gather byte `bb` of four words into one word (element j -> byte j)
 __device__ __forceinline__ uint32_t oz_gather(uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3, uint32_t bb) {
@@ -91,7 +112,9 @@ __global__ void __launch_bounds__(256, 3) ozaki_split_kernel(const OzSplitProble
   const OzSplitProblem q = probs[blockIdx.y];
   const int r0 = blockIdx.x * oz::SPLIT_ROWS;
   if (r0 >= q.rows_pad) return;
-  __shared__ cplx tile[oz::SPLIT_ROWS][33];
+  // two staging buffers of rows r0..r0+63 x one 32-wide K chunk (dynamic)
+  extern __shared__ __align__(16) unsigned char split_smem[];
+  cplx(*tile)[oz::SPLIT_ROWS][33] = reinterpret_cast<cplx(*)[oz::SPLIT_ROWS][33]>(split_smem);
   __shared__ double red[4][oz::SPLIT_ROWS];
   __shared__ int sh_e[oz::SPLIT_ROWS];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -104,6 +127,7 @@ __global__ void __launch_bounds__(256, 3) ozaki_split_kernel(const OzSplitProble
     const int r = tid & 63, gr = r0 + r;
     double mx = 0.0;
     if (gr < q.rows)
+#pragma unroll 4
       for (int k = tid >> 6; k < q.cols; k += 4) {
         const cplx v = q.X[(long long)gr + (long long)k * q.sk];
         mx = fmax(mx, fabs(v.x) + fabs(v.y));
@@ -122,6 +146,7 @@ __global__ void __launch_bounds__(256, 3) ozaki_split_kernel(const OzSplitProble
       const int r = warp + 8 * j, gr = r0 + r;
       double mx = 0.0;
       if (gr < q.rows)
+#pragma unroll 4
         for (int k = lane; k < q.cols; k += 32) {
           const cplx v = q.X[(long long)gr * q.sr + k];
           mx = fmax(mx, fabs(v.x) + fabs(v.y));
@@ -157,27 +182,42 @@ __global__ void __launch_bounds__(256, 3) ozaki_split_kernel(const OzSplitProble
   const size_t half = TR == oz::TM ? (size_t)TR * 16 : (size_t)oz::S * TR * 16;
   const size_t block = (size_t)oz::S * TR * oz::KC;
   const int ntiles = q.rows_pad / TR;
-  for (int c = 0; c < kch; ++c) {
-    // stage rows r0..r0+63, k = 32c..32c+31 (zeros outside)
+  // asynchronous staging of chunk c into buffer b (zero-filled outside Y)
+  auto stage = [&](int c, int b) {
     const int kbase = c * oz::KC;
     if (rows_contig) {
       const int r = tid & 63, gr = r0 + r;
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         const int kk = (tid >> 6) + 4 * j, gk = kbase + kk;
-        cplx v = make_double2(0.0, 0.0);
-        if (gr < q.rows && gk < q.cols) v = q.X[(long long)gr + (long long)gk * q.sk];
-        tile[r][kk] = v;
+        const bool in = gr < q.rows && gk < q.cols;
+        const void* src = in ? (const void*)(q.X + (long long)gr + (long long)gk * q.sk) : (const void*)probs;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(oz_smem(&tile[b][r][kk])), "l"(src),
+                     "r"(in ? 16 : 0)
+                     : "memory");
       }
     } else {
       const int kk = tid & 31, gk = kbase + kk;
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         const int r = (tid >> 5) + 8 * j, gr = r0 + r;
-        cplx v = make_double2(0.0, 0.0);
-        if (gr < q.rows && gk < q.cols) v = q.X[(long long)gr * q.sr + gk];
-        tile[r][kk] = v;
+        const bool in = gr < q.rows && gk < q.cols;
+        const void* src = in ? (const void*)(q.X + (long long)gr * q.sr + gk) : (const void*)probs;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(oz_smem(&tile[b][r][kk])), "l"(src),
+                     "r"(in ? 16 : 0)
+                     : "memory");
       }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  stage(0, 0);
+  for (int c = 0; c < kch; ++c) {
+    const int b = c & 1;
+    if (c + 1 < kch) {
+      stage(c + 1, b ^ 1);
+      asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     }
     __syncthreads();
 #pragma unroll
@@ -187,9 +227,9 @@ __global__ void __launch_bounds__(256, 3) ozaki_split_kernel(const OzSplitProble
       uint32_t lo[3][4], hi[3][4];
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        const cplx v = tile[rl][16 * h + 4 * kq + j];
-        const long long xr = __double2ll_rn(v.x * f1 * f2);
-        const long long xi = __double2ll_rn(v.y * fi * f2);
+        const cplx v = tile[b][rl][16 * h + 4 * kq + j];
+        const long long xr = oz_rint54(v.x * f1 * f2);
+        const long long xi = oz_rint54(v.y * fi * f2);
         const long long x3[3] = {xr + oz::C6, xi + oz::C6, xr + xi + oz::C6};
 #pragma unroll
         for (int p = 0; p < 3; ++p) {
@@ -218,7 +258,6 @@ __global__ void __launch_bounds__(256, 3) ozaki_split_kernel(const OzSplitProble
 // ---------------------------------------------------------------------------
 // product
 
-__device__ __forceinline__ uint32_t oz_smem(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ uint64_t oz_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
   uint64_t d = 0;
@@ -353,10 +392,11 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
   __shared__ uint32_t tmem_sh;
   __shared__ int abort_sh;
   // per (tile parity, warp): a copy of the tile's problem descriptor and the
-  // warp's 32 column scales, staged at the start of a tile for its epilogue
+  // warp's 32 column exponents and scales 2^eB, staged at the start of a tile
   constexpr int PROB_WORDS = (int)(sizeof(OzMmaProblem) / 4);
   static_assert(sizeof(OzMmaProblem) % 16 == 0 && PROB_WORDS <= 40, "epilogue staging layout");
-  __shared__ __align__(16) int ep_sh[2][DRAIN_WARPS][72];
+  // words 0..39 descriptor, 40..71 column exponents, 72..135 column scales
+  __shared__ __align__(16) int ep_sh[2][DRAIN_WARPS][136];
   volatile int* abort_flag = &abort_sh;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -503,6 +543,7 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
   bool ok = true;
   constexpr int mkch_all = 1 << 30;
   int my_eA = 0;
+  double my_scA = 1.0;
   for (int q = 0; q < my_tiles && ok; ++q) {
     const OzTile tq = oz_tile(tile_map, (int)blockIdx.x + q * G);
     double cr[32], ci[32];
@@ -522,8 +563,11 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
         int* eps = ep_sh[q & 1][warp];
         for (int w = lane; w < PROB_WORDS; w += 32) eps[w] = src[w];
         const OzMmaProblem* pp = probs + tq.prob;
-        eps[40 + lane] = pp->eB[tq.nt * TN + hh * 32 + lane];
+        const int eb = pp->eB[tq.nt * TN + hh * 32 + lane];
+        eps[40 + lane] = eb;
+        reinterpret_cast<double*>(eps + 72)[lane] = oz_pow2(eb);
         my_eA = pp->eA[tq.mt * TM + qd * 32 + lane];
+        my_scA = oz_pow2(my_eA);
         __syncwarp();
       }
       if (!oz_wait_warp(oz_smem(&accf_bar), (uint32_t)(P & 1), abort_flag, err)) {
@@ -531,8 +575,12 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::);
-      const double sr = (p == 2) ? 0.0 : (p == 0 ? 1.0 : -1.0);  // P1 -> +Re, P2 -> -Re
-      const double si = (p == 2) ? 1.0 : -1.0;                   // P3 -> +Im, P1, P2 -> -Im
+      // product p adds v to Re with sign sr and to Im with sign si (P1: +Re,
+      // -Im; P2: -Re, -Im; P3: +Im); alpha is folded in: (kr, ki) = alpha (sr, si)
+      const double sr = (p == 2) ? 0.0 : (p == 0 ? 1.0 : -1.0);
+      const double si = (p == 2) ? 1.0 : -1.0;
+      const cplx al = reinterpret_cast<const OzMmaProblem*>(ep_sh[q & 1][warp])->alpha;
+      const double kr = al.x * sr - al.y * si, ki = al.x * si + al.y * sr;
 #pragma unroll
       for (int c8 = 0; c8 < 4; ++c8) {
         double v[8];
@@ -560,8 +608,8 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
         }
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-          cr[c8 * 8 + j] = fma(sr, v[j], cr[c8 * 8 + j]);
-          ci[c8 * 8 + j] = fma(si, v[j], ci[c8 * 8 + j]);
+          cr[c8 * 8 + j] = fma(kr, v[j], cr[c8 * 8 + j]);
+          ci[c8 * 8 + j] = fma(ki, v[j], ci[c8 * 8 + j]);
         }
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::);
@@ -574,7 +622,8 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
     // rest follows after the epilogue, as does the load thread's refill
     if (mma_thread && mma_ok && (long long)(q + 1) * NP < my_products) issue_upto((long long)(q + 1) * NP, STAGES);
     __syncwarp();
-    // C = alpha * 2^(eA + eB) (Re, Im) + beta * Cin + diag * I, from the
+    // C = alpha 2^(eA + eB) (Re, Im) + beta Cin + diag I (alpha already in
+    // cr, ci), from the
     // staged descriptor and scales; Cin is read one group of columns ahead of
     // the stores
     const int* eps = ep_sh[q & 1][warp];
@@ -582,7 +631,7 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
     const int r = tq.mt * TM + qd * 32 + lane;
     if (r < ps.m) {
       const int pn = ps.n, ldc = ps.ldc, ldcin = ps.ldcin;
-      const cplx alpha = ps.alpha, beta = ps.beta;
+      const cplx beta = ps.beta;
       cplx* const Cout = ps.C;
       const cplx* const Cin = ps.Cin;
       const cplx dg = ps.diag_ptr ? *ps.diag_ptr : ps.diag;
@@ -609,19 +658,20 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
           const int j = g8 * GW + jj;
           const int c = c0 + j;
           if (c >= pn) continue;
-          const int e = my_eA + eps[40 + j];
+          // alpha 2^(eA + eB) (Re, Im): two exact power-of-two factors when
+          // both exponents are moderate, else one ldexp
+          const double scB = reinterpret_cast<const double*>(eps + 72)[j];
           double xr, xi;
-          if (e >= -1022 && e <= 1023) {  // 2^e as a normal double
-            const double sc = __longlong_as_double((long long)(e + 1023) << 52);
-            xr = cr[j] * sc;
-            xi = ci[j] * sc;
+          if (my_scA != 0.0 && scB != 0.0) {
+            xr = cr[j] * my_scA * scB;
+            xi = ci[j] * my_scA * scB;
           } else {
-            xr = ldexp(cr[j], e);
-            xi = ldexp(ci[j], e);
+            xr = ldexp(cr[j], my_eA + eps[40 + j]);
+            xi = ldexp(ci[j], my_eA + eps[40 + j]);
           }
           cplx v;
-          v.x = alpha.x * xr - alpha.y * xi + (beta.x * cb[jj].x - beta.y * cb[jj].y);
-          v.y = alpha.x * xi + alpha.y * xr + (beta.x * cb[jj].y + beta.y * cb[jj].x);
+          v.x = xr + (beta.x * cb[jj].x - beta.y * cb[jj].y);
+          v.y = xi + (beta.x * cb[jj].y + beta.y * cb[jj].x);
           if (r == c) {
             v.x += dg.x;
             v.y += dg.y;
@@ -651,15 +701,19 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
 
 size_t ozaki_mma_smem_bytes() { return (size_t)oz::STAGES * oz::STAGE; }
 
+constexpr size_t kSplitSmem = 2 * oz::SPLIT_ROWS * 33 * sizeof(cplx);
+
 cudaError_t ozaki_prepare() {
-  return cudaFuncSetAttribute(ozaki_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)ozaki_mma_smem_bytes());
+  cudaError_t e = cudaFuncSetAttribute(ozaki_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)ozaki_mma_smem_bytes());
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(ozaki_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSplitSmem);
 }
 
 cudaError_t launch_ozaki_split(const void* probs, int nprob, int max_rows_pad, cudaStream_t st) {
   if (nprob <= 0) return cudaSuccess;
   dim3 grid((max_rows_pad + oz::SPLIT_ROWS - 1) / oz::SPLIT_ROWS, nprob);
-  ozaki_split_kernel<<<grid, 256, 0, st>>>(static_cast<const OzSplitProblem*>(probs));
+  ozaki_split_kernel<<<grid, 256, kSplitSmem, st>>>(static_cast<const OzSplitProblem*>(probs));
   return cudaGetLastError();
 }
 
