@@ -11,7 +11,11 @@ all diagonal G^R and G^< blocks and T(E) = Tr[Gamma_L G^R_1N Gamma_R G^A_N1].
 Seeded synthetic data (numpy default_rng(0)); no dataset is involved.
 
 One step = one pass of RGF (shared upward pass) + downward G^R + RKD + the
-transmission chain over all 256 energies, on device-resident inputs.
+transmission chain over all 256 energies, on device-resident inputs, replayed
+as one CUDA graph.  The headline is the mixed-precision path (Schur products on
+the INT8 tensor cores with FP64-grade digit splitting; inversions in FP64),
+checked block by block against the FP64 path's outputs (bar 1e-10); the FP64
+path is timed beside it ("fp64_path").
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -54,7 +58,6 @@ def parse():
     ap.add_argument("--cpu-budget-s", type=float, default=12.0, help="time budget of each CPU baseline mode")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
     return ap.parse_args()
 
 
@@ -266,69 +269,129 @@ def run_ours(args):
 
     sysm = physics.physics_system(args.npl, args.b, seed=0)
     dev = negf.Device(sysm.Hd, sysm.Hu, sysm.sigL, sysm.sigR)
-    solver = negf.Solver(dev, args.ne, eta=sysm.eta)
-    stats = solver.stats()
     stream = torch.cuda.Stream()
     sh = stream.cuda_stream
-    solver.set_energies(my_E, sh)
-
-    # FP64 peak of this GPU (roofline denominator)
-    d1 = __import__("ctypes").c_double()
-    d2 = __import__("ctypes").c_double()
-    negf._lib.check(negf.load().negf_probe_fp64_peak(__import__("ctypes").byref(d1), __import__("ctypes").byref(d2)))
+    per = sum(b * b for b in dev.sizes)
+    import ctypes
+    # roofline denominators of this GPU, measured in-run
+    d1, d2, d3 = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    negf._lib.check(negf.load().negf_probe_fp64_peak(ctypes.byref(d1), ctypes.byref(d2)))
     fp64_peak = max(d1.value, d2.value)
-
-    for _ in range(args.warmup):
-        solver.run_profiled(sh)
-    torch.cuda.synchronize()
-    solver.profile_read(reset=True)
-    solver.check()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
+    negf._lib.check(negf.load().negf_probe_int8_peak(ctypes.byref(d3)))
+    int8_peak = d3.value
+    step_flops = canonical_flops(args.npl, args.b) * args.ne
+    total_pts = args.ne * args.steps * world
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(dev_index) as clk:
+
+    def timed(solver, clk=None):
+        """Warm-up, then K graph replays bracketed by barrier + sync; max over ranks."""
+        solver.set_energies(my_E, sh)
+        for _ in range(args.warmup):
+            solver.run(sh)
+        stream.synchronize()
+        solver.check()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
         ev0.record(stream)
         for _ in range(args.steps):
-            solver.run_profiled(sh)
+            solver.run(sh)
         ev1.record(stream)
         ev1.synchronize()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    prof = solver.profile_read(reset=True)
-    solver.check()
-    ms = max_over_ranks(ms, dist if world > 1 else None, "cuda")
-    total_pts = args.ne * args.steps * world
-    value = total_pts / (ms / 1000.0)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        solver.check()
+        return max_over_ranks(ev0.elapsed_time(ev1), dist if world > 1 else None, "cuda")
 
-    # dominant kernel (by device time) and its roofline
+    def profiled(solver):
+        """Per-kernel device time of one launch-by-launch pass."""
+        solver.profile_read(reset=True)
+        solver.run_profiled(sh)
+        stream.synchronize()
+        return solver.profile_read(reset=True)
+
+    def breakdown_of(prof):
+        tot = sum(v[0] for v in prof.values()) or 1.0
+        return {k: {"ms": v[0], "launches": v[2], "share": v[0] / tot,
+                    "tflops": (v[1] / (v[0] / 1000.0) / 1e12) if v[0] > 0 and v[1] > 0 else None}
+                for k, v in prof.items() if v[2]}
+
+    # ---- FP64 path (reference precision): timing, breakdown, reference outputs
+    solver = negf.Solver(dev, args.ne, eta=sysm.eta)
+    fstats = solver.stats()
+    fms = timed(solver)
+    fprof = profiled(solver)
+    k_ms, k_fl, k_n = fprof["gemm"]
+    f_ach = (k_fl / k_n) / ((k_ms / k_n) / 1000.0) / 1e12 if k_n else 0.0
+    fvalue = total_pts / (fms / 1000.0)
+    fp64 = {"value": fvalue, "unit": UNIT, "ms_per_step": fms / args.steps,
+            "algorithmic_tflops": step_flops / ((fms / args.steps) / 1000.0) / 1e12,
+            "gpu_launches": int(fstats["launches"]) * args.steps,
+            "kernels": breakdown_of(fprof),
+            "roofline": {"kernel": "zgemm3m_batched_kernel (DMMA m16n8k4 f64)", "bound": "tensor",
+                         "achieved": f_ach, "peak": fp64_peak, "unit": "TFLOP/s",
+                         "frac": f_ach / fp64_peak if fp64_peak else None,
+                         "peak_source": "FP64 mma.sync throughput measured in-run (negf_probe_fp64_peak)"}}
+    checked = list(range(0, args.ne, max(1, args.ne // 32)))
+    solver.run(sh)
+    stream.synchronize()
+    outs = solver.outputs()
+    refs = [_device_doubles(outs[w], 2 * args.ne * per).view(args.ne, 2 * per)[checked].clone() for w in range(2)]
+    t_ref = _device_doubles(outs[2], 2 * args.ne)[0::2].clone()
+    solver.close()
+
+    # ---- mixed path (the headline): INT8 tensor-core Schur products
+    solver = negf.Solver(dev, args.ne, eta=sysm.eta, precision="mixed")
+    stats = solver.stats()
+    with ClockSampler(dev_index) as clk:
+        ms = timed(solver)
+    prof = profiled(solver)
+    value = total_pts / (ms / 1000.0)
+    outs = solver.outputs()
+    errs = [0.0, 0.0]
+    for w in range(2):
+        got = _device_doubles(outs[w], 2 * args.ne * per).view(args.ne, 2 * per)[checked]
+        o = 0
+        for bsz in dev.sizes:
+            sl_ = slice(2 * o, 2 * (o + bsz * bsz))
+            num = torch.linalg.vector_norm(got[:, sl_] - refs[w][:, sl_], dim=1)
+            den = torch.linalg.vector_norm(refs[w][:, sl_], dim=1)
+            errs[w] = max(errs[w], float((num / den).max()))
+            o += bsz * bsz
+    t_mix = _device_doubles(outs[2], 2 * args.ne)[0::2]
+    t_err = float(((t_mix - t_ref).abs() / t_ref.abs().clamp(min=1.0)).max())
+    del refs, t_ref
+
+    # dominant kernel: the INT8 product kernel; algorithmic work per launch =
+    # 3 real products x 34 digit pairs x 2mnk int8 ops per complex product
+    # (8mnk complex flops) = 25.5 x its complex flops
     kind = max(prof, key=lambda k: prof[k][0])
     k_ms, k_fl, k_n = prof[kind]
-    achieved = (k_fl / k_n) / ((k_ms / k_n) / 1000.0) / 1e12 if k_n else 0.0
+    ops_per_cflop = 3 * 34 * 2 / 8.0
+    if kind == "oz_mma":
+        achieved = (k_fl * ops_per_cflop / k_n) / ((k_ms / k_n) / 1000.0) / 1e12
+        roof = {"kernel": "ozaki_mma_kernel (tcgen05.mma kind::i8, TMEM accumulators)", "bound": "tensor",
+                "achieved": achieved, "peak": int8_peak, "unit": "TOP/s (int8)",
+                "frac": achieved / int8_peak if int8_peak else None,
+                "peak_source": "dense kind::i8 tcgen05 throughput measured in-run (negf_probe_int8_peak)",
+                "complex_tflops_equivalent": (k_fl / k_n) / ((k_ms / k_n) / 1000.0) / 1e12}
+    else:
+        achieved = (k_fl / k_n) / ((k_ms / k_n) / 1000.0) / 1e12 if k_n else 0.0
+        roof = {"kernel": kind, "bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp64_peak if fp64_peak else None}
     traffic = load_traffic()
-    roof = {"kernel": "zgemm_batched_kernel (DMMA m16n8k4 f64)" if kind == "gemm" else kind,
-            "bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-            "frac": achieved / fp64_peak if fp64_peak else None,
-            "peak_source": "FP64 mma.sync throughput measured in-run (negf_probe_fp64_peak); MEASURED_PEAKS.json "
-                           "has no FP64 figure",
-            "traffic": traffic.get("zgemm_bytes_per_launch") if traffic else None,
-            "share": k_ms / sum(v[0] for v in prof.values()),
-            "launch_ms": k_ms / max(1, k_n)}
-    breakdown = {k: {"ms": v[0] / args.steps, "launches": v[2] // args.steps,
-                     "tflops": (v[1] / (v[0] / 1000.0) / 1e12) if v[0] > 0 and v[1] > 0 else None}
-                 for k, v in prof.items() if v[2]}
-    step_flops = canonical_flops(args.npl, args.b) * args.ne
+    roof["traffic"] = traffic.get("oz_mma_bytes_per_launch") if traffic else None
+    roof["share"] = k_ms / sum(v[0] for v in prof.values())
+    roof["launch_ms"] = k_ms / max(1, k_n)
     whole = {"algorithmic_tflops": step_flops / ((ms / args.steps) / 1000.0) / 1e12,
-             "executed_tflops": stats["flops"] / ((ms / args.steps) / 1000.0) / 1e12,
-             "frac_of_fp64_peak": step_flops / ((ms / args.steps) / 1000.0) / 1e12 / fp64_peak}
+             "executed_complex_tflops": stats["flops"] / ((ms / args.steps) / 1000.0) / 1e12,
+             "speedup_vs_fp64_path": value / fvalue}
 
-    # end to end through the public API with host buffers (pinned)
+    # ---- end to end through the public API with host buffers (pinned), mixed path
     e2e = None
     if not args.no_e2e:
-        per = sum(b * b for b in dev.sizes)
         nbytes = args.ne * per * 16
         gr_h = torch.empty(args.ne * per * 2, dtype=torch.float64, pin_memory=True)
         gl_h = torch.empty(args.ne * per * 2, dtype=torch.float64, pin_memory=True)
@@ -337,7 +400,6 @@ def run_ours(args):
         hu = [torch.from_numpy(np.asfortranarray(h).T.copy()).pin_memory() for h in sysm.Hu]
         sl = torch.from_numpy(np.asfortranarray(sysm.sigL).T.copy()).pin_memory()
         sr = torch.from_numpy(np.asfortranarray(sysm.sigR).T.copy()).pin_memory()
-        # host column-major views of the pinned arrays
         hd_np = [x.numpy().T for x in hd]
         hu_np = [x.numpy().T for x in hu]
 
@@ -359,83 +421,24 @@ def run_ours(args):
         e2e = {"value": total_pts / el, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(2 * nbytes + 16 * args.ne), "ms_per_step": 1000 * el / args.steps}
 
-    # mixed precision: the same workload with the Schur products on the INT8
-    # tensor cores (FP64-accurate digit splitting); compared block by block
-    # with the FP64 outputs of a sample of energies
-    mixed = None
-    if not args.no_mixed:
-        per = sum(b * b for b in dev.sizes)
-        checked = list(range(0, args.ne, max(1, args.ne // 32)))
-        stream.synchronize()
-        outs = solver.outputs()
-        refs = [_device_doubles(outs[w], 2 * args.ne * per).view(args.ne, 2 * per)[checked].clone()
-                for w in range(2)]
-        t_ref = _device_doubles(outs[2], 2 * args.ne)[0::2].clone()
-        solver.close()
-        msolver = negf.Solver(dev, args.ne, eta=sysm.eta, precision="mixed")
-        mstats = msolver.stats()
-        msolver.set_energies(my_E, sh)
-        for _ in range(args.warmup):
-            msolver.run_profiled(sh)
-        stream.synchronize()
-        msolver.profile_read(reset=True)
-        msolver.check()
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-        ev0.record(stream)
-        for _ in range(args.steps):
-            msolver.run_profiled(sh)
-        ev1.record(stream)
-        ev1.synchronize()
-        mms = max_over_ranks(ev0.elapsed_time(ev1), dist if world > 1 else None, "cuda")
-        mprof = msolver.profile_read(reset=True)
-        msolver.check()
-        outs = msolver.outputs()
-        errs = [0.0, 0.0]
-        for w in range(2):
-            got = _device_doubles(outs[w], 2 * args.ne * per).view(args.ne, 2 * per)[checked]
-            o = 0
-            for bsz in dev.sizes:
-                sl_ = slice(2 * o, 2 * (o + bsz * bsz))
-                num = torch.linalg.vector_norm(got[:, sl_] - refs[w][:, sl_], dim=1)
-                den = torch.linalg.vector_norm(refs[w][:, sl_], dim=1)
-                errs[w] = max(errs[w], float((num / den).max()))
-                o += bsz * bsz
-        t_mix = _device_doubles(outs[2], 2 * args.ne)[0::2]
-        t_err = float(((t_mix - t_ref).abs() / t_ref.abs().clamp(min=1.0)).max())
-        mval = total_pts / (mms / 1000.0)
-        tot_ms = sum(v[0] for v in mprof.values())
-        mixed = {"value": mval, "unit": UNIT, "ms_per_step": mms / args.steps, "speedup_vs_fp64": mval / value,
-                 "max_block_rel_err_vs_fp64": {"GR": errs[0], "GL": errs[1], "energies_checked": len(checked)},
-                 "max_T_err_vs_fp64": t_err,
-                 "kernels": {k: {"ms": v[0] / args.steps, "launches": v[2] // args.steps,
-                                 "share": v[0] / tot_ms if tot_ms else None}
-                             for k, v in mprof.items() if v[2]},
-                 "gpu_launches": int(mstats["launches"]) * args.steps,
-                 "algorithmic_tflops": step_flops / ((mms / args.steps) / 1000.0) / 1e12,
-                 "method": "3M complex products of 7-digit base-256 int8 splits of 54-bit fixed-point rows "
-                           "(34 digit pairs per real product) on tcgen05.mma kind::i8 with exact int32 TMEM "
-                           "accumulation; FP64 Gauss-Jordan inversions"}
-        if "oz_mma" in mprof and mprof["oz_mma"][2]:
-            k = mprof["oz_mma"]
-            mixed["int8_mma"] = {"complex_flops_per_s": k[1] / (k[0] / 1000.0),
-                                 "int8_ops_per_s": k[1] / (k[0] / 1000.0) * 34 * 3 / 4}
-        del refs, t_ref
-        solver = msolver
-
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded numpy generator of the config)",
+                "vs_baseline": None, "dtype": "int8 products / f64",
+                "data": "synthetic (seeded numpy generator of the config)",
                 "config": {"workload": WORKLOAD, "npl": args.npl, "b": args.b, "energies_per_gpu": args.ne,
-                           "eta": 1e-6, "mu_l": 0.1, "mu_r": -0.1, "kT": 0.025, "precision": "fp64",
+                           "eta": 1e-6, "mu_l": 0.1, "mu_r": -0.1, "kT": 0.025, "precision": "mixed",
                            "parallelism": "energies sharded across ranks, no collective" if world > 1 else "1 GPU",
                            "l2": "inputs larger than L2: %.1f GB device working set per pass" %
                                  (stats["workspace_bytes"] / 1e9)},
-                "roofline": roof, "kernels": breakdown, "whole_step": whole, "clocks": clk.summary(),
+                "accuracy_vs_fp64": {"max_block_rel_err_GR": errs[0], "max_block_rel_err_GL": errs[1],
+                                     "max_T_err": t_err, "energies_checked": len(checked), "bar": 1e-10},
+                "roofline": roof, "kernels": breakdown_of(prof), "whole_step": whole, "clocks": clk.summary(),
                 "gpu_launches": int(stats["launches"]) * args.steps,
-                "e2e": e2e, "cpu_baseline": cpu, "mixed": mixed}
+                "e2e": e2e, "cpu_baseline": cpu, "fp64_path": fp64,
+                "method": "3M complex products of 7-digit base-256 int8 splits of 54-bit fixed-point rows (34 digit "
+                          "pairs per real product) on tcgen05.mma kind::i8 with exact int32 TMEM accumulation; "
+                          "FP64 Gauss-Jordan inversions"}
         print(json.dumps(line), flush=True)
     solver.close()
     dev.close()

@@ -66,8 +66,8 @@ typedef struct {
 int negf_zgemm_batched(char opA, char opB, int32_t nprob, const negf_zgemm_problem* probs, void* stream);
 
 /* negf_zgemm_batched in the MIXED precision mode (INT8 tensor cores with
- * digit splitting; see NEGF_PREC_MIXED).  Same problems and results within
- * ~1e-13 relative to |op(A)| |op(B)|; k <= 1024. */
+ * digit splitting; see NEGF_PREC_MIXED).  Same problems; results agree with
+ * the FP64 ones to ~1e-15 relative to |op(A)| |op(B)| (FP64-grade); k <= 1024. */
 int negf_zgemm_batched_mixed(char opA, char opB, int32_t nprob, const negf_zgemm_problem* probs, void* stream);
 
 /* Batched be_copy_in_hw! / be_ctranspose! (src/backend_cpu.jl:42-68):
@@ -275,11 +275,12 @@ CCscMatrix run_bndiag_wrapper(int32_t m, int32_t n, int32_t nnz_in, int32_t* col
                               const char** dict_keys_in, int32_t* dict_vals_in, int32_t is_hermitian);
 
 /* ------------------------------------------------------------------------
- * Measurement helper: FP64 throughput of the tensor (mma.sync f64) and
- * DFMA paths on the current device, TFLOP/s (the roofline denominator of
- * the FP64 path; MEASURED_PEAKS.json has no FP64 figure).
+ * Measurement helpers (roofline denominators measured on the device):
+ * FP64 throughput of the tensor (mma.sync f64) and DFMA paths, TFLOP/s, for
+ * the FP64 path; dense INT8 tcgen05 throughput, TOP/s, for the mixed path.
  * ---------------------------------------------------------------------- */
 int negf_probe_fp64_peak(double* dmma_tflops, double* dfma_tflops);
+int negf_probe_int8_peak(double* tops);
 
 #ifdef __cplusplus
 }

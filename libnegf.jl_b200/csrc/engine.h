@@ -45,6 +45,8 @@ struct OzSplitProblem;
 struct OzMmaProblem;
 size_t ozaki_mma_smem_bytes();
 cudaError_t ozaki_prepare();
+// dense INT8 tensor-core throughput of this device, TOP/s
+cudaError_t ozaki_probe_int8(double* tops);
 cudaError_t launch_ozaki_split(const void* probs, int nprob, int max_rows_pad, cudaStream_t st);
 // tile_map: per output tile an int4 (problem, m tile | n tile << 16,
 // K chunks | m tiles << 16, n tiles)

@@ -885,4 +885,11 @@ int negf_probe_fp64_peak(double* dmma_tflops, double* dfma_tflops) {
   return NEGF_SUCCESS;
 }
 
+int negf_probe_int8_peak(double* tops) {
+  if (int r = check_device()) return r;
+  cudaError_t e = ozaki_probe_int8(tops);
+  if (e != cudaSuccess) return cuda_fail(e, "int8 probe");
+  return NEGF_SUCCESS;
+}
+
 }  // extern "C"

@@ -699,6 +699,86 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
   }
 }
 
+// ---------------------------------------------------------------------------
+// measurement: dense INT8 tensor-core throughput of one CTA per SM issuing
+// back-to-back 128 x 256 x 32 kind::i8 MMAs on resident shared-memory
+// operands (the roofline denominator of the product kernel)
+
+__global__ void __launch_bounds__(128, 1) ozaki_probe_kernel(int rounds, int* err) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tm;
+  for (int i = threadIdx.x; i < (4096 + 8192) / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(sm)[i] = 0u;
+  if (threadIdx.x < 32) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(oz_smem(&tm)), "r"(512));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(oz_smem(&bar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::);
+  const uint32_t t = tm;
+  if (threadIdx.x == 0) {
+    const uint64_t da = oz_desc(oz_smem(sm), 128 * 16, 128), db = oz_desc(oz_smem(sm) + 4096, 256 * 16, 128);
+    constexpr uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(256 >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+    for (int it = 0; it < rounds; ++it) {
+#pragma unroll
+      for (int u = 0; u < 32; ++u) {
+        const uint32_t acc = (it > 0 || u >= 2) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+                t + (uint32_t)((u & 1) * 256)),
+            "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+      }
+    }
+    oz_commit(oz_smem(&bar));
+    int dummy = 0;
+    if (!oz_wait(oz_smem(&bar), 0, &dummy, err, false)) atomicExch(err, 1);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::);
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::);
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(t), "r"(512));
+  }
+}
+
+cudaError_t ozaki_probe_int8(double* tops) {
+  int dev = 0, sms = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  constexpr int smem = 16 * 1024, rounds = 625;
+  int* err = nullptr;
+  if ((e = cudaMalloc(&err, sizeof(int))) != cudaSuccess) return e;
+  cudaMemset(err, 0, sizeof(int));
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  ozaki_probe_kernel<<<sms, 128, smem>>>(20, err);
+  cudaEventRecord(a);
+  ozaki_probe_kernel<<<sms, 128, smem>>>(rounds, err);
+  cudaEventRecord(b);
+  cudaEventSynchronize(b);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  int h = 0;
+  cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost);
+  e = cudaGetLastError();
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(err);
+  if (e != cudaSuccess) return e;
+  if (h) return cudaErrorLaunchTimeout;
+  if (tops) *tops = 2.0 * 128 * 256 * 32 * 32.0 * rounds * sms / (ms * 1e9);
+  return cudaSuccess;
+}
+
 size_t ozaki_mma_smem_bytes() { return (size_t)oz::STAGES * oz::STAGE; }
 
 constexpr size_t kSplitSmem = 2 * oz::SPLIT_ROWS * 33 * sizeof(cplx);
