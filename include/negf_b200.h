@@ -203,6 +203,10 @@ typedef struct {
   int32_t max_chunk; /* energies per device-resident batch (0: by HBM budget) */
   double hbm_budget_gb; /* 0: 80% of free device memory */
   int32_t precision; /* NEGF_PREC_FP64 or NEGF_PREC_MIXED */
+  /* Schedule knobs (0: library default); chosen per batch by the autotuner
+   * of the Python layer (libnegf_b200.autotune): */
+  int32_t gemm_form; /* FP64 complex products: 1 = four real products, 2 = 3M (Gauss, default) */
+  int32_t gj_nb;     /* Gauss-Jordan panel width for blocks > 112: 8, 16 or 32 (must fit shared memory) */
 } negf_solve_opts;
 
 /* Precision modes.  FP64: every product in FP64 on the DMMA tensor path.
@@ -224,6 +228,23 @@ int negf_solve(negf_device_t dev, int32_t nE, const double* energies, const negf
  * energies with inputs and outputs kept in device memory. */
 typedef struct negf_solver_s* negf_solver_t;
 int negf_solver_create(negf_device_t dev, int32_t nE, const negf_solve_opts* opts, negf_solver_t* out);
+/* One resident plan for a batch of devices of different layer counts and
+ * block sizes (nE[k] energies of devs[k]): every recursion step is one
+ * batched launch over all (device, energy) pairs that reach it.  The energy
+ * array of negf_solver_set_energies and the outputs are device-major: the
+ * nE[0] energies of devs[0], then those of devs[1], ...; gr/gl hold, per
+ * energy, the diagonal blocks of its device in layer order.  Transmission
+ * needs equal first and last block sizes per device.  (The reference solves
+ * one system and one energy per call; this is the batching of
+ * src/matinvertndiag_rgf.jl:114-200 and src/keldyshndiag.jl:120-317 over
+ * systems.) */
+int negf_solver_create_batch(int32_t ndev, const negf_device_t* devs, const int32_t* nE,
+                             const negf_solve_opts* opts, negf_solver_t* out);
+/* Device bytes a batch solver of these devices / energy counts would
+ * allocate (workspace and outputs, the estimate negf_solve uses to split an
+ * energy list by its HBM budget); for admission control. */
+int negf_batch_bytes(int32_t ndev, const negf_device_t* devs, const int32_t* nE, const negf_solve_opts* opts,
+                     int64_t* bytes);
 int negf_solver_destroy(negf_solver_t s);
 /* energies: host array of nE values (uploaded to a device parameter table). */
 int negf_solver_set_energies(negf_solver_t s, const double* energies, void* stream);

@@ -42,6 +42,11 @@ int gj_panel_width(int max_n) {
   return 8;
 }
 
+int Plan::panel_width(int max_n) const {
+  if (gj_nb_ > 0 && max_n > 112) return gj_nb_;
+  return gj_panel_width(max_n);
+}
+
 int TriSystem::maxb() const {
   int m = 0;
   for (int x : b) m = std::max(m, x);
@@ -220,6 +225,7 @@ void Plan::gemm_fp64(char opA, char opB, const std::vector<ZGemmProblem>& probs)
   s.opA = opA;
   s.opB = opB;
   s.preload = pre;
+  s.form = gemm_form_;
   s.off = push_bytes(v.data(), v.size() * sizeof(ZGemmProblem));
   s.tiles_off = push_bytes(starts.data(), starts.size() * sizeof(int));
   s.count = static_cast<int>(v.size());
@@ -240,7 +246,7 @@ void Plan::inv(const std::vector<InvSpec>& specs) {
     max_n = std::max(max_n, sp.n);
   }
   if (v.empty()) return;
-  int nb = gj_panel_width(max_n);
+  int nb = panel_width(max_n);
   bool blocked = nb < max_n;
   size_t off = push_bytes(v.data(), v.size() * sizeof(ZInvProblem));
   double gj_flops = 0.0;
@@ -493,7 +499,7 @@ cudaError_t Plan::launch_step(const Step& s, const unsigned char* base, cudaStre
     switch (s.kind) {
       case Step::GEMM:
         e = launch_zgemm_batched_ex(s.opA, s.opB, s.preload, reinterpret_cast<const ZGemmProblem*>(base + s.off),
-                                    reinterpret_cast<const int*>(base + s.tiles_off), s.count, s.total_tiles, stream);
+                                    reinterpret_cast<const int*>(base + s.tiles_off), s.count, s.total_tiles, stream, s.form);
         break;
       case Step::GJ_PANEL:
         e = launch_zgj_panel(reinterpret_cast<const ZInvProblem*>(base + s.off), s.count, s.k0, s.nb, s.blocked,
@@ -534,7 +540,7 @@ cudaError_t Plan::launch_step(const Step& s, const unsigned char* base, cudaStre
 void alloc_rgf_work(Plan& plan, const TriSystem& s, RgfWork& w) {
   int n = s.npl();
   int mb = s.maxb();
-  int nb = gj_panel_width(mb);
+  int nb = std::max(plan.panel_width(mb), mb > 112 ? 32 : 0);  // room for any tuned width
   w.g.assign(n, nullptr);
   w.R.assign(n > 0 ? n - 1 : 0, nullptr);
   w.L.assign(n > 0 ? n - 1 : 0, nullptr);

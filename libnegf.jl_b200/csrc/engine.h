@@ -21,7 +21,8 @@ namespace negf {
 cudaError_t launch_zgemm_batched(char opA, char opB, const ZGemmProblem* probs_dev, const int* tile_start_dev,
                                  int nprob, int total_tiles, cudaStream_t stream);
 cudaError_t launch_zgemm_batched_ex(char opA, char opB, bool preload, const ZGemmProblem* probs_dev,
-                                    const int* tile_start_dev, int nprob, int total_tiles, cudaStream_t stream);
+                                    const int* tile_start_dev, int nprob, int total_tiles, cudaStream_t stream,
+                                    int form = 0);
 bool zgemm_preload_ok(const ZGemmProblem& p);
 int zgemm_tiles(int m, int n);
 size_t zgemm_smem_bytes();
@@ -112,6 +113,7 @@ struct Step {
   int count = 0, total_tiles = 0, max_m = 0, max_n = 0;
   int k0 = 0, nb = 0, blocked = 0;
   bool preload = false;  // GEMM: accumulators start from Cin (all problems alpha, beta = +-1)
+  int form = 0;          // GEMM: 0 default, 1 four real products, 2 3M
   size_t smem = 0;
   double flops = 0.0;    // real flops of the step (8mnk per complex GEMM)
 };
@@ -134,6 +136,10 @@ class Plan {
   void gemm_fp64(char opA, char opB, const std::vector<ZGemmProblem>& probs);
   void gemm_mixed(char opA, char opB, const std::vector<ZGemmProblem>& probs);
   void set_mixed(bool on) { mixed_ = on; }
+  // schedule knobs: FP64 GEMM form (0 default, 1 four products, 2 3M) and the
+  // Gauss-Jordan panel width for blocks > 112 (0 default)
+  void set_schedule(int gemm_form, int gj_nb) { gemm_form_ = gemm_form; gj_nb_ = gj_nb; }
+  int panel_width(int max_n) const;
   bool mixed() const { return mixed_; }
   int* error_flag() const { return err_; }
   void inv(const std::vector<InvSpec>& specs);
@@ -165,6 +171,7 @@ class Plan {
   cudaGraphExec_t gexec_ = nullptr;
   cudaStream_t graph_stream_ = nullptr;
   bool mixed_ = false;
+  int gemm_form_ = 0, gj_nb_ = 0;
   int* err_ = nullptr;            // tensor-core wait time-out flag (device int)
   unsigned char* oz_pool_ = nullptr;  // digit-slice scratch shared by all mixed steps
   size_t oz_pool_bytes_ = 0;

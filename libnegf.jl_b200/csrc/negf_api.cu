@@ -141,8 +141,11 @@ struct negf_device_s {
 };
 
 struct negf_solver_s {
-  negf_device_s* dev = nullptr;
-  int nE = 0;
+  negf_device_s* dev = nullptr;             // the first (or only) device
+  std::vector<negf_device_s*> devs;         // devices of the batch, in order
+  std::vector<int> dev_nE;                  // energies per device
+  size_t out_total = 0;                     // elements of gr / gl (all devices and energies)
+  int nE = 0;                               // energies of all devices
   negf_solve_opts opts{};
   std::unique_ptr<Plan> plan;
   cplx* params = nullptr;  // [shift (nE) | f_L (nE) | f_R (nE) | i (1)]
@@ -150,7 +153,7 @@ struct negf_solver_s {
   cplx* gl = nullptr;
   double* t2 = nullptr;    // 2 * nE (re, im)
   int* info = nullptr;
-  size_t per_energy = 0;   // sum b_i^2
+  size_t per_energy = 0;   // sum b_i^2 (single-device solvers; 0 for a multi-device batch)
   std::vector<std::vector<cudaEvent_t>> ev_sets;  // one event set per profiled pass
   size_t ev_used = 0;
   ~negf_solver_s() {
@@ -173,30 +176,70 @@ size_t solver_bytes_per_energy(const negf_device_s& d, const negf_solve_opts& o)
   return c * sizeof(cplx) + 64;
 }
 
+// Opt-in shared memory per block of the current device (bytes).
+size_t max_panel_smem() {
+  int dev = 0, v = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
+  return (size_t)v;
+}
+
+// One plan for every (device, energy) item of the batch: the devices may differ
+// in layer count and block sizes; each batched launch takes the items whose
+// recursion reaches that step. Item e uses parameter slots e (shift), nE + e
+// (f_L), 2 nE + e (f_R) and output blocks at offset off(e) in gr / gl
+// (device-major, then energy, then layer).
 int build_solver(negf_solver_s& S) {
-  negf_device_s& d = *S.dev;
-  const int n = d.npl;
   const int nE = S.nE;
   Plan& plan = *S.plan;
-  S.per_energy = 0;
-  for (int x : d.b) S.per_energy += (size_t)x * x;
+  struct Item {
+    negf_device_s* d;
+    size_t off;
+  };
+  std::vector<Item> items;
+  size_t off = 0;
+  for (size_t k = 0; k < S.devs.size(); ++k) {
+    size_t pe = 0;
+    for (int x : S.devs[k]->b) pe += (size_t)x * x;
+    for (int e = 0; e < S.dev_nE[k]; ++e) {
+      items.push_back({S.devs[k], off});
+      off += pe;
+    }
+  }
+  if ((int)items.size() != nE) return fail(NEGF_ERR_INVALID, "energy counts do not add up");
+  S.out_total = off;
+  S.per_energy = S.devs.size() == 1 ? off / (size_t)nE : 0;
   S.params = plan.alloc_c(3 * (size_t)nE + 1);
   S.info = static_cast<int*>(plan.alloc(sizeof(int) * nE));
-  if (S.opts.want_gr) S.gr = plan.alloc_c(S.per_energy * nE);
-  if (S.opts.want_gl) S.gl = plan.alloc_c(S.per_energy * nE);
+  if (S.opts.want_gr) S.gr = plan.alloc_c(S.out_total);
+  if (S.opts.want_gl) S.gl = plan.alloc_c(S.out_total);
   if (S.opts.want_t) S.t2 = static_cast<double*>(plan.alloc(sizeof(double) * 2 * nE));
   const cplx i_unit = make_double2(0.0, 1.0);
   NEGF_TRY_CUDA(cudaMemcpy(S.params + 3 * nE, &i_unit, sizeof(cplx), cudaMemcpyHostToDevice), "solver params");
   if (S.opts.precision != NEGF_PREC_FP64 && S.opts.precision != NEGF_PREC_MIXED)
     return fail(NEGF_ERR_INVALID, "precision must be NEGF_PREC_FP64 or NEGF_PREC_MIXED");
-  for (int x : d.b)
-    if (S.opts.precision == NEGF_PREC_MIXED && x > 1024)
-      return fail(NEGF_ERR_INVALID, "the mixed precision mode supports blocks up to 1024");
+  for (negf_device_s* dv : S.devs) {
+    for (int x : dv->b)
+      if (S.opts.precision == NEGF_PREC_MIXED && x > 1024)
+        return fail(NEGF_ERR_INVALID, "the mixed precision mode supports blocks up to 1024");
+    if (S.opts.want_t && dv->b.front() != dv->b.back())
+      return fail(NEGF_ERR_INVALID, "transmission needs equal first and last block sizes");
+  }
   plan.set_mixed(S.opts.precision == NEGF_PREC_MIXED);
+  if (S.opts.gemm_form < 0 || S.opts.gemm_form > 2) return fail(NEGF_ERR_INVALID, "gemm_form must be 0, 1 or 2");
+  if (S.opts.gj_nb != 0 && S.opts.gj_nb != 8 && S.opts.gj_nb != 16 && S.opts.gj_nb != 32)
+    return fail(NEGF_ERR_INVALID, "gj_nb must be 0, 8, 16 or 32");
+  for (negf_device_s* dv : S.devs)
+    for (int x : dv->b)
+      if (S.opts.gj_nb > 0 && x > 112 && zgj_panel_smem_bytes(x, S.opts.gj_nb) > max_panel_smem())
+        return fail(NEGF_ERR_INVALID, "gj_nb too wide for the block size (shared memory)");
+  plan.set_schedule(S.opts.gemm_form, S.opts.gj_nb);
 
   std::vector<TriSystem> sys(nE);
   std::vector<RgfWork> work(nE);
   for (int e = 0; e < nE; ++e) {
+    const negf_device_s& d = *items[e].d;
+    const int n = d.npl;
     TriSystem& t = sys[e];
     t.b = d.b;
     for (int i = 0; i < n; ++i) { t.D.push_back(d.D[i]); t.ldD.push_back(d.b[i]); }
@@ -214,9 +257,10 @@ int build_solver(negf_solver_s& S) {
   }
   // block pointers inside the output arrays
   auto out_blocks = [&](cplx* base, int e) {
+    const negf_device_s& d = *items[e].d;
     std::vector<cplx*> v;
-    size_t o = (size_t)e * S.per_energy;
-    for (int i = 0; i < n; ++i) { v.push_back(base + o); o += (size_t)d.b[i] * d.b[i]; }
+    size_t o = items[e].off;
+    for (int i = 0; i < d.npl; ++i) { v.push_back(base + o); o += (size_t)d.b[i] * d.b[i]; }
     return v;
   };
   std::vector<HermBlocks> herm(nE);
@@ -224,6 +268,8 @@ int build_solver(negf_solver_s& S) {
     // Sigma^in = f_L Gamma_L (+) f_R Gamma_R in Hermitian storage
     std::vector<ZBlockOp> zero, setL, addR;
     for (int e = 0; e < nE; ++e) {
+      const negf_device_s& d = *items[e].d;
+      const int n = d.npl;
       HermBlocks& h = herm[e];
       h.d = out_blocks(S.gl, e);
       for (int i = 0; i < n; ++i) h.ldd.push_back(d.b[i]);
@@ -255,12 +301,13 @@ int build_solver(negf_solver_s& S) {
   if (S.opts.want_gr) {
     std::vector<TriOut> out(nE);
     for (int e = 0; e < nE; ++e) {
+      const negf_device_s& d = *items[e].d;
       TriOut& o = out[e];
       o.d = out_blocks(S.gr, e);
-      for (int i = 0; i < n; ++i) o.ldd.push_back(d.b[i]);
+      for (int i = 0; i < d.npl; ++i) o.ldd.push_back(d.b[i]);
       int mb = sys[e].maxb();
       cplx* ring = plan.alloc_c(4 * (size_t)mb * mb);
-      for (int i = 0; i + 1 < n; ++i) {
+      for (int i = 0; i + 1 < d.npl; ++i) {
         o.u.push_back(ring + (size_t)(i % 2) * mb * mb);
         o.l.push_back(ring + (size_t)(2 + i % 2) * mb * mb);
         o.ldu.push_back(d.b[i]);
@@ -273,31 +320,36 @@ int build_solver(negf_solver_s& S) {
     build_rkd(plan, sys, work, herm);
     // G^< = i G^n
     std::vector<ZBlockOp> sc;
-    for (int e = 0; e < nE; ++e)
-      for (int i = 0; i < n; ++i) {
+    for (int e = 0; e < nE; ++e) {
+      const negf_device_s& d = *items[e].d;
+      for (int i = 0; i < d.npl; ++i) {
         ZBlockOp o{}; o.A = herm[e].d[i]; o.lda = d.b[i]; o.C = herm[e].d[i]; o.ldc = d.b[i];
         o.m = o.n = d.b[i]; o.kind = ZOP_AXPBY; o.alpha_ptr = S.params + 3 * nE; o.beta = make_double2(0.0, 0.0);
         sc.push_back(o);
       }
+    }
     plan.blockops(sc);
   }
   if (S.opts.want_t) {
     // G^R_{1N} by G_{1,j} = -G_{1,j-1} R_{j-1}, G_{1,1} = g_1 (rgf.jl:169, :185-199)
-    const int b0 = d.b[0], bN = d.b[n - 1];
     std::vector<std::vector<cplx*>> Y(nE);
     std::vector<cplx*> P(nE), Q(nE);
-    int mb = 0;
-    for (int x : d.b) mb = std::max(mb, x);
+    int maxN = 0;
     for (int e = 0; e < nE; ++e) {
+      const int mb = sys[e].maxb();
+      maxN = std::max(maxN, items[e].d->npl);
       cplx* a = plan.alloc_c(4 * (size_t)mb * mb);
       Y[e] = {a, a + (size_t)mb * mb};
       P[e] = a + 2 * (size_t)mb * mb;
       Q[e] = a + 3 * (size_t)mb * mb;
     }
     auto ycur = [&](int e, int j) -> const cplx* { return j == 0 ? work[e].g[0] : Y[e][j % 2]; };
-    for (int j = 1; j < n; ++j) {
+    for (int j = 1; j < maxN; ++j) {
       std::vector<ZGemmProblem> pr;
       for (int e = 0; e < nE; ++e) {
+        const negf_device_s& d = *items[e].d;
+        if (j >= d.npl) continue;
+        const int b0 = d.b[0];
         ZGemmProblem p{};
         p.A = ycur(e, j - 1); p.lda = b0;
         p.B = work[e].R[j - 1]; p.ldb = d.b[j - 1];
@@ -311,6 +363,8 @@ int build_solver(negf_solver_s& S) {
     std::vector<ZGemmProblem> p1, p2;
     std::vector<ZTraceProblemHost> tr;
     for (int e = 0; e < nE; ++e) {
+      const negf_device_s& d = *items[e].d;
+      const int n = d.npl, b0 = d.b[0], bN = d.b[n - 1];
       const cplx* G1N = ycur(e, n - 1);
       ZGemmProblem a{};  // P = Gamma_L G1N  (b0 x bN)
       a.A = d.gamL; a.lda = b0; a.B = G1N; a.ldb = b0; a.C = P[e]; a.ldc = b0; a.ldcin = 1;
@@ -323,7 +377,6 @@ int build_solver(negf_solver_s& S) {
       ZTraceProblemHost t{};
       t.X = P[e]; t.ldx = b0; t.Y = Q[e]; t.ldy = bN; t.n = b0; t.out = S.t2 + 2 * e;
       tr.push_back(t);
-      if (b0 != bN) return fail(NEGF_ERR_INVALID, "transmission needs equal first and last block sizes");
     }
     plan.gemm('N', 'N', p1);
     plan.gemm('N', 'C', p2);
@@ -657,6 +710,8 @@ int negf_solver_create(negf_device_t dev, int32_t nE, const negf_solve_opts* opt
   if (!dev || nE <= 0 || !opts || !out) return fail(NEGF_ERR_INVALID, "bad arguments");
   std::unique_ptr<negf_solver_s> s(new negf_solver_s);
   s->dev = dev;
+  s->devs = {dev};
+  s->dev_nE = {nE};
   s->nE = nE;
   s->opts = *opts;
   s->plan.reset(new Plan);
@@ -666,6 +721,41 @@ int negf_solver_create(negf_device_t dev, int32_t nE, const negf_solve_opts* opt
     return fail(NEGF_ERR_NOMEM, "device allocation failed (reduce the number of energies per batch)");
   }
   *out = s.release();
+  return NEGF_SUCCESS;
+}
+
+int negf_solver_create_batch(int32_t ndev, const negf_device_t* devs, const int32_t* nE,
+                             const negf_solve_opts* opts, negf_solver_t* out) {
+  if (int r = check_device()) return r;
+  if (ndev <= 0 || !devs || !nE || !opts || !out) return fail(NEGF_ERR_INVALID, "bad arguments");
+  std::unique_ptr<negf_solver_s> s(new negf_solver_s);
+  for (int k = 0; k < ndev; ++k) {
+    if (!devs[k] || nE[k] <= 0) return fail(NEGF_ERR_INVALID, "every device needs a handle and nE > 0");
+    s->devs.push_back(devs[k]);
+    s->dev_nE.push_back(nE[k]);
+    s->nE += nE[k];
+  }
+  s->dev = devs[0];
+  s->opts = *opts;
+  s->plan.reset(new Plan);
+  try {
+    if (int r = build_solver(*s)) return r;
+  } catch (const std::bad_alloc&) {
+    return fail(NEGF_ERR_NOMEM, "device allocation failed (split the batch)");
+  }
+  *out = s.release();
+  return NEGF_SUCCESS;
+}
+
+int negf_batch_bytes(int32_t ndev, const negf_device_t* devs, const int32_t* nE, const negf_solve_opts* opts,
+                     int64_t* bytes) {
+  if (ndev < 0 || (ndev > 0 && (!devs || !nE)) || !opts || !bytes) return fail(NEGF_ERR_INVALID, "bad arguments");
+  size_t total = 0;
+  for (int k = 0; k < ndev; ++k) {
+    if (!devs[k] || nE[k] < 0) return fail(NEGF_ERR_INVALID, "bad device or energy count");
+    total += (size_t)nE[k] * solver_bytes_per_energy(*devs[k], *opts);
+  }
+  *bytes = (int64_t)total;
   return NEGF_SUCCESS;
 }
 
@@ -744,7 +834,7 @@ int negf_solver_profile_read(negf_solver_t s, double* ms, double* flops, int64_t
 int negf_solver_download(negf_solver_t s, void* gr_host, void* gl_host, double* t_host, void* stream) {
   if (!s) return fail(NEGF_ERR_INVALID, "NULL solver");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const size_t bytes = (size_t)s->nE * s->per_energy * sizeof(cplx);
+  const size_t bytes = s->out_total * sizeof(cplx);
   if (gr_host && s->gr) NEGF_TRY_CUDA(cudaMemcpyAsync(gr_host, s->gr, bytes, cudaMemcpyDeviceToHost, st), "download");
   if (gl_host && s->gl) NEGF_TRY_CUDA(cudaMemcpyAsync(gl_host, s->gl, bytes, cudaMemcpyDeviceToHost, st), "download");
   if (t_host && s->t2)

@@ -420,9 +420,10 @@ bool zgemm_preload_ok(const ZGemmProblem& p) {
 // counts).  preload may only be set when zgemm_preload_ok holds for every
 // problem of the launch.
 cudaError_t launch_zgemm_batched_ex(char opA, char opB, bool preload, const ZGemmProblem* probs_dev,
-                                    const int* tile_start_dev, int nprob, int total_tiles, cudaStream_t stream) {
+                                    const int* tile_start_dev, int nprob, int total_tiles, cudaStream_t stream,
+                                    int form) {
   if (nprob <= 0 || total_tiles <= 0) return cudaSuccess;
-  const bool g3m = use_3m();
+  const bool g3m = form == 0 ? use_3m() : form == 2;
   pick_kernel(opA, opB, preload, g3m)<<<total_tiles, g3m ? gemm3m::THREADS : gemm::THREADS, gemm::SMEM_BYTES,
                                         stream>>>(probs_dev, tile_start_dev, nprob);
   return cudaGetLastError();

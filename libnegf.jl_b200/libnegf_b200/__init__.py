@@ -11,6 +11,6 @@ Layers:
 from ._lib import load, NegfError, SingularError, LIB_PATH  # noqa: F401
 from .blockmatrix import *  # noqa: F401,F403
 from .algorithms import *  # noqa: F401,F403
-from .negf import Device, Solver, make_opts  # noqa: F401
+from .negf import BatchSolver, Device, Solver, make_opts  # noqa: F401
 
 __version__ = "1.0"

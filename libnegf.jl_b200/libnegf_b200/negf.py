@@ -26,15 +26,18 @@ def _host_blocks(blocks):
 
 
 def make_opts(eta=1e-6, mu_l=0.1, mu_r=-0.1, kT=0.025, want_gr=True, want_gl=True, want_t=True, max_chunk=0,
-              hbm_budget_gb=0.0, precision="fp64"):
+              hbm_budget_gb=0.0, precision="fp64", gemm_form=0, gj_nb=0):
     """precision: "fp64" (every product in FP64) or "mixed" (Schur products on
-    the INT8 tensor cores with FP64-accurate digit splitting)."""
+    the INT8 tensor cores with FP64-accurate digit splitting).  gemm_form /
+    gj_nb: schedule knobs (0 = library default; see libnegf_b200.autotune)."""
     o = _lib.SolveOpts()
     o.eta, o.mu_l, o.mu_r, o.kT = eta, mu_l, mu_r, kT
     o.want_gr, o.want_gl, o.want_t = int(want_gr), int(want_gl), int(want_t)
     o.max_chunk = int(max_chunk)
     o.hbm_budget_gb = float(hbm_budget_gb)
     o.precision = {"fp64": _lib.NEGF_PREC_FP64, "mixed": _lib.NEGF_PREC_MIXED}[precision]
+    o.gemm_form = int(gemm_form)
+    o.gj_nb = int(gj_nb)
     return o
 
 
@@ -113,6 +116,8 @@ class Solver:
 
     def __init__(self, device, nE, **kw):
         self.device = device
+        self.devices = [device]
+        self.counts = [int(nE)]
         self.nE = int(nE)
         self.opts = make_opts(**kw)
         self._h = ctypes.c_void_p()
@@ -164,6 +169,17 @@ class Solver:
         check(load().negf_solver_stats(self._h, ctypes.byref(f), ctypes.byref(n), ctypes.byref(w)))
         return {"flops": f.value, "launches": n.value, "workspace_bytes": w.value}
 
+    def layout(self):
+        """(device index, energy index within the device, element offset) of every
+        energy's output blocks in gr / gl (device-major)."""
+        out, off = [], 0
+        for k, (d, n) in enumerate(zip(self.devices, self.counts)):
+            per = sum(b * b for b in d.sizes)
+            for e in range(n):
+                out.append((k, e, off))
+                off += per
+        return out, off
+
     def close(self):
         if self._h:
             load().negf_solver_destroy(self._h)
@@ -174,3 +190,51 @@ class Solver:
             self.close()
         except Exception:
             pass
+
+
+class BatchSolver(Solver):
+    """One resident plan over several devices of different layer counts and
+    block sizes (counts[k] energies of devices[k]); energies and outputs are
+    device-major (see negf_solver_create_batch)."""
+
+    def __init__(self, devices, counts, **kw):
+        self.devices = list(devices)
+        self.device = self.devices[0]
+        self.counts = [int(c) for c in counts]
+        self.nE = sum(self.counts)
+        self.opts = make_opts(**kw)
+        self._h = ctypes.c_void_p()
+        handles = (ctypes.c_void_p * len(self.devices))(*[d.handle.value for d in self.devices])
+        cnt = (ctypes.c_int32 * len(self.counts))(*self.counts)
+        check(load().negf_solver_create_batch(len(self.devices), handles, cnt, ctypes.byref(self.opts),
+                                              ctypes.byref(self._h)))
+
+    def host_outputs(self, stream=None):
+        """Download everything and split it: (gr, gl, t) with gr[k][e][i] the
+        diagonal block i of energy e of device k (numpy), t[k][e] real."""
+        lay, total = self.layout()
+        gr = np.empty(total, dtype=np.complex128) if self.opts.want_gr else None
+        gl = np.empty(total, dtype=np.complex128) if self.opts.want_gl else None
+        t2 = np.empty(2 * self.nE, dtype=np.float64) if self.opts.want_t else None
+        self.download(gr.ctypes.data if gr is not None else None, gl.ctypes.data if gl is not None else None,
+                      t2.ctypes.data if t2 is not None else None, stream)
+
+        def split(flat):
+            if flat is None:
+                return None
+            res = [[None] * n for n in self.counts]
+            for (k, e, off) in lay:
+                row, o = [], off
+                for b in self.devices[k].sizes:
+                    row.append(flat[o:o + b * b].reshape(b, b, order="F"))
+                    o += b * b
+                res[k][e] = row
+            return res
+
+        t = None
+        if t2 is not None:
+            t, g = [], 0
+            for n in self.counts:
+                t.append(t2[0::2][g:g + n])
+                g += n
+        return split(gr), split(gl), t
