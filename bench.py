@@ -58,6 +58,14 @@ def parse():
     ap.add_argument("--cpu-budget-s", type=float, default=12.0, help="time budget of each CPU baseline mode")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg4", "cfg5"],
+                    help="cfg2 (default, the headline line); cfg4: a bounded sample of the uneven batch (systems "
+                         "of N in U{8..96}, b in {32..384}, 16 energies each); cfg5: a bounded sample of the "
+                         "Poisson-arrival request stream through the server (p50/p99 latency)")
+    ap.add_argument("--systems", type=int, default=96, help="cfg4: number of systems in the sample")
+    ap.add_argument("--requests", type=int, default=16, help="cfg5: number of requests in the sample")
+    ap.add_argument("--rate", type=float, default=2.0, help="cfg5: mean arrival rate, requests/s")
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"], help="cfg4 / cfg5 precision")
     ap.add_argument("--launch-list", action="store_true",
                     help="only two launch-by-launch passes of the mixed solver (for an ncu launch list: skip the "
                          "first pass's launches, capture the second's); prints no bench line")
@@ -461,10 +469,98 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_cfg4(args):
+    """Uneven batch: seeded systems with N ~ U{8..96}, b in {32,64,128,192,256,384}
+    (first = last block for T), 16 energies each, through the budget-packed
+    scheduler with autotuned knobs; device time of the solves only."""
+    import torch
+    import libnegf_b200 as negf
+    from libnegf_b200.batch import solve_uneven
+    from oracle import physics
+    rng = np.random.default_rng(4)
+    specs = [(int(rng.integers(8, 97)), int(rng.choice([32, 64, 128, 192, 256, 384]))) for _ in range(args.systems)]
+    devs = []
+    for k, (n, b) in enumerate(specs):
+        s = physics.physics_system(n, b, seed=1000 + k)
+        devs.append(negf.Device(s.Hd, s.Hu, s.sigL, s.sigR))
+    energies = [np.linspace(-0.9, 0.9, 16) + 1e-3 * k for k in range(len(devs))]
+    flops = sum(canonical_flops(n, b) * 16 for n, b in specs)
+    clk = ClockSampler(torch.cuda.current_device())
+    with clk:
+        st = solve_uneven(devs, energies, precision=args.precision, eta=1e-6)
+    print(json.dumps({"metric": "energy pts/s (uneven batch)", "value": st["pts_per_s_device"], "unit": UNIT,
+                      "wall_pts_per_s": st["pts_per_s_wall"], "n_gpus": 1, "dtype": args.precision,
+                      "data": "synthetic (seeded)",
+                      "config": {"workload": "uneven batch, bounded sample of %d systems (N in U{8..96}, b in "
+                                             "{32,64,128,192,256,384}), 16 energies each" % len(devs),
+                                 "groups": st["groups"], "budget_gb": st["budget_bytes"] / 1e9,
+                                 "knobs": st["knobs"]},
+                      "energy_points": st["energy_points"], "device_ms": st["device_ms"],
+                      "algorithmic_tflops": flops / (st["device_ms"] / 1000.0) / 1e12,
+                      "tuning_ms_per_pass": [(c, t) for c, t in (st["tuning"] or [])],
+                      "clocks": clk.summary()}), flush=True)
+    for d in devs:
+        d.close()
+
+
+def run_cfg5(args):
+    """Request stream: seeded requests (N in {16..128}, b in {64..512}, energy
+    lists of 32..1024 scaled to a bounded sample) arriving as a Poisson process
+    at --rate, served by NegfServer; latency = arrival to completion."""
+    import torch
+    from libnegf_b200.server import NegfServer
+    from oracle import physics
+    rng = np.random.default_rng(5)
+    reqs = []
+    for k in range(args.requests):
+        n = int(rng.integers(16, 129))
+        b = int(rng.choice([64, 128, 192, 256, 384, 512]))
+        ne = int(rng.integers(32, 1025)) // 8  # bounded sample: 1/8 of the energy-list length
+        s = physics.physics_system(n, b, seed=2000 + k)
+        reqs.append((s, np.linspace(-0.9, 0.9, ne)))
+    gaps = rng.exponential(1.0 / args.rate, size=len(reqs))
+    srv = NegfServer(precision=args.precision, eta=1e-6)
+    # tune once per block-size class before the clock starts (a long-running
+    # server carries its tuning cache)
+    from libnegf_b200.autotune import autotune
+    from libnegf_b200.negf import Device
+    for b in sorted({len(s.Hd[0]) for s, _ in reqs}):
+        s0 = physics.physics_system(4, b, seed=1)
+        d0 = Device(s0.Hd, s0.Hu, s0.sigL, s0.sigR)
+        autotune([d0], [4], precision=args.precision)
+        d0.close()
+    handles = []
+    clk = ClockSampler(torch.cuda.current_device())
+    with clk:
+        t0 = time.perf_counter()
+        for (s, E), gap in zip(reqs, gaps):
+            time.sleep(gap)
+            handles.append(srv.submit(s.Hd, s.Hu, s.sigL, s.sigR, E))
+        for h in handles:
+            h.wait(timeout=1800)
+        wall = time.perf_counter() - t0
+    lat = srv.latency_stats()
+    pts = sum(len(E) for _, E in reqs)
+    print(json.dumps({"metric": "energy pts/s and p50/p99 solve latency (request stream)", "value": pts / wall,
+                      "unit": UNIT, "p50_s": lat["p50_s"], "p99_s": lat["p99_s"], "mean_latency_s": lat["mean_s"],
+                      "device_pts_per_s": pts / (srv.device_ms / 1000.0), "n_gpus": 1, "dtype": args.precision,
+                      "data": "synthetic (seeded)",
+                      "config": {"workload": "bounded sample of the request stream: %d requests, N in {16..128}, "
+                                             "b in {64..512}, energy lists of 4..128 (1/8 of 32..1024), Poisson "
+                                             "arrivals at %.2f/s" % (len(reqs), args.rate),
+                                 "groups": srv.groups, "budget_gb": srv.budget / 1e9},
+                      "clocks": clk.summary()}), flush=True)
+    srv.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "cfg4":
+        run_cfg4(args)
+    elif args.workload == "cfg5":
+        run_cfg5(args)
     else:
         run_ours(args)
 

@@ -173,7 +173,15 @@ size_t solver_bytes_per_energy(const negf_device_s& d, const negf_solve_opts& o)
   if (o.want_gr) c += sb2 + 4 * mb * mb;              // G^R diagonal + rings
   if (o.want_gl) c += sb2 + sbb + 3 * n * mb * mb;    // G^n storage + RKD scratch
   if (o.want_t) c += 4 * mb * mb;
-  return c * sizeof(cplx) + 64;
+  size_t bytes = c * sizeof(cplx) + 64;
+  if (o.precision == NEGF_PREC_MIXED) {
+    // digit slices of the INT8 products (21 bytes per padded element): the
+    // widest steps (the Keldysh per-layer products of all layers at once)
+    // split about three operands per layer
+    const size_t pad = (mb + 127) / 128 * 128;
+    bytes += 21 * 3 * n * pad * pad;
+  }
+  return bytes;
 }
 
 // Opt-in shared memory per block of the current device (bytes).

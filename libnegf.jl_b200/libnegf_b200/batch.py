@@ -18,7 +18,7 @@ import time
 import numpy as np
 
 from . import _lib
-from ._lib import check, load
+from ._lib import NegfError, check, load
 from .negf import BatchSolver, make_opts
 
 
@@ -60,6 +60,24 @@ def pack(items, budget):
     return groups
 
 
+def halve(group):
+    """Split a group's energies into a first and a second half, in order (the
+    item at the boundary is split)."""
+    total = sum(c for _, _, c in group)
+    half = max(1, total // 2)
+    first, second, acc = [], [], 0
+    for k, s, c in group:
+        if acc >= half:
+            second.append((k, s, c))
+            continue
+        take = min(c, half - acc)
+        first.append((k, s, take))
+        if take < c:
+            second.append((k, s + take, c - take))
+        acc += take
+    return [g for g in (first, second) if g]
+
+
 def default_budget():
     import torch
     free, _ = torch.cuda.mem_get_info()
@@ -87,11 +105,20 @@ def solve_uneven(devices, energies, precision="fp64", budget_bytes=None, tune=Tr
     st = stream or torch.cuda.Stream()
     sh = st.cuda_stream
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    dev_ms, pts = 0.0, 0
+    dev_ms, pts, solved = 0.0, 0, 0
     t0 = time.perf_counter()
-    for g in groups:
-        solver = BatchSolver([devices[k] for k, _, _ in g], [c for _, _, c in g], precision=precision, **phys,
-                             **knobs)
+    pending = list(groups)
+    while pending:
+        g = pending.pop(0)
+        try:
+            solver = BatchSolver([devices[k] for k, _, _ in g], [c for _, _, c in g], precision=precision, **phys,
+                                 **knobs)
+        except NegfError as exc:
+            # the estimate was short: halve the group and retry
+            if exc.code != _lib.NEGF_ERR_NOMEM or sum(c for _, _, c in g) <= 1:
+                raise
+            pending[:0] = halve(g)
+            continue
         try:
             solver.set_energies(np.concatenate([np.asarray(energies[k][s:s + c], dtype=np.float64)
                                                 for k, s, c in g]), sh)
@@ -102,11 +129,12 @@ def solve_uneven(devices, energies, precision="fp64", budget_bytes=None, tune=Tr
             solver.check()
             dev_ms += ev0.elapsed_time(ev1)
             pts += solver.nE
+            solved += 1
             if on_group is not None:
                 on_group(solver, g)
         finally:
             solver.close()
     wall = time.perf_counter() - t0
-    return {"groups": len(groups), "energy_points": pts, "device_ms": dev_ms, "wall_s": wall,
+    return {"groups": solved, "energy_points": pts, "device_ms": dev_ms, "wall_s": wall,
             "pts_per_s_device": pts / (dev_ms / 1000.0) if dev_ms else None, "pts_per_s_wall": pts / wall,
             "knobs": knobs, "tuning": table, "budget_bytes": budget}

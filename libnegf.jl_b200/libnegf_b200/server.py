@@ -23,6 +23,7 @@ import time
 
 import numpy as np
 
+from ._lib import NEGF_ERR_NOMEM, NegfError
 from .batch import bytes_per_energy, default_budget, pack
 from .negf import BatchSolver, Device
 
@@ -147,8 +148,18 @@ class NegfServer:
                 from .autotune import autotune
                 knobs, _ = autotune(devs, [c for _, _, c in group], precision=self.precision, eta=self.phys["eta"])
             try:
-                solver = BatchSolver(devs, [c for _, _, c in group], precision=self.precision, want_gr=want_blocks,
-                                     want_gl=want_blocks, want_t=True, **self.phys, **knobs)
+                try:
+                    solver = BatchSolver(devs, [c for _, _, c in group], precision=self.precision,
+                                         want_gr=want_blocks, want_gl=want_blocks, want_t=True, **self.phys, **knobs)
+                except NegfError as exc:
+                    if exc.code != NEGF_ERR_NOMEM or sum(c for _, _, c in group) <= 1:
+                        raise
+                    # the estimate was short: requeue the group, halve the budget
+                    with self._lock:
+                        for item in reversed(group):
+                            self._queue.appendleft(item)
+                        self.budget = max(1, self.budget // 2)
+                    continue
                 try:
                     solver.set_energies(np.concatenate([r.energies[s:s + c] for r, s, c in group]), sh)
                     ev0.record(self._stream)

@@ -40,3 +40,14 @@ def test_counts_are_conserved(budget):
     for k, s, c in _flatten(pack(items, budget)):
         got[k] = got.get(k, 0) + c
     assert got == total
+
+
+def test_halve_conserves_and_orders():
+    from libnegf_b200.batch import halve
+    g = [(0, 0, 3), (1, 2, 5), (2, 0, 1)]
+    a, b = halve(g)
+    got = {}
+    for k, s, c in a + b:
+        got.setdefault(k, []).append((s, c))
+    assert got == {0: [(0, 3)], 1: [(2, 1), (3, 4)], 2: [(0, 1)]}
+    assert sum(c for _, _, c in a) == 4
