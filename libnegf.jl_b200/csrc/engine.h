@@ -49,6 +49,13 @@ cudaError_t ozaki_prepare();
 // dense INT8 tensor-core throughput of this device, TOP/s
 cudaError_t ozaki_probe_int8(double* tops);
 cudaError_t launch_ozaki_split(const void* probs, int nprob, int max_rows_pad, cudaStream_t st);
+// CSC <-> band blocks on the device (csc.cu); block table slot 3 i + (j - i + 1)
+cudaError_t launch_csc_scatter(int n, const int* colptr, const int* rowval, const cplx* nz, int nnz, const int* blk_of,
+                               const int* off, const int* bsz, cplx* const* blocks, int hermitian, cudaStream_t st);
+cudaError_t launch_csc_band_out(int pass, int n, int npl, int wout, const int* blk_of, const int* off, const int* bsz,
+                                const cplx* const* res, const int* colptr_in, const int* rowval_in,
+                                const cplx* nz_in, int nnz_in, int* counts, const int* colptr_out, int* rowval_out,
+                                cplx* nz_out, cudaStream_t st);
 // tile_map: per output tile an int4 (problem, m tile | n tile << 16,
 // K chunks | m tiles << 16, n tiles)
 cudaError_t launch_ozaki_mma(const void* probs, const void* tile_map, int total_tiles, int* err, cudaStream_t st);

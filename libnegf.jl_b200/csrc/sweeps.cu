@@ -558,133 +558,136 @@ CCscMatrix run_bndiag_wrapper(int32_t m, int32_t n, int32_t nnz_in, int32_t* col
   std::vector<int> blk_of(n);
   for (int i = 0; i < npl; ++i)
     for (int r = off[i]; r < off[i + 1]; ++r) blk_of[r] = i;
-  // host blocks of the tridiagonal band (column-major)
-  std::map<std::pair<int, int>, std::vector<cplx>> H;
-  auto getb = [&](int i, int j) -> std::vector<cplx>& {
-    auto& v = H[{i, j}];
-    if (v.empty()) v.assign((size_t)b[i] * b[j], make_double2(0.0, 0.0));
-    return v;
-  };
-  for (int i = 0; i < npl; ++i) {
-    getb(i, i);
-    if (i + 1 < npl) { getb(i, i + 1); getb(i + 1, i); }
-  }
-  const cplx* nz = static_cast<const cplx*>(nzval_in);
-  for (int c = 0; c < n; ++c)
-    for (int p = colptr_in[c]; p < colptr_in[c + 1]; ++p) {
-      int r = rowval_in[p];
-      if (r < 0 || r >= n || p < 0 || p >= nnz_in) continue;
-      int bi = blk_of[r], bj = blk_of[c];
-      if (std::abs(bi - bj) > 1) continue;
-      if (is_hermitian && bi > bj) continue;  // Hermitian storage: diagonal + upper
-      getb(bi, bj)[(r - off[bi]) + (size_t)(c - off[bj]) * b[bi]] = nz[p];
-    }
-  if (is_hermitian)
-    for (int i = 0; i + 1 < npl; ++i) {
-      auto& u = H[{i, i + 1}];
-      auto& l = H[{i + 1, i}];
-      for (int r = 0; r < b[i]; ++r)
-        for (int c = 0; c < b[i + 1]; ++c) l[c + (size_t)r * b[i + 1]] = cconj(u[r + (size_t)c * b[i]]);
-    }
-  // device blocks
+  // device buffers: the CSC input, index tables, one arena for the input and
+  // result band blocks (the conversions run on the device; the reference
+  // converts on the host, src/blockmatrix.jl:34-127)
   std::vector<void*> owned;
   auto cleanup = [&]() {
     for (void* p : owned) cudaFree(p);
   };
-  auto up = [&](const std::vector<cplx>& v) -> void* {
+  auto dalloc = [&](size_t bytes) -> void* {
     void* p = nullptr;
-    if (cudaMalloc(&p, v.size() * sizeof(cplx)) != cudaSuccess) return nullptr;
-    owned.push_back(p);
-    if (cudaMemcpy(p, v.data(), v.size() * sizeof(cplx), cudaMemcpyHostToDevice) != cudaSuccess) return nullptr;
-    return p;
-  };
-  auto zal = [&](size_t cnt) -> void* {
-    void* p = nullptr;
-    if (cudaMalloc(&p, cnt * sizeof(cplx)) != cudaSuccess) return nullptr;
+    if (cudaMalloc(&p, std::max<size_t>(bytes, 16)) != cudaSuccess) return nullptr;
     owned.push_back(p);
     return p;
   };
-  std::vector<void*> Md(npl), Mu(npl > 1 ? npl - 1 : 1), Ml(npl > 1 ? npl - 1 : 1), Gd(npl),
-      Gu(npl > 1 ? npl - 1 : 1), Gl(npl > 1 ? npl - 1 : 1);
-  for (int i = 0; i < npl; ++i) {
-    Md[i] = up(H[{i, i}]);
-    Gd[i] = zal((size_t)b[i] * b[i]);
-    if (!Md[i] || !Gd[i]) { cleanup(); fail(NEGF_ERR_NOMEM, "run_bndiag_wrapper: device allocation failed"); return bad; }
+  auto oom = [&]() {
+    cleanup();
+    fail(NEGF_ERR_NOMEM, "run_bndiag_wrapper: device allocation failed");
+    return bad;
+  };
+  auto cerr = [&](cudaError_t e) {
+    cleanup();
+    cuda_fail(e, "run_bndiag_wrapper");
+    return bad;
+  };
+  size_t band = 0;
+  for (int i = 0; i < npl; ++i) band += (size_t)b[i] * b[i];
+  for (int i = 0; i + 1 < npl; ++i) band += 2 * (size_t)b[i] * b[i + 1];
+  int* d_colptr = static_cast<int*>(dalloc(sizeof(int) * (n + 1)));
+  int* d_rowval = static_cast<int*>(dalloc(sizeof(int) * (size_t)std::max(1, nnz_in)));
+  cplx* d_nz = static_cast<cplx*>(dalloc(sizeof(cplx) * (size_t)std::max(1, nnz_in)));
+  int* d_blk = static_cast<int*>(dalloc(sizeof(int) * n));
+  int* d_off = static_cast<int*>(dalloc(sizeof(int) * (npl + 1)));
+  int* d_b = static_cast<int*>(dalloc(sizeof(int) * npl));
+  cplx* arena = static_cast<cplx*>(dalloc(2 * band * sizeof(cplx)));  // input band | result band
+  cplx** d_tab = static_cast<cplx**>(dalloc(sizeof(cplx*) * 6 * npl));
+  int* d_counts = static_cast<int*>(dalloc(sizeof(int) * n));
+  int* d_colptr_out = static_cast<int*>(dalloc(sizeof(int) * (n + 1)));
+  if (!d_colptr || !d_rowval || !d_nz || !d_blk || !d_off || !d_b || !arena || !d_tab || !d_counts || !d_colptr_out)
+    return oom();
+  std::vector<void*> Md(npl), Mu(std::max(1, npl - 1)), Ml(std::max(1, npl - 1)), Gd(npl),
+      Gu(std::max(1, npl - 1)), Gl(std::max(1, npl - 1));
+  std::vector<cplx*> tin(3 * npl, nullptr), tres(3 * npl, nullptr);  // slot 3i + (j - i + 1)
+  {
+    size_t o = 0;
+    auto take = [&](size_t cnt) { cplx* p = arena + o; o += cnt; return p; };
+    for (int i = 0; i < npl; ++i) {
+      tin[3 * i + 1] = static_cast<cplx*>(Md[i] = take((size_t)b[i] * b[i]));
+      tres[3 * i + 1] = static_cast<cplx*>(Gd[i] = take((size_t)b[i] * b[i]));
+    }
+    for (int i = 0; i + 1 < npl; ++i) {
+      const size_t cnt = (size_t)b[i] * b[i + 1];
+      tin[3 * i + 2] = static_cast<cplx*>(Mu[i] = take(cnt));
+      tin[3 * (i + 1) + 0] = static_cast<cplx*>(Ml[i] = take(cnt));
+      tres[3 * i + 2] = static_cast<cplx*>(Gu[i] = take(cnt));
+      tres[3 * (i + 1) + 0] = static_cast<cplx*>(Gl[i] = take(cnt));
+    }
   }
-  for (int i = 0; i + 1 < npl; ++i) {
-    Mu[i] = up(H[{i, i + 1}]);
-    Ml[i] = up(H[{i + 1, i}]);
-    Gu[i] = zal((size_t)b[i] * b[i + 1]);
-    Gl[i] = zal((size_t)b[i] * b[i + 1]);
-    if (!Mu[i] || !Ml[i] || !Gu[i] || !Gl[i]) {
+  cudaError_t e;
+  if ((e = cudaMemset(arena, 0, 2 * band * sizeof(cplx))) != cudaSuccess) return cerr(e);
+  if ((e = cudaMemcpy(d_colptr, colptr_in, sizeof(int) * (n + 1), cudaMemcpyHostToDevice)) != cudaSuccess) return cerr(e);
+  if (nnz_in > 0) {
+    if ((e = cudaMemcpy(d_rowval, rowval_in, sizeof(int) * nnz_in, cudaMemcpyHostToDevice)) != cudaSuccess)
+      return cerr(e);
+    if ((e = cudaMemcpy(d_nz, nzval_in, sizeof(cplx) * nnz_in, cudaMemcpyHostToDevice)) != cudaSuccess)
+      return cerr(e);
+  }
+  if ((e = cudaMemcpy(d_blk, blk_of.data(), sizeof(int) * n, cudaMemcpyHostToDevice)) != cudaSuccess) return cerr(e);
+  if ((e = cudaMemcpy(d_off, off.data(), sizeof(int) * (npl + 1), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return cerr(e);
+  if ((e = cudaMemcpy(d_b, b.data(), sizeof(int) * npl, cudaMemcpyHostToDevice)) != cudaSuccess) return cerr(e);
+  std::vector<cplx*> tabs(tin);
+  tabs.insert(tabs.end(), tres.begin(), tres.end());
+  if ((e = cudaMemcpy(d_tab, tabs.data(), sizeof(cplx*) * 6 * npl, cudaMemcpyHostToDevice)) != cudaSuccess)
+    return cerr(e);
+  if ((e = launch_csc_scatter(n, d_colptr, d_rowval, d_nz, std::max(0, nnz_in), d_blk, d_off, d_b, d_tab,
+                              is_hermitian ? 1 : 0, 0)) != cudaSuccess)
+    return cerr(e);
+  if (is_hermitian && npl > 1) {
+    // lower band blocks are the conjugate transposes of the upper ones
+    std::vector<int32_t> mm(npl - 1), nn(npl - 1), la(npl - 1), lc(npl - 1);
+    for (int i = 0; i + 1 < npl; ++i) { mm[i] = b[i + 1]; nn[i] = b[i]; la[i] = b[i]; lc[i] = b[i + 1]; }
+    if (negf_zcopy_batched('C', npl - 1, mm.data(), nn.data(), Mu.data(), la.data(), Ml.data(), lc.data(), nullptr) !=
+        NEGF_SUCCESS) {
       cleanup();
-      fail(NEGF_ERR_NOMEM, "run_bndiag_wrapper: device allocation failed");
       return bad;
     }
   }
   int rc = negf_ddrgf(1, npl, b.data(), Md.data(), Mu.data(), Ml.data(), 0, Gd.data(), Gu.data(), Gl.data(), nullptr);
   if (rc != NEGF_SUCCESS) { cleanup(); return bad; }
-  // download the result band (the output keeps the input's ndiag "out" pattern;
-  // DDRGF fills the tridiagonal, wider bands keep the input blocks as the
-  // reference's bm_copy(MbmIN) + bm_copy!(MbmOUT, buffMout) does)
-  std::map<std::pair<int, int>, std::vector<cplx>> R;
-  for (int i = 0; i < npl; ++i) {
-    auto& v = R[{i, i}];
-    v.resize((size_t)b[i] * b[i]);
-    cudaMemcpy(v.data(), Gd[i], v.size() * sizeof(cplx), cudaMemcpyDeviceToHost);
-  }
-  for (int i = 0; i + 1 < npl; ++i) {
-    auto& u = R[{i, i + 1}];
-    u.resize((size_t)b[i] * b[i + 1]);
-    cudaMemcpy(u.data(), Gu[i], u.size() * sizeof(cplx), cudaMemcpyDeviceToHost);
-    auto& l = R[{i + 1, i}];
-    l.resize((size_t)b[i] * b[i + 1]);
-    cudaMemcpy(l.data(), Gl[i], l.size() * sizeof(cplx), cudaMemcpyDeviceToHost);
-  }
-  cleanup();
+  // output: the input's "out" band; DDRGF fills the tridiagonal, wider bands keep
+  // the input blocks as the reference's bm_copy(MbmIN) + bm_copy!(MbmOUT,
+  // buffMout) does (rows sorted within a column, as in Julia's SparseMatrixCSC)
   const int wout = std::max(1, (nd_out - 1) / 2);
-  // out-of-tridiagonal blocks of a wider "out" band come from the input
-  std::vector<int> colptr(n + 1, 0);
-  std::vector<int> rows;
-  std::vector<cplx> vals;
-  for (int c = 0; c < n; ++c) {
-    int bj = blk_of[c];
-    for (int bi = std::max(0, bj - wout); bi <= std::min(npl - 1, bj + wout); ++bi) {
-      bool tri = std::abs(bi - bj) <= 1;
-      for (int r = off[bi]; r < off[bi + 1]; ++r) {
-        cplx v;
-        if (tri) {
-          v = R[{bi, bj}][(r - off[bi]) + (size_t)(c - off[bj]) * b[bi]];
-        } else {
-          v = make_double2(0.0, 0.0);
-          for (int p = colptr_in[c]; p < colptr_in[c + 1]; ++p)
-            if (rowval_in[p] == r) v = nz[p];
-        }
-        if (v.x != 0.0 || v.y != 0.0) {
-          rows.push_back(r);
-          vals.push_back(v);
-        }
-      }
-    }
-    colptr[c + 1] = static_cast<int>(rows.size());
-  }
+  if ((e = launch_csc_band_out(0, n, npl, wout, d_blk, d_off, d_b, d_tab + 3 * npl, d_colptr, d_rowval, d_nz,
+                               std::max(0, nnz_in), d_counts, nullptr, nullptr, nullptr, 0)) != cudaSuccess)
+    return cerr(e);
+  std::vector<int> counts(n), colptr(n + 1, 0);
+  if ((e = cudaMemcpy(counts.data(), d_counts, sizeof(int) * n, cudaMemcpyDeviceToHost)) != cudaSuccess) return cerr(e);
+  for (int c = 0; c < n; ++c) colptr[c + 1] = colptr[c] + counts[c];
+  const int nnz_out = colptr[n];
+  int* d_rows = static_cast<int*>(dalloc(sizeof(int) * (size_t)std::max(1, nnz_out)));
+  cplx* d_vals = static_cast<cplx*>(dalloc(sizeof(cplx) * (size_t)std::max(1, nnz_out)));
+  if (!d_rows || !d_vals) return oom();
+  if ((e = cudaMemcpy(d_colptr_out, colptr.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return cerr(e);
+  if ((e = launch_csc_band_out(1, n, npl, wout, d_blk, d_off, d_b, d_tab + 3 * npl, d_colptr, d_rowval, d_nz,
+                               std::max(0, nnz_in), nullptr, d_colptr_out, d_rows, d_vals, 0)) != cudaSuccess)
+    return cerr(e);
   CCscMatrix out;
   out.m = m;
   out.n = n;
-  out.nnz = static_cast<int32_t>(rows.size());
+  out.nnz = nnz_out;
   out.colptr = static_cast<int32_t*>(std::malloc(sizeof(int32_t) * (n + 1)));
-  out.rowval = static_cast<int32_t*>(std::malloc(sizeof(int32_t) * std::max<size_t>(1, rows.size())));
-  out.nzval = std::malloc(sizeof(cplx) * std::max<size_t>(1, vals.size()));
+  out.rowval = static_cast<int32_t*>(std::malloc(sizeof(int32_t) * std::max(1, nnz_out)));
+  out.nzval = std::malloc(sizeof(cplx) * std::max(1, nnz_out));
   if (!out.colptr || !out.rowval || !out.nzval) {
     std::free(out.colptr); std::free(out.rowval); std::free(out.nzval);
+    cleanup();
     fail(NEGF_ERR_NOMEM, "run_bndiag_wrapper: host allocation failed");
     return bad;
   }
   std::memcpy(out.colptr, colptr.data(), sizeof(int32_t) * (n + 1));
-  if (!rows.empty()) {
-    std::memcpy(out.rowval, rows.data(), sizeof(int32_t) * rows.size());
-    std::memcpy(out.nzval, vals.data(), sizeof(cplx) * vals.size());
+  if (nnz_out > 0) {
+    e = cudaMemcpy(out.rowval, d_rows, sizeof(int32_t) * nnz_out, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(out.nzval, d_vals, sizeof(cplx) * nnz_out, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+      std::free(out.colptr); std::free(out.rowval); std::free(out.nzval);
+      return cerr(e);
+    }
   }
+  cleanup();
   return out;
 }
 

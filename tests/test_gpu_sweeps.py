@@ -193,3 +193,64 @@ def test_run_bndiag_wrapper(negf):
         libc.free(ctypes.cast(p, ctypes.c_void_p))
     ref = band_of_dense(np.linalg.inv(D), M.blockSizes, {"in": 3, "out": 3})
     assert rel_fro(out, ref) < 2.5e-10
+
+
+def _call_wrapper(negf, D, npl, b, out_nd, hermitian):
+    import scipy.sparse as sp
+    from libnegf_b200._lib import int_array
+    csc = sp.csc_matrix(D)
+    csc.sort_indices()
+    n = D.shape[0]
+    colptr = np.ascontiguousarray(csc.indptr, dtype=np.int32)
+    rowval = np.ascontiguousarray(csc.indices, dtype=np.int32)
+    nz = np.ascontiguousarray(csc.data, dtype=np.complex128)
+    keys = (ctypes.c_char_p * 2)(b"in", b"out")
+    lib = negf.load()
+    sizes = b if isinstance(b, list) else [b] * npl
+    res = lib.run_bndiag_wrapper(n, n, csc.nnz, colptr.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                 rowval.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), nz.ctypes.data, npl,
+                                 int_array(sizes), 2, keys, int_array([3, out_nd]), int(hermitian))
+    assert res.m == n and res.nnz > 0
+    cp = np.ctypeslib.as_array(res.colptr, shape=(n + 1,)).copy()
+    rv = np.ctypeslib.as_array(res.rowval, shape=(res.nnz,)).copy()
+    vals = np.ctypeslib.as_array(ctypes.cast(res.nzval, ctypes.POINTER(ctypes.c_double)), shape=(2 * res.nnz,)).copy()
+    libc = ctypes.CDLL(None)
+    for p in (res.colptr, res.rowval, res.nzval):
+        libc.free(ctypes.cast(p, ctypes.c_void_p))
+    # every column's rows are sorted and inside the matrix
+    for c in range(n):
+        r = rv[cp[c]:cp[c + 1]]
+        assert np.all(np.diff(r) > 0) and (r.size == 0 or (r[0] >= 0 and r[-1] < n))
+    return sp.csc_matrix((vals[0::2] + 1j * vals[1::2], rv, cp), shape=(n, n)).toarray()
+
+
+def test_run_bndiag_wrapper_hermitian_ragged(negf):
+    from oracle import physics as o_phys
+    sizes = [24, 40, 16, 32, 24]
+    s = o_phys.physics_system(len(sizes), 0, seed=31, block_sizes=sizes)
+    n = sum(sizes)
+    off = np.cumsum([0] + sizes)
+    H = np.zeros((n, n), dtype=np.complex128)
+    for i, h in enumerate(s.Hd):
+        H[off[i]:off[i + 1], off[i]:off[i + 1]] = h
+    for i, h in enumerate(s.Hu):
+        H[off[i]:off[i + 1], off[i + 1]:off[i + 2]] = h
+        H[off[i + 1]:off[i + 2], off[i]:off[i + 1]] = h.conj().T
+    D = 0.3 * np.eye(n) - H  # Hermitian, M = E - H at a real energy
+    D[np.abs(D) < 1e-3] = 0.0
+    # the full matrix is passed; with is_hermitian only its diagonal and upper
+    # blocks are read (src/c_interface/libnegf_c_interface.jl:115-121)
+    out = _call_wrapper(negf, D, len(sizes), sizes, 3, True)
+    ref = band_of_dense(np.linalg.inv(D), sizes, {"in": 3, "out": 3})
+    assert rel_fro(out, ref) < 2.5e-10 * max(1.0, np.linalg.cond(D) / 1e4)
+
+
+def test_run_bndiag_wrapper_wide_out_band(negf):
+    # "out" = 5: the tridiagonal of the inverse plus the input's blocks at
+    # distance 2 (absent in a tridiagonal input), through the device lookup
+    npl, b = 8, 24
+    M = bm_create_synthetic_random(npl, b, seed=77, uniform=True)
+    D = bm_convert_dense(M)
+    out = _call_wrapper(negf, D, npl, b, 5, False)
+    ref = band_of_dense(np.linalg.inv(D), M.blockSizes, {"in": 3, "out": 3})
+    assert rel_fro(out, ref) < 2.5e-10 * max(1.0, np.linalg.cond(D) / 1e4)
