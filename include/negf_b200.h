@@ -194,6 +194,12 @@ int negf_device_create(int32_t npl, const int32_t* block_sizes, const void* cons
 int negf_device_upload(negf_device_t dev, const void* const* Hd, const void* const* Hu, const void* sigL,
                        const void* sigR);
 int negf_device_destroy(negf_device_t dev);
+/* Overlap matrix S of a non-orthogonal basis (host blocks: Sd[i] b_i x b_i,
+ * Su[i] = S_{i,i+1} b_i x b_{i+1}, S_{i+1,i} = Su[i]^H; a NULL array or entry
+ * is the identity / zero).  Solvers created afterwards form
+ * M(E) = (E + i eta) S - H - Sigma(E) per energy on the device, as the
+ * reference's build_M_from_HS (src/matloader.jl:89-95). */
+int negf_device_set_overlap(negf_device_t dev, const void* const* Sd, const void* const* Su);
 
 typedef struct {
   double eta, mu_l, mu_r, kT;
@@ -207,6 +213,10 @@ typedef struct {
    * of the Python layer (libnegf_b200.autotune): */
   int32_t gemm_form; /* FP64 complex products: 1 = four real products, 2 = 3M (Gauss, default) */
   int32_t gj_nb;     /* Gauss-Jordan panel width for blocks > 112: 8, 16 or 32 (must fit shared memory) */
+  /* 1: the lead self-energies depend on the energy; solvers then take them per
+   * energy from negf_solver_set_self_energies (replacing the device's
+   * constant ones) and form Gamma(E) on the device. */
+  int32_t sigma_per_energy;
 } negf_solve_opts;
 
 /* Precision modes.  FP64: every product in FP64 on the DMMA tensor path.
@@ -246,6 +256,10 @@ int negf_solver_create_batch(int32_t ndev, const negf_device_t* devs, const int3
 int negf_batch_bytes(int32_t ndev, const negf_device_t* devs, const int32_t* nE, const negf_solve_opts* opts,
                      int64_t* bytes);
 int negf_solver_destroy(negf_solver_t s);
+/* Per-energy lead self-energies (host arrays of nE block pointers in the
+ * solver's energy order; Sigma_L(E) b_0 x b_0, Sigma_R(E) b_{N-1} x b_{N-1})
+ * for a solver created with opts.sigma_per_energy = 1; copied before return. */
+int negf_solver_set_self_energies(negf_solver_t s, const void* const* sigL, const void* const* sigR, void* stream);
 /* energies: host array of nE values (uploaded to a device parameter table). */
 int negf_solver_set_energies(negf_solver_t s, const double* energies, void* stream);
 /* One pass over all energies (captured into a CUDA graph on first use). */

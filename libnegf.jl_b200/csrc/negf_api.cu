@@ -130,6 +130,8 @@ struct negf_device_s {
   cplx* gamR = nullptr;
   cplx* sigL = nullptr;
   cplx* sigR = nullptr;
+  std::vector<cplx*> Sd, Su;       // overlap blocks (set by negf_device_set_overlap)
+  bool has_S = false;
   std::unique_ptr<Plan> assemble;  // Sigma / Gamma assembly launches
   cudaStream_t stream = nullptr;
   std::vector<void*> owned;
@@ -153,6 +155,8 @@ struct negf_solver_s {
   cplx* gl = nullptr;
   double* t2 = nullptr;    // 2 * nE (re, im)
   int* info = nullptr;
+  std::vector<cplx*> sigL_e, sigR_e;  // per-energy self-energies (opts.sigma_per_energy)
+  std::vector<int> bL_e, bR_e;        // their sizes
   size_t per_energy = 0;   // sum b_i^2 (single-device solvers; 0 for a multi-device batch)
   std::vector<std::vector<cudaEvent_t>> ev_sets;  // one event set per profiled pass
   size_t ev_used = 0;
@@ -173,6 +177,8 @@ size_t solver_bytes_per_energy(const negf_device_s& d, const negf_solve_opts& o)
   if (o.want_gr) c += sb2 + 4 * mb * mb;              // G^R diagonal + rings
   if (o.want_gl) c += sb2 + sbb + 3 * n * mb * mb;    // G^n storage + RKD scratch
   if (o.want_t) c += 4 * mb * mb;
+  if (d.has_S || o.sigma_per_energy) c += sb2 + 2 * sbb;  // per-energy M blocks
+  if (o.sigma_per_energy) c += 2 * ((size_t)d.b.front() * d.b.front() + (size_t)d.b.back() * d.b.back());
   size_t bytes = c * sizeof(cplx) + 64;
   if (o.precision == NEGF_PREC_MIXED) {
     // digit slices of the INT8 products (21 bytes per padded element): the
@@ -243,26 +249,99 @@ int build_solver(negf_solver_s& S) {
         return fail(NEGF_ERR_INVALID, "gj_nb too wide for the block size (shared memory)");
   plan.set_schedule(S.opts.gemm_form, S.opts.gj_nb);
 
+  const bool sig_e = S.opts.sigma_per_energy != 0;
   std::vector<TriSystem> sys(nE);
   std::vector<RgfWork> work(nE);
+  std::vector<cplx*> gamL_of(nE), gamR_of(nE);
+  // per-energy M(E) = z S - H - Sigma(E) (z = E + i eta) when the device has an
+  // overlap or the self-energies depend on the energy (build_M_from_HS,
+  // src/matloader.jl:89-95); otherwise M is never formed (shift in the GEMM
+  // epilogue, off-diagonal blocks shared)
+  std::vector<ZBlockOp> asm_set, asm_add, asm_l1, asm_l2, asm_r1, asm_r2;
+  auto op = [](ZOpKind k, const cplx* A, int lda, cplx* C, int ldc, int m, int n2, cplx alpha, cplx beta,
+               const cplx* alpha_ptr = nullptr) {
+    ZBlockOp o{};
+    o.A = A; o.lda = lda; o.C = C; o.ldc = ldc; o.m = m; o.n = n2; o.kind = k;
+    o.alpha = alpha; o.beta = beta; o.alpha_ptr = alpha_ptr;
+    return o;
+  };
+  const cplx P1 = make_double2(1.0, 0.0), M1 = make_double2(-1.0, 0.0), Z0 = make_double2(0.0, 0.0);
+  if (sig_e) {
+    S.sigL_e.assign(nE, nullptr);
+    S.sigR_e.assign(nE, nullptr);
+    S.bL_e.assign(nE, 0);
+    S.bR_e.assign(nE, 0);
+  }
   for (int e = 0; e < nE; ++e) {
     const negf_device_s& d = *items[e].d;
     const int n = d.npl;
     TriSystem& t = sys[e];
     t.b = d.b;
-    for (int i = 0; i < n; ++i) { t.D.push_back(d.D[i]); t.ldD.push_back(d.b[i]); }
-    for (int i = 0; i + 1 < n; ++i) {
-      t.U.push_back(d.Hu[i]); t.ldU.push_back(d.b[i]);
-      t.Lw.push_back(d.Hu[i]); t.ldL.push_back(d.b[i]);
-    }
-    t.dscale = make_double2(-1.0, 0.0);
-    t.uscale = make_double2(-1.0, 0.0);
-    t.lscale = make_double2(-1.0, 0.0);
-    t.lop = 'C';
-    t.shift_ptr = S.params + e;
     t.info = S.info + e;
+    gamL_of[e] = d.gamL;
+    gamR_of[e] = d.gamR;
+    if (sig_e || d.has_S) {
+      const cplx* z = S.params + e;
+      std::vector<cplx*> md(n);
+      for (int i = 0; i < n; ++i) {
+        cplx* m = md[i] = plan.alloc_c((size_t)d.b[i] * d.b[i]);
+        t.D.push_back(m); t.ldD.push_back(d.b[i]);
+        asm_set.push_back(op(ZOP_AXPBY, d.D[i], d.b[i], m, d.b[i], d.b[i], d.b[i], M1, Z0));
+        if (d.has_S) asm_add.push_back(op(ZOP_AXPBY, d.Sd[i], d.b[i], m, d.b[i], d.b[i], d.b[i], P1, P1, z));
+        else asm_add.push_back(op(ZOP_ADD_DIAG, nullptr, 1, m, d.b[i], d.b[i], d.b[i], P1, P1, z));
+      }
+      for (int i = 0; i + 1 < n; ++i) {
+        const int bi = d.b[i], bj = d.b[i + 1];
+        cplx* u = plan.alloc_c((size_t)bi * bj);
+        cplx* l = plan.alloc_c((size_t)bi * bj);
+        t.U.push_back(u); t.ldU.push_back(bi);
+        t.Lw.push_back(l); t.ldL.push_back(bj);
+        asm_set.push_back(op(ZOP_AXPBY, d.Hu[i], bi, u, bi, bi, bj, M1, Z0));
+        asm_set.push_back(op(ZOP_CTRANS_AXPBY, d.Hu[i], bi, l, bj, bj, bi, M1, Z0));
+        if (d.has_S) {
+          asm_add.push_back(op(ZOP_AXPBY, d.Su[i], bi, u, bi, bi, bj, P1, P1, z));
+          asm_add.push_back(op(ZOP_CTRANS_AXPBY, d.Su[i], bi, l, bj, bj, bi, P1, P1, z));
+        }
+      }
+      t.dscale = P1; t.uscale = P1; t.lscale = P1;
+      t.lop = 'N';
+      t.shift_ptr = nullptr;
+      if (sig_e) {
+        // Sigma(E) replaces the device's constant self-energy (already in D[0], D[N-1])
+        const int b0 = d.b.front(), bN = d.b.back();
+        S.bL_e[e] = b0; S.bR_e[e] = bN;
+        S.sigL_e[e] = plan.alloc_c((size_t)b0 * b0);
+        S.sigR_e[e] = plan.alloc_c((size_t)bN * bN);
+        gamL_of[e] = plan.alloc_c((size_t)b0 * b0);
+        gamR_of[e] = plan.alloc_c((size_t)bN * bN);
+        asm_set.push_back(op(ZOP_GAMMA, S.sigL_e[e], b0, gamL_of[e], b0, b0, b0, P1, Z0));
+        asm_set.push_back(op(ZOP_GAMMA, S.sigR_e[e], bN, gamR_of[e], bN, bN, bN, P1, Z0));
+        asm_l1.push_back(op(ZOP_AXPBY, d.sigL, b0, md[0], b0, b0, b0, P1, P1));
+        asm_l2.push_back(op(ZOP_AXPBY, S.sigL_e[e], b0, md[0], b0, b0, b0, M1, P1));
+        asm_r1.push_back(op(ZOP_AXPBY, d.sigR, bN, md[n - 1], bN, bN, bN, P1, P1));
+        asm_r2.push_back(op(ZOP_AXPBY, S.sigR_e[e], bN, md[n - 1], bN, bN, bN, M1, P1));
+      }
+    } else {
+      for (int i = 0; i < n; ++i) { t.D.push_back(d.D[i]); t.ldD.push_back(d.b[i]); }
+      for (int i = 0; i + 1 < n; ++i) {
+        t.U.push_back(d.Hu[i]); t.ldU.push_back(d.b[i]);
+        t.Lw.push_back(d.Hu[i]); t.ldL.push_back(d.b[i]);
+      }
+      t.dscale = make_double2(-1.0, 0.0);
+      t.uscale = make_double2(-1.0, 0.0);
+      t.lscale = make_double2(-1.0, 0.0);
+      t.lop = 'C';
+      t.shift_ptr = S.params + e;
+    }
     alloc_rgf_work(plan, t, work[e]);
   }
+  // one launch per list: every block is written at most once per launch
+  plan.blockops(asm_set);
+  plan.blockops(asm_add);
+  plan.blockops(asm_l1);
+  plan.blockops(asm_l2);
+  plan.blockops(asm_r1);
+  plan.blockops(asm_r2);
   // block pointers inside the output arrays
   auto out_blocks = [&](cplx* base, int e) {
     const negf_device_s& d = *items[e].d;
@@ -294,10 +373,10 @@ int build_solver(negf_solver_s& S) {
         ZBlockOp z{}; z.C = h.u[i]; z.ldc = d.b[i]; z.m = d.b[i]; z.n = d.b[i + 1]; z.kind = ZOP_FILL;
         zero.push_back(z);
       }
-      ZBlockOp l{}; l.A = d.gamL; l.lda = d.b[0]; l.C = h.d[0]; l.ldc = d.b[0]; l.m = l.n = d.b[0];
+      ZBlockOp l{}; l.A = gamL_of[e]; l.lda = d.b[0]; l.C = h.d[0]; l.ldc = d.b[0]; l.m = l.n = d.b[0];
       l.kind = ZOP_AXPBY; l.alpha_ptr = S.params + nE + e; l.beta = make_double2(1.0, 0.0);
       setL.push_back(l);
-      ZBlockOp r{}; r.A = d.gamR; r.lda = d.b[n - 1]; r.C = h.d[n - 1]; r.ldc = d.b[n - 1];
+      ZBlockOp r{}; r.A = gamR_of[e]; r.lda = d.b[n - 1]; r.C = h.d[n - 1]; r.ldc = d.b[n - 1];
       r.m = r.n = d.b[n - 1]; r.kind = ZOP_AXPBY; r.alpha_ptr = S.params + 2 * nE + e; r.beta = make_double2(1.0, 0.0);
       addR.push_back(r);
     }
@@ -375,11 +454,11 @@ int build_solver(negf_solver_s& S) {
       const int n = d.npl, b0 = d.b[0], bN = d.b[n - 1];
       const cplx* G1N = ycur(e, n - 1);
       ZGemmProblem a{};  // P = Gamma_L G1N  (b0 x bN)
-      a.A = d.gamL; a.lda = b0; a.B = G1N; a.ldb = b0; a.C = P[e]; a.ldc = b0; a.ldcin = 1;
+      a.A = gamL_of[e]; a.lda = b0; a.B = G1N; a.ldb = b0; a.C = P[e]; a.ldc = b0; a.ldcin = 1;
       a.m = b0; a.n = bN; a.k = b0; a.alpha = make_double2(1.0, 0.0);
       p1.push_back(a);
       ZGemmProblem c{};  // Q = Gamma_R G1N^H  (bN x b0)
-      c.A = d.gamR; c.lda = bN; c.B = G1N; c.ldb = b0; c.C = Q[e]; c.ldc = bN; c.ldcin = 1;
+      c.A = gamR_of[e]; c.lda = bN; c.B = G1N; c.ldb = b0; c.C = Q[e]; c.ldc = bN; c.ldcin = 1;
       c.m = bN; c.n = b0; c.k = bN; c.alpha = make_double2(1.0, 0.0);
       p2.push_back(c);
       ZTraceProblemHost t{};
@@ -687,6 +766,65 @@ int negf_device_create(int32_t npl, const int32_t* block_sizes, const void* cons
                                                                    : (delete h, NEGF_ERR_CUDA);
 }
 
+int negf_device_set_overlap(negf_device_t d, const void* const* Sd, const void* const* Su) {
+  if (!d) return fail(NEGF_ERR_INVALID, "NULL device");
+  const int n = d->npl;
+  auto dalloc = [&](size_t elems) -> cplx* {
+    void* p = nullptr;
+    if (cudaMalloc(&p, elems * sizeof(cplx)) != cudaSuccess) return nullptr;
+    d->owned.push_back(p);
+    return static_cast<cplx*>(p);
+  };
+  if (d->Sd.empty()) {
+    for (int i = 0; i < n; ++i) {
+      cplx* p = dalloc((size_t)d->b[i] * d->b[i]);
+      if (!p) return fail(NEGF_ERR_NOMEM, "device allocation failed");
+      d->Sd.push_back(p);
+    }
+    for (int i = 0; i + 1 < n; ++i) {
+      cplx* p = dalloc((size_t)d->b[i] * d->b[i + 1]);
+      if (!p) return fail(NEGF_ERR_NOMEM, "device allocation failed");
+      d->Su.push_back(p);
+    }
+  }
+  for (int i = 0; i < n; ++i) {
+    const size_t cnt = (size_t)d->b[i] * d->b[i];
+    if (Sd && Sd[i]) {
+      NEGF_TRY_CUDA(cudaMemcpy(d->Sd[i], Sd[i], cnt * sizeof(cplx), cudaMemcpyHostToDevice), "set overlap");
+    } else {
+      std::vector<cplx> eye(cnt, make_double2(0.0, 0.0));
+      for (int r = 0; r < d->b[i]; ++r) eye[r + (size_t)r * d->b[i]] = make_double2(1.0, 0.0);
+      NEGF_TRY_CUDA(cudaMemcpy(d->Sd[i], eye.data(), cnt * sizeof(cplx), cudaMemcpyHostToDevice), "set overlap");
+    }
+  }
+  for (int i = 0; i + 1 < n; ++i) {
+    const size_t cnt = (size_t)d->b[i] * d->b[i + 1];
+    if (Su && Su[i]) {
+      NEGF_TRY_CUDA(cudaMemcpy(d->Su[i], Su[i], cnt * sizeof(cplx), cudaMemcpyHostToDevice), "set overlap");
+    } else {
+      NEGF_TRY_CUDA(cudaMemset(d->Su[i], 0, cnt * sizeof(cplx)), "set overlap");
+    }
+  }
+  d->has_S = true;
+  return NEGF_SUCCESS;
+}
+
+int negf_solver_set_self_energies(negf_solver_t s, const void* const* sigL, const void* const* sigR, void* stream) {
+  if (!s || !sigL || !sigR) return fail(NEGF_ERR_INVALID, "bad arguments");
+  if (!s->opts.sigma_per_energy)
+    return fail(NEGF_ERR_INVALID, "the solver was not created with opts.sigma_per_energy");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  for (int e = 0; e < s->nE; ++e) {
+    if (!sigL[e] || !sigR[e]) return fail(NEGF_ERR_INVALID, "NULL self-energy block");
+    NEGF_TRY_CUDA(cudaMemcpyAsync(s->sigL_e[e], sigL[e], sizeof(cplx) * s->bL_e[e] * s->bL_e[e],
+                                  cudaMemcpyHostToDevice, st), "set self-energies");
+    NEGF_TRY_CUDA(cudaMemcpyAsync(s->sigR_e[e], sigR[e], sizeof(cplx) * s->bR_e[e] * s->bR_e[e],
+                                  cudaMemcpyHostToDevice, st), "set self-energies");
+  }
+  NEGF_TRY_CUDA(cudaStreamSynchronize(st), "set self-energies");
+  return NEGF_SUCCESS;
+}
+
 int negf_device_upload(negf_device_t d, const void* const* Hd, const void* const* Hu, const void* sigL,
                        const void* sigR) {
   if (!d) return fail(NEGF_ERR_INVALID, "NULL device");
@@ -887,6 +1025,9 @@ int negf_solver_check(negf_solver_t s) {
 
 int negf_solve(negf_device_t dev, int32_t nE, const double* energies, const negf_solve_opts* opts, void* gr_out,
                void* gl_out, double* t_out, int32_t out_on_device, void* stream) {
+  if (opts && opts->sigma_per_energy)
+    return fail(NEGF_ERR_INVALID, "negf_solve has no per-energy self-energies; use a solver and "
+                                  "negf_solver_set_self_energies");
   if (int r = check_device()) return r;
   if (!dev || nE <= 0 || !energies || !opts) return fail(NEGF_ERR_INVALID, "bad arguments");
   negf_solve_opts o = *opts;

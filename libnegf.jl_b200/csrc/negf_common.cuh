@@ -127,6 +127,8 @@ enum ZOpKind : int {
   ZOP_IDENTITY = 4,    // C = alpha * I
   ZOP_HERM_PART = 5,   // C = (A + A^H)/2
   ZOP_GAMMA = 6,       // C = i (A - A^H)   (broadening of a self-energy)
+  ZOP_CTRANS_AXPBY = 7,  // C = alpha*A^H + beta*C   (A is n x m)
+  ZOP_ADD_DIAG = 8,    // C[r, r] += alpha
 };
 
 struct ZBlockOp {

@@ -17,7 +17,7 @@ __global__ void zblockop_kernel(const ZBlockOp* __restrict__ ops) {
   const int tilesn = (o.n + EL_TILE - 1) / EL_TILE;
   for (int t = blockIdx.x; t < tilesm * tilesn; t += gridDim.x) {
     const int r0 = (t % tilesm) * EL_TILE, c0 = (t / tilesm) * EL_TILE;
-    if (o.kind == ZOP_CTRANSPOSE || o.kind == ZOP_HERM_PART || o.kind == ZOP_GAMMA) {
+    if (o.kind == ZOP_CTRANSPOSE || o.kind == ZOP_HERM_PART || o.kind == ZOP_GAMMA || o.kind == ZOP_CTRANS_AXPBY) {
       // A is n x m here (C = A^H is m x n); read A tile (c0.., r0..) coalesced along its rows
       for (int i = threadIdx.y; i < EL_TILE; i += blockDim.y) {
         int ar = c0 + threadIdx.x, ac = r0 + i;  // element A[ar, ac], ar < n, ac < m
@@ -35,6 +35,9 @@ __global__ void zblockop_kernel(const ZBlockOp* __restrict__ ops) {
             cplx a = o.A[r + (size_t)c * o.lda];
             cplx d = make_double2(a.x - v.x, a.y - v.y);  // A - A^H
             v = make_double2(-d.y, d.x);                  // i * d
+          } else if (o.kind == ZOP_CTRANS_AXPBY) {
+            v = cmul(o.alpha, v);
+            if (o.beta.x != 0.0 || o.beta.y != 0.0) v = cadd(v, cmul(o.beta, o.C[r + (size_t)c * o.ldc]));
           }
           o.C[r + (size_t)c * o.ldc] = v;
         }
@@ -48,12 +51,16 @@ __global__ void zblockop_kernel(const ZBlockOp* __restrict__ ops) {
         cplx v;
         switch (o.kind) {
           case ZOP_COPY: v = o.A[r + (size_t)c * o.lda]; break;
-          case ZOP_AXPBY: {
+          case ZOP_AXPBY: {  // beta = 0 does not read C (BLAS semantics)
             cplx a = o.A[r + (size_t)c * o.lda];
-            cplx x = o.C[ci];
-            v = cadd(cmul(o.alpha, a), cmul(o.beta, x));
+            v = cmul(o.alpha, a);
+            if (o.beta.x != 0.0 || o.beta.y != 0.0) v = cadd(v, cmul(o.beta, o.C[ci]));
             break;
           }
+          case ZOP_ADD_DIAG:
+            if (r != c) continue;
+            v = cadd(o.C[ci], o.alpha);
+            break;
           case ZOP_FILL: v = o.alpha; break;
           case ZOP_IDENTITY: v = (r == c) ? o.alpha : make_double2(0.0, 0.0); break;
           default: v = make_double2(0.0, 0.0); break;

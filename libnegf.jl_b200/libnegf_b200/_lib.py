@@ -33,7 +33,8 @@ class SolveOpts(ctypes.Structure):
     _fields_ = [("eta", ctypes.c_double), ("mu_l", ctypes.c_double), ("mu_r", ctypes.c_double),
                 ("kT", ctypes.c_double), ("want_gr", ctypes.c_int32), ("want_gl", ctypes.c_int32),
                 ("want_t", ctypes.c_int32), ("max_chunk", ctypes.c_int32), ("hbm_budget_gb", ctypes.c_double),
-                ("precision", ctypes.c_int32), ("gemm_form", ctypes.c_int32), ("gj_nb", ctypes.c_int32)]
+                ("precision", ctypes.c_int32), ("gemm_form", ctypes.c_int32), ("gj_nb", ctypes.c_int32),
+                ("sigma_per_energy", ctypes.c_int32)]
 
 
 NEGF_PREC_FP64 = 0
@@ -90,6 +91,8 @@ PROTOTYPES = {
     "negf_batch_bytes": (ctypes.c_int, [ctypes.c_int32, c_void_pp, ctypes.POINTER(ctypes.c_int32),
                                         ctypes.POINTER(SolveOpts), ctypes.POINTER(ctypes.c_int64)]),
     "negf_solver_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "negf_device_set_overlap": (ctypes.c_int, [ctypes.c_void_p, c_void_pp, c_void_pp]),
+    "negf_solver_set_self_energies": (ctypes.c_int, [ctypes.c_void_p, c_void_pp, c_void_pp, ctypes.c_void_p]),
     "negf_solver_set_energies": (ctypes.c_int, [ctypes.c_void_p, c_double_p, ctypes.c_void_p]),
     "negf_solver_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "negf_solver_outputs": (ctypes.c_int, [ctypes.c_void_p, c_void_pp, c_void_pp,

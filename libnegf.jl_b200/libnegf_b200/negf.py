@@ -26,7 +26,7 @@ def _host_blocks(blocks):
 
 
 def make_opts(eta=1e-6, mu_l=0.1, mu_r=-0.1, kT=0.025, want_gr=True, want_gl=True, want_t=True, max_chunk=0,
-              hbm_budget_gb=0.0, precision="fp64", gemm_form=0, gj_nb=0):
+              hbm_budget_gb=0.0, precision="fp64", gemm_form=0, gj_nb=0, sigma_per_energy=False):
     """precision: "fp64" (every product in FP64) or "mixed" (Schur products on
     the INT8 tensor cores with FP64-accurate digit splitting).  gemm_form /
     gj_nb: schedule knobs (0 = library default; see libnegf_b200.autotune)."""
@@ -38,6 +38,7 @@ def make_opts(eta=1e-6, mu_l=0.1, mu_r=-0.1, kT=0.025, want_gr=True, want_gl=Tru
     o.precision = {"fp64": _lib.NEGF_PREC_FP64, "mixed": _lib.NEGF_PREC_MIXED}[precision]
     o.gemm_form = int(gemm_form)
     o.gj_nb = int(gj_nb)
+    o.sigma_per_energy = int(bool(sigma_per_energy))
     return o
 
 
@@ -61,6 +62,14 @@ class Device:
         sl = np.asfortranarray(np.asarray(sigL, dtype=np.complex128))
         sr = np.asfortranarray(np.asarray(sigR, dtype=np.complex128))
         check(load().negf_device_upload(self._handle, ptr_array(pd), ptr_array(pu), sl.ctypes.data, sr.ctypes.data))
+
+    def set_overlap(self, Sd=None, Su=None):
+        """Overlap matrix S (diagonal blocks Sd, upper blocks Su; None: identity /
+        zero): solvers created afterwards use M(E) = (E + i eta) S - H - Sigma."""
+        kd, pd = _host_blocks(Sd) if Sd is not None else (None, None)
+        ku, pu = _host_blocks(Su) if Su is not None else (None, None)
+        check(load().negf_device_set_overlap(self._handle, ptr_array(pd) if pd is not None else None,
+                                             ptr_array(pu) if pu is not None else None))
 
     @property
     def handle(self):
@@ -128,6 +137,13 @@ class Solver:
         assert len(E) == self.nE
         check(load().negf_solver_set_energies(self._h, E.ctypes.data_as(_lib.c_double_p), stream))
 
+    def set_self_energies(self, sigL, sigR, stream=None):
+        """Per-energy Sigma_L(E), Sigma_R(E) (lists of nE blocks in the energy
+        order) for a solver made with sigma_per_energy=True."""
+        kl, pl = _host_blocks(sigL)
+        kr, pr = _host_blocks(sigR)
+        check(load().negf_solver_set_self_energies(self._h, ptr_array(pl), ptr_array(pr), stream))
+
     def run(self, stream=None):
         check(load().negf_solver_run(self._h, stream))
 
@@ -180,35 +196,6 @@ class Solver:
                 off += per
         return out, off
 
-    def close(self):
-        if self._h:
-            load().negf_solver_destroy(self._h)
-            self._h = ctypes.c_void_p()
-
-    def __del__(self):
-        try:
-            self.close()
-        except Exception:
-            pass
-
-
-class BatchSolver(Solver):
-    """One resident plan over several devices of different layer counts and
-    block sizes (counts[k] energies of devices[k]); energies and outputs are
-    device-major (see negf_solver_create_batch)."""
-
-    def __init__(self, devices, counts, **kw):
-        self.devices = list(devices)
-        self.device = self.devices[0]
-        self.counts = [int(c) for c in counts]
-        self.nE = sum(self.counts)
-        self.opts = make_opts(**kw)
-        self._h = ctypes.c_void_p()
-        handles = (ctypes.c_void_p * len(self.devices))(*[d.handle.value for d in self.devices])
-        cnt = (ctypes.c_int32 * len(self.counts))(*self.counts)
-        check(load().negf_solver_create_batch(len(self.devices), handles, cnt, ctypes.byref(self.opts),
-                                              ctypes.byref(self._h)))
-
     def host_outputs(self, stream=None):
         """Download everything and split it: (gr, gl, t) with gr[k][e][i] the
         diagonal block i of energy e of device k (numpy), t[k][e] real."""
@@ -238,3 +225,33 @@ class BatchSolver(Solver):
                 t.append(t2[0::2][g:g + n])
                 g += n
         return split(gr), split(gl), t
+
+    def close(self):
+        if self._h:
+            load().negf_solver_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BatchSolver(Solver):
+    """One resident plan over several devices of different layer counts and
+    block sizes (counts[k] energies of devices[k]); energies and outputs are
+    device-major (see negf_solver_create_batch)."""
+
+    def __init__(self, devices, counts, **kw):
+        self.devices = list(devices)
+        self.device = self.devices[0]
+        self.counts = [int(c) for c in counts]
+        self.nE = sum(self.counts)
+        self.opts = make_opts(**kw)
+        self._h = ctypes.c_void_p()
+        handles = (ctypes.c_void_p * len(self.devices))(*[d.handle.value for d in self.devices])
+        cnt = (ctypes.c_int32 * len(self.counts))(*self.counts)
+        check(load().negf_solver_create_batch(len(self.devices), handles, cnt, ctypes.byref(self.opts),
+                                              ctypes.byref(self._h)))
+

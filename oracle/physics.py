@@ -30,12 +30,21 @@ def _cn(rng, shape, var):
 
 
 class DeviceSystem:
-    """Energy-independent data of one device: H blocks and lead self-energies."""
+    """Data of one device: H blocks, lead self-energies (constant, or a
+    function of the energy) and optionally an overlap matrix S (diagonal
+    blocks Sd, upper blocks Su; S = I when absent), so that
+    M(E) = (E + i eta) S - H - Sigma(E) as the reference's build_M_from_HS
+    (src/matloader.jl:89-95) forms it."""
 
-    def __init__(self, Hd, Hu, sigL, sigR, eta=1e-6, muL=0.1, muR=-0.1, kT=0.025):
+    def __init__(self, Hd, Hu, sigL, sigR, eta=1e-6, muL=0.1, muR=-0.1, kT=0.025, Sd=None, Su=None, sigma_fn=None):
         self.Hd, self.Hu = Hd, Hu          # diagonal blocks, upper blocks H_{i,i+1}
         self.sigL, self.sigR = sigL, sigR
         self.eta, self.muL, self.muR, self.kT = eta, muL, muR, kT
+        self.Sd, self.Su, self.sigma_fn = Sd, Su, sigma_fn
+
+    def sig(self, E):
+        """(Sigma_L(E), Sigma_R(E))."""
+        return self.sigma_fn(E) if self.sigma_fn is not None else (self.sigL, self.sigR)
 
     @property
     def npl(self):
@@ -56,16 +65,22 @@ class DeviceSystem:
         n = self.npl
         bm = BlockMatrix(self.sizes, {"in": 3, "out": 3}, False)
         z = E + 1j * self.eta
+        sL, sR = self.sig(E)
         for i in range(n):
-            d = z * np.eye(self.sizes[i]) - self.Hd[i]
+            S = self.Sd[i] if self.Sd is not None else np.eye(self.sizes[i])
+            d = z * S - self.Hd[i]
             if i == 0:
-                d = d - self.sigL
+                d = d - sL
             if i == n - 1:
-                d = d - self.sigR
+                d = d - sR
             bm.M[(i, i)] = d
         for i in range(n - 1):
-            bm.M[(i, i + 1)] = -self.Hu[i]
-            bm.M[(i + 1, i)] = -np.conj(self.Hu[i]).T
+            up, lo = -self.Hu[i], -np.conj(self.Hu[i]).T
+            if self.Su is not None:
+                up = up + z * self.Su[i]
+                lo = lo + z * np.conj(self.Su[i]).T
+            bm.M[(i, i + 1)] = up
+            bm.M[(i + 1, i)] = lo
         return bm
 
     def sigma_in(self, E):
@@ -76,8 +91,9 @@ class DeviceSystem:
             bm.M[(i, i)] = np.zeros((self.sizes[i], self.sizes[i]), dtype=np.complex128)
         for i in range(n - 1):
             bm.M[(i, i + 1)] = np.zeros((self.sizes[i], self.sizes[i + 1]), dtype=np.complex128)
-        bm.M[(0, 0)] = bm.M[(0, 0)] + self.fermi(E, self.muL) * self.gamma(self.sigL)
-        bm.M[(n - 1, n - 1)] = bm.M[(n - 1, n - 1)] + self.fermi(E, self.muR) * self.gamma(self.sigR)
+        sL, sR = self.sig(E)
+        bm.M[(0, 0)] = bm.M[(0, 0)] + self.fermi(E, self.muL) * self.gamma(sL)
+        bm.M[(n - 1, n - 1)] = bm.M[(n - 1, n - 1)] + self.fermi(E, self.muR) * self.gamma(sR)
         return bm
 
 
@@ -102,6 +118,35 @@ def physics_system(npl, b, seed=0, eta=1e-6, block_sizes=None):
     return DeviceSystem(Hd, Hu, sigL, sigR, eta=eta)
 
 
+def with_overlap_and_sigma_of_E(sysm, seed=0):
+    """The same device with an overlap matrix S = I + a small Hermitian band
+    (positive definite) and energy-dependent lead self-energies
+    Sigma(E) = (1 + 0.1 E) X - 0.05 i (1 + 0.5 sin 2E)(Y Y^H + 0.1 I)."""
+    rng = np.random.default_rng(seed)
+    sizes = sysm.sizes
+    Sd, Su = [], []
+    for b in sizes:
+        A = _cn(rng, (b, b), 1.0) / np.sqrt(b)
+        Sd.append(np.eye(b) + 0.02 * (A + np.conj(A).T))
+    for i in range(len(sizes) - 1):
+        Su.append(0.01 * _cn(rng, (sizes[i], sizes[i + 1]), 1.0) / np.sqrt(sizes[i]))
+
+    def parts(n):
+        B = _cn(rng, (n, n), 0.1)
+        Y = _cn(rng, (n, n), 1.0) / np.sqrt(n)
+        return (B + np.conj(B).T) / 2.0, Y @ np.conj(Y).T + 0.1 * np.eye(n)
+
+    XL, PL = parts(sizes[0])
+    XR, PR = parts(sizes[-1])
+
+    def sigma_fn(E):
+        g = 0.05 * (1.0 + 0.5 * np.sin(2.0 * E))
+        return (1.0 + 0.1 * E) * XL - 1j * g * PL, (1.0 + 0.1 * E) * XR - 1j * g * PR
+
+    return DeviceSystem(sysm.Hd, sysm.Hu, sysm.sigL, sysm.sigR, eta=sysm.eta, muL=sysm.muL, muR=sysm.muR,
+                        kT=sysm.kT, Sd=Sd, Su=Su, sigma_fn=sigma_fn)
+
+
 def energy_grid(n, lo=-1.0, hi=1.0):
     return np.linspace(lo, hi, n)
 
@@ -124,8 +169,9 @@ def solve_energy(sysm, E, want_keldysh=True):
     g1 = GR.M[(0, 0)]
     for j in range(1, sysm.npl):
         g1 = be_gemm("N", "N", -1.0, g1, R[j - 1], 0.0, None)
-    gL = sysm.gamma(sysm.sigL)
-    gR = sysm.gamma(sysm.sigR)
+    sL, sR = sysm.sig(E)
+    gL = sysm.gamma(sL)
+    gR = sysm.gamma(sR)
     T = np.trace(gL @ g1 @ gR @ np.conj(g1).T)
     out["T"] = float(np.real(T))
     out["G1N"] = g1

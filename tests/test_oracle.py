@@ -214,3 +214,26 @@ def test_library_fails_loudly_without_device():
     assert lib.negf_version() == 100
     with pytest.raises(libnegf_b200.NegfError):
         libnegf_b200._lib.check(lib.negf_probe_fp64_peak(None, None))
+
+
+def test_oracle_overlap_and_energy_dependent_sigma_vs_dense():
+    # M(E) = (E + i eta) S - H - Sigma(E) (build_M_from_HS, src/matloader.jl:89-95)
+    from oracle import physics
+    base = physics.physics_system(5, 12, seed=17)
+    s = physics.with_overlap_and_sigma_of_E(base, seed=3)
+    for E in (-0.4, 0.35):
+        M = s.M_of_E(E)
+        D = bm_convert_dense(M)
+        G = np.linalg.inv(D)
+        r = physics.solve_energy(s, E)
+        off = np.cumsum([0] + s.sizes)
+        Sin = bm_convert_dense(s.sigma_in(E))
+        Gn = G @ Sin @ np.conj(G).T
+        for i in range(5):
+            blk = np.s_[off[i]:off[i + 1], off[i]:off[i + 1]]
+            assert np.linalg.norm(r["GR"].M[(i, i)] - G[blk]) < 1e-11 * np.linalg.norm(G[blk])
+            assert np.linalg.norm(r["Gn"].M[(i, i)] - Gn[blk]) < 1e-11 * np.linalg.norm(Gn[blk])
+        sL, sR = s.sig(E)
+        g1n = G[off[0]:off[1], off[4]:off[5]]
+        T = np.real(np.trace(s.gamma(sL) @ g1n @ s.gamma(sR) @ np.conj(g1n).T))
+        assert abs(T - r["T"]) < 1e-11 * max(1.0, abs(T))
