@@ -158,22 +158,56 @@ int negf_general_rgf(int32_t nsys, int32_t npl, int32_t ndiag, const int32_t* bl
  * 3 = both.  In place. */
 int negf_selected_inverse(int32_t npl, int32_t b, void* const* Ab, const uint8_t* fill, int32_t mode, void* stream);
 
-/* Domain-decomposed RGF: bndiag_of_inv_ddrgf! with one level
- * (src/matinvertndiag_ddrgf_core.jl:719-758) and the reference's partition
- * (separators of one layer at t*(D1+1), src/matinvertndiag_ddrgf_utils.jl:
- * 278-312, :478-575).  block_size_d1 <= 0 picks the partition from the
- * library's cost model.  Output as negf_rgf (Gu/Gl may be NULL).
- * schur (optional, nsys*3*ntasks dptrs: diag, upper, lower of the separator
- * Schur complement) receives the Schur complement blocks. */
+/* Domain-decomposed RGF: bndiag_of_inv_ddrgf! (src/matinvertndiag_ddrgf_core.jl:
+ * 719-758) with one level and the reference's partition (separators of one
+ * layer at t*(D1+1), src/matinvertndiag_ddrgf_utils.jl:278-312, :478-575);
+ * the separator Schur complement is inverted by sequential RGF.
+ * block_size_d1 <= 0 picks the interior size from the library's cost model.
+ * Output as negf_rgf (Gu/Gl may be NULL). */
 int negf_ddrgf(int32_t nsys, int32_t npl, const int32_t* block_sizes, void* const* Md, void* const* Mu,
                void* const* Ml, int32_t block_size_d1, void* const* Gd, void* const* Gu, void* const* Gl,
                void* stream);
 
+#define NEGF_DDRGF_MAX_LEVELS 6
+
+/* Multi-level DDRGF: level k (k = 0 .. nlevels-1) partitions the separator
+ * Schur complement of level k-1 (the original matrix for k = 0) with interior
+ * size block_size_d1[k]; the last level's Schur complement is inverted by
+ * sequential RGF.  This is the recursion of bndiag_of_inv_ddrgf! through
+ * _inv_Schur_compl! (src/matinvertndiag_ddrgf_core.jl:656-680) over the
+ * levels allocate_aux_data_DDRGF builds (src/matinvertndiag_ddrgf_setup.jl:
+ * 4-51).  A level whose partition has a single task runs sequential RGF
+ * (core.jl:726-729); an impossible partition (get_nr_tasks = -1) is
+ * NEGF_ERR_INVALID.  nlevels = 0 picks the levels from the library's GPU cost
+ * model (negf_ddrgf_choose_levels).  nlevels <= NEGF_DDRGF_MAX_LEVELS.  All
+ * systems share npl; block sizes may differ per system.  Output as negf_rgf
+ * (Gu/Gl may be NULL). */
+int negf_ddrgf_levels(int32_t nsys, int32_t npl, const int32_t* block_sizes, void* const* Md, void* const* Mu,
+                      void* const* Ml, int32_t nlevels, const int32_t* block_size_d1, void* const* Gd,
+                      void* const* Gu, void* const* Gl, void* stream);
+
 /* The reference's partition helper (src/matinvertndiag_ddrgf_utils.jl:
  * 278-312): writes nr_tasks (-1: impossible) and the last interior size. */
 int negf_ddrgf_get_nr_tasks(int32_t npl, int32_t block_size_d1, int32_t* nr_tasks, int32_t* last_d1);
-/* Partition choice of the library's cost model for npl layers of size b. */
+/* One-level partition choice of the library's GPU cost model for npl layers
+ * of size b (npl: sequential RGF is cheaper). */
 int negf_ddrgf_choose_d1(int32_t npl, int32_t b, int32_t nsys, int32_t* block_size_d1);
+/* Level choice of the library's GPU cost model: up to max_levels interior
+ * sizes into block_size_d1 (nlevels = 0: sequential RGF is cheapest).  The
+ * model weighs the serial launch depth of each level against its batched
+ * GEMM work; host only. */
+int negf_ddrgf_choose_levels(int32_t npl, int32_t b, int32_t nsys, int32_t max_levels, int32_t* nlevels,
+                             int32_t* block_size_d1);
+/* The reference's own partition search, restated: opt_params
+ * (src/matinvertndiag_ddrgf_utils.jl:357-453) with cost_rgf / cost_ddrgf
+ * (:221-276) and check_nr_threads (:455-465), for nr_threads CPU threads and
+ * the measured ratios r_lu = t(LU)/t(GEMM), r_mldiv = t(solve)/t(GEMM),
+ * damp_rgf = t(GEMM, 1 thread)/t(GEMM, all threads).  Writes nr_levels and,
+ * per level, nr_tasks and block_size_d1 (arrays of NEGF_DDRGF_MAX_LEVELS) and
+ * the model cost (may be NULL).  allocate_aux_data_DDRGF builds
+ * max(1, nr_levels - 1) DDRGF levels from these (setup.jl:36-48).  Host only. */
+int negf_ddrgf_opt_params(int32_t npl, int32_t nr_threads, double r_lu, double r_mldiv, double damp_rgf,
+                          int32_t* nr_levels, int32_t* nr_tasks, int32_t* block_size_d1, double* cost);
 
 /* ------------------------------------------------------------------------
  * Batched-energy NEGF solver (the reference has no energy loop; this is the
@@ -308,6 +342,25 @@ typedef struct {
 CCscMatrix run_bndiag_wrapper(int32_t m, int32_t n, int32_t nnz_in, int32_t* colptr_in, int32_t* rowval_in,
                               void* nzval_in, int32_t n_blocks, int32_t* block_sizes_in, int32_t n_dict,
                               const char** dict_keys_in, int32_t* dict_vals_in, int32_t is_hermitian);
+
+/* Dense debug path: bndiag_of_inv_direct (src/matinvertndiag_direct.jl:17-61,
+ * :78-85) -- the block n-diagonal part of M^{-1} through the whole inverse,
+ * as a cross-check of the recursive methods on small systems.  M is an n x n
+ * CSC matrix (0-based, rows sorted within each column, as from Julia's
+ * SparseMatrixCSC), block_sizes the layers (sum n), ndiag_out the output
+ * band (odd).  The CSC -> dense scatter, the inverse and the band extraction
+ * run on the device.  Up to n = 1024 the inverse is one Gauss-Jordan
+ * inversion with partial pivoting over all rows (LAPACK's inv does getrf +
+ * getri); above, block elimination over the layers (no pivoting between
+ * layers; every layer <= 1024).  The result is M with its out band replaced
+ * by the inverse's, as the reference's in-place version leaves it: stored
+ * entries of M outside the band are kept, exact zeros of the inverse inside
+ * the band are not stored.  *result receives malloc'd arrays the caller
+ * frees with free().  Device memory: 2 n^2 complex plus the inversion's
+ * workspace. */
+int negf_bndiag_of_inv_direct(int32_t n, int32_t nnz, const int32_t* colptr, const int32_t* rowval,
+                              const void* nzval, int32_t n_blocks, const int32_t* block_sizes, int32_t ndiag_out,
+                              CCscMatrix* result);
 
 /* ------------------------------------------------------------------------
  * Measurement helpers (roofline denominators measured on the device):

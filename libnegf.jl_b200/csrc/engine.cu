@@ -63,8 +63,11 @@ Plan::~Plan() {
   for (void* p : owned_) cudaFree(p);
 }
 
-void* Plan::alloc(size_t bytes) {
-  if (bytes == 0) bytes = 16;
+// Workspace comes from a bump arena of zeroed chunks: the first is 1 MiB and
+// each next one doubles up to 64 MiB, so a plan of thousands of small blocks
+// costs a handful of cudaMalloc calls instead of one per block; a request of
+// 32 MiB or more gets a chunk of its own.  Every piece is 256-byte aligned.
+void* Plan::raw_alloc(size_t bytes) {
   void* p = nullptr;
   if (cudaMalloc(&p, bytes) != cudaSuccess) throw std::bad_alloc();
   if (cudaMemset(p, 0, bytes) != cudaSuccess) {
@@ -73,6 +76,22 @@ void* Plan::alloc(size_t bytes) {
   }
   owned_.push_back(p);
   owned_bytes_ += bytes;
+  return p;
+}
+
+void* Plan::alloc(size_t bytes) {
+  constexpr size_t kFirst = size_t(1) << 20, kCap = size_t(64) << 20;
+  bytes = (std::max<size_t>(bytes, 16) + 255) & ~size_t(255);
+  if (bytes >= kCap / 2) return raw_alloc(bytes);
+  if (chunk_left_ < bytes) {
+    chunk_size_ = chunk_size_ ? std::min(kCap, 2 * chunk_size_) : kFirst;
+    while (chunk_size_ < bytes) chunk_size_ *= 2;
+    chunk_ = static_cast<unsigned char*>(raw_alloc(chunk_size_));
+    chunk_left_ = chunk_size_;
+  }
+  void* p = chunk_;
+  chunk_ += bytes;
+  chunk_left_ -= bytes;
   return p;
 }
 

@@ -56,6 +56,13 @@ cudaError_t launch_csc_band_out(int pass, int n, int npl, int wout, const int* b
                                 const cplx* const* res, const int* colptr_in, const int* rowval_in,
                                 const cplx* nz_in, int nnz_in, int* counts, const int* colptr_out, int* rowval_out,
                                 cplx* nz_out, cudaStream_t st);
+cudaError_t launch_csc_full_scatter(int n, const int* colptr, const int* rowval, const cplx* nz, int nnz,
+                                    const int* blk_of, const int* off, const int* bsz, cplx* const* table, int nb,
+                                    cudaStream_t st);
+cudaError_t launch_csc_direct_out(int pass, int n, int npl, int wout, const int* blk_of, const int* off,
+                                  const int* iblk_of, const int* ioff, const int* ibsz, int nb, const cplx* const* res,
+                                  const int* colptr_in, const int* rowval_in, const cplx* nz_in, int nnz_in,
+                                  int* counts, const int* colptr_out, int* rowval_out, cplx* nz_out, cudaStream_t st);
 // tile_map: per output tile an int4 (problem, m tile | n tile << 16,
 // K chunks | m tiles << 16, n tiles)
 cudaError_t launch_ozaki_mma(const void* probs, const void* tile_map, int total_tiles, int* err, cudaStream_t st);
@@ -132,7 +139,8 @@ class Plan {
   Plan(const Plan&) = delete;
   Plan& operator=(const Plan&) = delete;
 
-  // device memory owned by the plan (workspace); zero-initialised
+  // device memory owned by the plan (workspace); zero-initialised, 256-byte
+  // aligned, sub-allocated from a few large chunks
   void* alloc(size_t bytes);
   cplx* alloc_c(size_t n) { return static_cast<cplx*>(alloc(n * sizeof(cplx))); }
 
@@ -163,16 +171,20 @@ class Plan {
 
   double flops() const;
   size_t num_launches() const;
+  // device bytes the plan holds (its chunks)
   size_t workspace_bytes() const { return owned_bytes_; }
   std::vector<Step> steps;
 
  private:
   cudaError_t launch_step(const Step& s, const unsigned char* base, cudaStream_t stream);
   size_t push_bytes(const void* p, size_t n);
+  void* raw_alloc(size_t bytes);
   std::vector<unsigned char> blob_;
   void* dblob_ = nullptr;
   std::vector<void*> owned_;
   size_t owned_bytes_ = 0;
+  unsigned char* chunk_ = nullptr;  // bump pointer into the current chunk
+  size_t chunk_left_ = 0, chunk_size_ = 0;
   bool finalized_ = false;
   cudaGraph_t graph_ = nullptr;
   cudaGraphExec_t gexec_ = nullptr;

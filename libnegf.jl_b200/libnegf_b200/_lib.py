@@ -16,6 +16,7 @@ NEGF_ERR_INVALID = 1
 NEGF_ERR_CUDA = 2
 NEGF_ERR_SINGULAR = 3
 NEGF_ERR_NOMEM = 4
+NEGF_DDRGF_MAX_LEVELS = 6
 
 c_int32_p = ctypes.POINTER(ctypes.c_int32)
 c_void_pp = ctypes.POINTER(ctypes.c_void_p)
@@ -78,6 +79,12 @@ PROTOTYPES = {
                                   ctypes.c_int32, c_void_pp, c_void_pp, c_void_pp, ctypes.c_void_p]),
     "negf_ddrgf_get_nr_tasks": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, c_int32_p, c_int32_p]),
     "negf_ddrgf_choose_d1": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, c_int32_p]),
+    "negf_ddrgf_levels": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, c_int32_p, c_void_pp, c_void_pp, c_void_pp,
+                                         ctypes.c_int32, c_int32_p, c_void_pp, c_void_pp, c_void_pp, ctypes.c_void_p]),
+    "negf_ddrgf_choose_levels": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                                c_int32_p, c_int32_p]),
+    "negf_ddrgf_opt_params": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_double, c_int32_p, c_int32_p, c_int32_p, c_double_p]),
     "negf_device_create": (ctypes.c_int, [ctypes.c_int32, c_int32_p, c_void_pp, c_void_pp, ctypes.c_void_p,
                                           ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
     "negf_device_upload": (ctypes.c_int, [ctypes.c_void_p, c_void_pp, c_void_pp, ctypes.c_void_p, ctypes.c_void_p]),
@@ -105,6 +112,9 @@ PROTOTYPES = {
                                                 ctypes.POINTER(ctypes.c_int64), ctypes.c_int32]),
     "negf_solver_stats": (ctypes.c_int, [ctypes.c_void_p, c_double_p, ctypes.POINTER(ctypes.c_int64),
                                          ctypes.POINTER(ctypes.c_int64)]),
+    "negf_bndiag_of_inv_direct": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, c_int32_p, c_int32_p,
+                                                 ctypes.c_void_p, ctypes.c_int32, c_int32_p, ctypes.c_int32,
+                                                 ctypes.POINTER(CCscMatrix)]),
     "run_bndiag_wrapper": (CCscMatrix, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, c_int32_p, c_int32_p,
                                         ctypes.c_void_p, ctypes.c_int32, c_int32_p, ctypes.c_int32,
                                         ctypes.POINTER(ctypes.c_char_p), c_int32_p, ctypes.c_int32]),

@@ -275,37 +275,213 @@ def bndiag_of_inv_ddrgf_get_nr_tasks(npl, blockSizeD1, blockSizeD2=1):
 
 
 class AuxDataDDRGF:
-    """src/matinvertndiag_ddrgf_core.jl:1-30 (one level): the partition and
-    the output buffer ``buffMout``."""
+    """One DDRGF level (src/matinvertndiag_ddrgf_core.jl:1-30): the layer sizes
+    of the matrix this level partitions (the original matrix at level 1, the
+    previous level's separator Schur complement below), its interior size and
+    task count, and -- at level 1 -- the output buffer ``buffMout``.  The
+    coarse levels' Schur complements live inside the library's plan."""
 
-    def __init__(self, M, blockSizeD1):
+    def __init__(self, blockSizes, blockSizeD1, level=1):
+        self.level = level
+        self.blockSizes = list(blockSizes)
         self.blockSizeD1 = int(blockSizeD1)
         self.blockSizeD2 = 1
-        self.nrTasks, self.lastSizeD1 = bndiag_of_inv_ddrgf_get_nr_tasks(M.npl, self.blockSizeD1)
-        self.buffMout = BlockMatrix(M.blockSizes, None, {"in": 3, "out": 3}, False, False)
-        bm_blocks_define_(self.buffMout, 1)
+        self.nrTasks, self.lastSizeD1 = bndiag_of_inv_ddrgf_get_nr_tasks(len(self.blockSizes), self.blockSizeD1)
+        self.buffMout = None
+        if level == 1:
+            self.buffMout = BlockMatrix(self.blockSizes, None, {"in": 3, "out": 3}, False, False)
+            bm_blocks_define_(self.buffMout, 1)
+
+    def separator_sizes(self):
+        """Layer sizes of this level's Schur complement (one per separator)."""
+        if self.nrTasks < 1:
+            return []
+        return [self.blockSizes[t * (self.blockSizeD1 + 1)] for t in range(self.nrTasks)]
 
 
-def allocate_aux_data_DDRGF(Min, td=None, cd=None, blockSizeD1=None):
-    """allocate_aux_data_DDRGF (src/matinvertndiag_ddrgf_setup.jl:4-51): the
-    reference times LAPACK probes and searches a cost model
-    (ddrgf_utils.jl:357-453); here the library's cost model for the GPU picks
-    the interior domain size unless blockSizeD1 is given."""
-    if blockSizeD1 is None:
-        d1 = ctypes.c_int32()
-        check(load().negf_ddrgf_choose_d1(Min.npl, max(Min.blockSizes), 1, ctypes.byref(d1)))
-        blockSizeD1 = d1.value
-    return [AuxDataDDRGF(Min, blockSizeD1)]
+def _probe_samples(M):
+    # the reference's sample count (ddrgf_utils.jl:42-44), capped for the GPU
+    avg = max(1, sum(M.blockSizes) // len(M.blockSizes))
+    return avg, min(64, int(1.0e4 * 1.0e5 / avg ** 3) + 10)
+
+
+def _time_ratio(M, op):
+    """Per-sample ratios t(op)/t(GEMM) on blocks of the average size, timed with
+    CUDA events around single-block library calls (one sample = one call)."""
+    import torch
+    from .blockmatrix import be_random_array, be_zero_lu, be_gemm_
+    avg, n = _probe_samples(M)
+    rng = np.random.default_rng(0)
+    A = be_random_array((avg, avg), rng) + to_device(avg * np.eye(avg))
+    B = be_random_array((avg, avg), rng)
+    C = dzeros(avg, avg)
+    lu = be_zero_lu(avg)
+    be_gemm_("N", "N", 1.0, A, B, 1.0, C)
+    op(A, B, C, lu)
+    st = torch.cuda.current_stream()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    ratios = []
+    for _ in range(n):
+        e0.record(st)
+        be_gemm_("N", "N", 1.0, A, B, 1.0, C)
+        e1.record(st)
+        op(A, B, C, lu)
+        e2.record(st)
+        e2.synchronize()
+        ratios.append(e1.elapsed_time(e2) / max(1e-6, e0.elapsed_time(e1)))
+    return np.array(ratios)
+
+
+def get_rLU(M, td=None, cd=None):
+    """get_rLU (src/matinvertndiag_ddrgf_utils.jl:158-219): [mean, std] of
+    t(be_lu!)/t(be_gemm!) on blocks of the average size, on the GPU."""
+    from .blockmatrix import be_lu_
+    r = _time_ratio(M, lambda A, B, C, lu: be_lu_(lu, A))
+    return [float(r.mean()), float(r.std())]
+
+
+def get_rMLDIV(M, td=None, cd=None):
+    """get_rMLDIV (src/matinvertndiag_ddrgf_utils.jl:95-156): [mean, std] of
+    t(be_mldivide!)/t(be_gemm!) with an already factored block, on the GPU."""
+    from .blockmatrix import be_mldivide_
+    r = _time_ratio(M, lambda A, B, C, lu: be_mldivide_("N", C, B, lu))
+    return [float(r.mean()), float(r.std())]
+
+
+def get_dampRGF(M, td=None, cd=None):
+    """get_dampRGF (src/matinvertndiag_ddrgf_utils.jl:36-93) measures how much
+    slower a GEMM runs on one BLAS thread than on all of them, the share of
+    the machine the coarse sequential RGF gets.  A GPU step has no such split
+    (every launch of the Schur RGF gets the whole GPU): [1.0, 0.0]."""
+    return [1.0, 0.0]
+
+
+def _max_levels():
+    from ._lib import NEGF_DDRGF_MAX_LEVELS
+    return NEGF_DDRGF_MAX_LEVELS
+
+
+def opt_params(Min, rLU, rMLDIV, dampRGF, nrThreads=None):
+    """opt_params (src/matinvertndiag_ddrgf_utils.jl:357-453), the reference's
+    partition search restated in the library: returns (nrLevels,
+    nrTasksList, blockSizeD1List, optCost) for nrThreads CPU threads
+    (default: all host cores).  Min: a BlockMatrix or its layer count."""
+    import os
+    K = _max_levels()
+    nl = ctypes.c_int32()
+    tasks = (ctypes.c_int32 * K)()
+    d1 = (ctypes.c_int32 * K)()
+    cost = ctypes.c_double()
+    npl = Min if isinstance(Min, int) else len(Min.blockSizes)
+    check(load().negf_ddrgf_opt_params(npl, int(nrThreads or os.cpu_count() or 1), float(rLU), float(rMLDIV),
+                                       float(dampRGF), ctypes.byref(nl), tasks, d1, ctypes.byref(cost)))
+    return nl.value, list(tasks[:nl.value]), list(d1[:nl.value]), cost.value
+
+
+def choose_levels(npl, blockSize, nsys=1, maxLevels=None):
+    """Interior sizes per level from the library's GPU cost model ([] when
+    sequential RGF is cheapest)."""
+    nl = ctypes.c_int32()
+    d1 = (ctypes.c_int32 * _max_levels())()
+    check(load().negf_ddrgf_choose_levels(npl, blockSize, nsys, int(maxLevels or _max_levels()), ctypes.byref(nl),
+                                          d1))
+    return list(d1[:nl.value])
+
+
+def allocate_aux_data_DDRGF(Min, td=None, cd=None, blockSizeD1=None, costModel="gpu", nrThreads=None):
+    """allocate_aux_data_DDRGF (src/matinvertndiag_ddrgf_setup.jl:4-51): one
+    ``AuxDataDDRGF`` per level.
+
+    blockSizeD1: an interior size (one level) or a list (one per level).
+    Without it the levels come from a cost model: ``costModel="reference"``
+    runs the reference's probes (get_rLU / get_rMLDIV / get_dampRGF, timed on
+    the GPU) and its opt_params search, and builds max(1, nrLevels - 1)
+    levels from the result as the reference does (setup.jl:36-48);
+    ``costModel="gpu"`` (default) uses the library's GPU model (serial
+    launch depth against batched GEMM work).  An empty choice (sequential RGF
+    is cheapest) gives one level with blockSizeD1 = npl."""
+    npl = Min.npl
+    if blockSizeD1 is not None:
+        d1s = [int(blockSizeD1)] if np.isscalar(blockSizeD1) else [int(d) for d in blockSizeD1]
+    elif costModel == "reference":
+        rLU = get_rLU(Min, td, cd)[0]
+        rMLDIV = get_rMLDIV(Min, td, cd)[0]
+        damp = get_dampRGF(Min, td, cd)[0]
+        nrLevels, _, d1List, _ = opt_params(Min, rLU, rMLDIV, damp, nrThreads)
+        d1s = d1List[:max(1, nrLevels - 1)]
+    else:
+        d1s = choose_levels(npl, max(Min.blockSizes), 1) or [npl]
+    aux, sizes = [], list(Min.blockSizes)
+    for k, d1 in enumerate(d1s):
+        a = AuxDataDDRGF(sizes, d1, level=k + 1)
+        aux.append(a)
+        if a.nrTasks < 2 or d1 >= len(sizes):
+            break
+        sizes = a.separator_sizes()
+    return aux
 
 
 def bndiag_of_inv_ddrgf_(Min, listOfAuxData, td=None, cd=None, depth=1):
-    """bndiag_of_inv_ddrgf! (src/matinvertndiag_ddrgf_core.jl:719-758): the
-    block tridiagonal of Min^{-1} lands in listOfAuxData[0].buffMout."""
+    """bndiag_of_inv_ddrgf! (src/matinvertndiag_ddrgf_core.jl:719-758) over
+    the levels listOfAuxData[depth-1:], in one library call: the block
+    tridiagonal of Min^{-1} lands in listOfAuxData[depth-1].buffMout."""
     aux = listOfAuxData[depth - 1]
+    if aux.buffMout is None:
+        raise ValueError("the output of a coarse DDRGF level stays inside the library")
     npl, sizes, Md, Mu, Ml = _tri_tables([Min])
     out = aux.buffMout
     Gd = [dptr(out.M[(i, i)]) for i in range(npl)]
     Gu = [dptr(out.M[(i, i + 1)]) for i in range(npl - 1)]
     Gl = [dptr(out.M[(i + 1, i)]) for i in range(npl - 1)]
-    check(load().negf_ddrgf(1, npl, int_array(sizes), ptr_array(Md), ptr_array(Mu), ptr_array(Ml),
-                            aux.blockSizeD1, ptr_array(Gd), ptr_array(Gu), ptr_array(Gl), stream_handle()))
+    d1s = [a.blockSizeD1 for a in listOfAuxData[depth - 1:]]
+    check(load().negf_ddrgf_levels(1, npl, int_array(sizes), ptr_array(Md), ptr_array(Mu), ptr_array(Ml),
+                                   len(d1s), int_array(d1s), ptr_array(Gd), ptr_array(Gu), ptr_array(Gl),
+                                   stream_handle()))
+
+
+# --------------------------------------------------------------------------
+# Dense debug path (src/matinvertndiag_direct.jl)
+
+def _csc_direct(M, blockSizes, ndiag):
+    import scipy.sparse as sp
+    from ._lib import CCscMatrix
+    A = sp.csc_matrix(M, dtype=np.complex128, copy=True)
+    A.sort_indices()
+    n = A.shape[0]
+    if A.shape[1] != n:
+        raise ValueError("bndiag_of_inv_direct needs a square matrix")
+    colptr = np.ascontiguousarray(A.indptr, dtype=np.int32)
+    rowval = np.ascontiguousarray(A.indices, dtype=np.int32)
+    nz = np.ascontiguousarray(A.data, dtype=np.complex128)
+    res = CCscMatrix()
+    c_int32_p = ctypes.POINTER(ctypes.c_int32)
+    check(load().negf_bndiag_of_inv_direct(n, A.nnz, colptr.ctypes.data_as(c_int32_p),
+                                           rowval.ctypes.data_as(c_int32_p), nz.ctypes.data, len(blockSizes),
+                                           int_array([int(b) for b in blockSizes]), int(ndiag.get("out", 3)),
+                                           ctypes.byref(res)))
+    libc = ctypes.CDLL(None)
+    try:
+        cp = np.ctypeslib.as_array(res.colptr, shape=(n + 1,)).copy()
+        rv = np.ctypeslib.as_array(res.rowval, shape=(max(1, res.nnz),))[:res.nnz].copy()
+        vals = np.ctypeslib.as_array(ctypes.cast(res.nzval, ctypes.POINTER(ctypes.c_double)),
+                                     shape=(2 * max(1, res.nnz),))[:2 * res.nnz].copy()
+    finally:
+        for p in (res.colptr, res.rowval, res.nzval):
+            libc.free(ctypes.cast(p, ctypes.c_void_p))
+    return sp.csc_matrix((vals[0::2] + 1j * vals[1::2], rv, cp), shape=(n, n))
+
+
+def bndiag_of_inv_direct(M, blockSizes, ndiag):
+    """bndiag_of_inv_direct (src/matinvertndiag_direct.jl:78-85, and the
+    catch-all form :100-140 for dense input): the block n-diagonal part of
+    M^{-1} (ndiag["out"]) through the whole inverse, computed on the GPU; M is
+    a scipy sparse matrix or a dense array, the result a scipy CSC matrix."""
+    return _csc_direct(M, blockSizes, ndiag)
+
+
+def bndiag_of_inv_direct_(M, blockSizes, ndiag):
+    """bndiag_of_inv_direct! (src/matinvertndiag_direct.jl:17-61): M (scipy
+    CSC) becomes itself with its out band replaced by the inverse's."""
+    R = _csc_direct(M, blockSizes, ndiag)
+    M.data, M.indices, M.indptr = R.data, R.indices, R.indptr
+    M.has_sorted_indices = True

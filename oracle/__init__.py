@@ -22,4 +22,4 @@ and through committed fixtures under ``tests/golden/`` made by
 """
 
 from .blockmatrix import BlockMatrix, bm_convert_dense, bm_from_dense, bm_copy  # noqa: F401
-from . import backend_cpu, generators, rgf, general_rgf, keldysh, selected_inverse, ddrgf, physics  # noqa: F401
+from . import backend_cpu, generators, rgf, general_rgf, keldysh, selected_inverse, ddrgf, physics, direct  # noqa: F401

@@ -15,6 +15,7 @@ import pytest
 
 from conftest import kappa_tol, rel_fro
 from oracle import rgf as o_rgf, general_rgf as o_grgf, selected_inverse as o_si, ddrgf as o_dd
+from oracle import direct as o_direct
 from oracle.blockmatrix import bm_convert_dense, band_of_dense, bm_fuse_to_tridiagonal as o_fuse
 from oracle.generators import bm_create_synthetic_random, set_sparse_block, full_of_blocks
 
@@ -165,6 +166,79 @@ def test_ddrgf_auto_partition(negf):
     assert rel_fro(negf.bm_to_dense(aux[0].buffMout), seq) < 2.5e-10
 
 
+@pytest.mark.parametrize("npl,b,d1s", [(128, 16, [4, 3]), (64, 24, [3, 1, 1]), (40, 12, [3, 1, 2]),
+                                       (128, 8, [7, 7]), (200, 8, None)])
+def test_ddrgf_multilevel_vs_rgf(negf, npl, b, d1s):
+    # the recursion of bndiag_of_inv_ddrgf! through _inv_Schur_compl!
+    # (matinvertndiag_ddrgf_core.jl:656-680); None = the GPU cost model's levels
+    M = bm_create_synthetic_random(npl, b, seed=npl * 7 + b)
+    seq = bm_convert_dense(o_rgf.bndiag_of_inv_rgf_local(M))
+    dM = _to_gpu_bm(negf, M)
+    aux = negf.allocate_aux_data_DDRGF(dM, blockSizeD1=d1s)
+    used = [a.blockSizeD1 for a in aux]
+    if d1s is not None:
+        assert used == d1s
+    else:
+        assert len(used) >= 2, used
+    n = npl
+    for a in aux:  # task counts chain through the levels as the oracle's partition
+        assert a.nrTasks == o_dd.get_nr_tasks(n, a.blockSizeD1)[0]
+        n = a.nrTasks
+    negf.bndiag_of_inv_ddrgf_(dM, aux)
+    G = negf.bm_to_dense(aux[0].buffMout)
+    assert rel_fro(G, seq) < 2.5e-10
+    o_par, _ = o_dd.bndiag_of_inv_ddrgf(M, used)
+    assert rel_fro(G, bm_convert_dense(o_par)) < 2.5e-10
+
+
+def test_ddrgf_reference_cost_model(negf):
+    # test_matinvertndiag_ddrgf.jl:13-14, :86-158: npl = 128, b = 64, levels from
+    # allocate_aux_data_DDRGF's probes + opt_params (here the probes time the
+    # library's kernels), DDRGF vs sequential RGF at 2.5e-10
+    M = bm_create_synthetic_random(128, 64, seed=1234)
+    seq = bm_convert_dense(o_rgf.bndiag_of_inv_rgf_local(M))
+    dM = _to_gpu_bm(negf, M)
+    rlu, rml = negf.get_rLU(dM), negf.get_rMLDIV(dM)
+    assert rlu[0] > 0 and rml[0] > 0
+    aux = negf.allocate_aux_data_DDRGF(dM, costModel="reference", nrThreads=8)
+    assert 1 <= len(aux) <= 6 and all(1 <= a.blockSizeD1 <= 4 for a in aux)
+    negf.bndiag_of_inv_ddrgf_(dM, aux)
+    assert rel_fro(negf.bm_to_dense(aux[0].buffMout), seq) < 2.5e-10
+
+
+def test_ddrgf_levels_batched_uneven_and_errors(negf):
+    # two systems of 48 layers with different block sizes in one call, upper /
+    # lower outputs not requested (NULL); then an impossible coarse partition
+    from libnegf_b200._lib import NegfError, check, int_array, ptr_array
+    lib = negf.load()
+    npl, d1s = 48, [3, 2]
+    mats = [bm_create_synthetic_random(npl, 10, seed=3), bm_create_synthetic_random(npl, 17, seed=4)]
+    keep, sizes, Md, Mu, Ml, Gd, outs = [], [], [], [], [], [], []
+    for M in mats:
+        sizes += M.blockSizes
+        for i in range(npl):
+            keep.append(negf.to_device(M.M[(i, i)])); Md.append(keep[-1].data_ptr())
+        for i in range(npl - 1):
+            keep.append(negf.to_device(M.M[(i, i + 1)])); Mu.append(keep[-1].data_ptr())
+            keep.append(negf.to_device(M.M[(i + 1, i)])); Ml.append(keep[-1].data_ptr())
+        o = [negf.dzeros(b, b) for b in M.blockSizes]
+        outs.append(o)
+        Gd += [t.data_ptr() for t in o]
+    check(lib.negf_ddrgf_levels(2, npl, int_array(sizes), ptr_array(Md), ptr_array(Mu), ptr_array(Ml), len(d1s),
+                                int_array(d1s), ptr_array(Gd), None, None, None))
+    for M, o in zip(mats, outs):
+        ref, _ = o_dd.bndiag_of_inv_ddrgf(M, d1s)
+        for i in range(npl):
+            assert rel_fro(negf.to_host(o[i]), ref.M[(i, i)]) < 2.5e-10
+    # 48 layers, D1 = 3: 12 separators; D1 = 2 on 12 layers: 4 tasks; D1 = 2 on 4
+    # layers is impossible (get_nr_tasks = -1): rejected before any launch
+    assert o_dd.get_nr_tasks(4, 2)[0] == -1
+    bad = [3, 2, 2]
+    with pytest.raises(NegfError):
+        check(lib.negf_ddrgf_levels(2, npl, int_array(sizes), ptr_array(Md), ptr_array(Mu), ptr_array(Ml), 3,
+                                    int_array(bad), ptr_array(Gd), None, None, None))
+
+
 def test_run_bndiag_wrapper(negf):
     # the reference C example (src/c_interface/libnegf_c_example.c) builds a
     # random block tridiagonal CSC matrix and calls run_bndiag_wrapper
@@ -254,3 +328,68 @@ def test_run_bndiag_wrapper_wide_out_band(negf):
     out = _call_wrapper(negf, D, npl, b, 5, False)
     ref = band_of_dense(np.linalg.inv(D), M.blockSizes, {"in": 3, "out": 3})
     assert rel_fro(out, ref) < 2.5e-10 * max(1.0, np.linalg.cond(D) / 1e4)
+
+
+def _direct_case(negf, M, sizes, nd_out):
+    import scipy.sparse as sp
+    A = sp.csc_matrix(M)
+    R = negf.bndiag_of_inv_direct(A, sizes, {"in": 3, "out": nd_out})
+    ref, inv = o_direct.bndiag_of_inv_direct(A, sizes, {"in": 3, "out": nd_out})
+    return R, ref, inv
+
+
+@pytest.mark.parametrize("npl,b,nd_out", [(12, 32, 3), (6, 50, 5), (10, 128, 3), (3, 7, 3), (1, 40, 3)])
+def test_bndiag_of_inv_direct(negf, npl, b, nd_out):
+    # test_matinvertndiag_direct.jl:34-47: relErr (2-norm) of the direct band
+    # against the reference band < roundoff * cond * 10; n = 1280 (10 x 128)
+    # takes the block-elimination form, the others one Gauss-Jordan inverse
+    Mb = bm_create_synthetic_random(npl, b, seed=npl * 11 + b)
+    D = bm_convert_dense(Mb)
+    R, ref, inv = _direct_case(negf, D, Mb.blockSizes, nd_out)
+    G = R.toarray()
+    cond = np.linalg.cond(D)
+    assert np.linalg.norm(G - ref, 2) / np.linalg.norm(ref, 2) < 1e-15 * cond * 10
+    # and against RGF's tridiagonal of the inverse (an independent method)
+    if nd_out == 3 and npl > 1:
+        seq = bm_convert_dense(o_rgf.bndiag_of_inv_rgf_local(Mb))
+        assert rel_fro(G, seq) < kappa_tol(cond)
+    # stored pattern: the out band of the inverse (no exact zeros there)
+    off = np.concatenate([[0], np.cumsum(Mb.blockSizes)])
+    w = (nd_out - 1) // 2
+    mask = np.zeros_like(D, dtype=bool)
+    for i in range(npl):
+        for j in range(max(0, i - w), min(npl, i + w + 1)):
+            mask[off[i]:off[i + 1], off[j]:off[j + 1]] = True
+    assert R.nnz == int(mask.sum())
+    assert np.all(R.toarray()[~mask] == 0)
+
+
+def test_bndiag_of_inv_direct_keeps_entries_outside_the_band(negf):
+    # a pentadiagonal input with a tridiagonal output: the reference writes the
+    # tridiagonal of the inverse into M, whose other stored entries stay
+    import scipy.sparse as sp
+    Mb = bm_create_synthetic_random(8, 24, seed=21, ndiag=5)
+    D = bm_convert_dense(Mb)
+    A = sp.csc_matrix(D)
+    R, ref, inv = _direct_case(negf, D, Mb.blockSizes, 3)
+    G = R.toarray()
+    off = np.concatenate([[0], np.cumsum(Mb.blockSizes)])
+    band = np.zeros_like(D, dtype=bool)
+    for i in range(8):
+        for j in range(max(0, i - 1), min(8, i + 2)):
+            band[off[i]:off[i + 1], off[j]:off[j + 1]] = True
+    assert np.array_equal(G[~band], D[~band])  # bit-exact copies of M
+    assert rel_fro(G[band], inv[band]) < 1e-12
+    # in place on a scipy matrix
+    negf.bndiag_of_inv_direct_(A, Mb.blockSizes, {"in": 5, "out": 3})
+    assert np.array_equal(A.toarray(), G)
+
+
+def test_bndiag_of_inv_direct_rejects_bad_input(negf):
+    import scipy.sparse as sp
+    from libnegf_b200 import NegfError
+    D = np.eye(8, dtype=np.complex128)
+    with pytest.raises(NegfError):
+        negf.bndiag_of_inv_direct(sp.csc_matrix(D), [4, 3], {"out": 3})  # sizes do not add up
+    with pytest.raises(NegfError):
+        negf.bndiag_of_inv_direct(sp.csc_matrix(D), [4, 4], {"out": 4})  # even band

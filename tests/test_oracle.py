@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from conftest import ROOT, rel_fro
-from oracle import rgf, general_rgf, keldysh, selected_inverse, ddrgf, physics
+from oracle import rgf, general_rgf, keldysh, selected_inverse, ddrgf, physics, direct
 from oracle.blockmatrix import bm_convert_dense, band_of_dense, bm_from_dense, bm_fuse_to_tridiagonal
 from oracle.generators import bm_create_synthetic_random, hermitian_random_like, set_sparse_block, full_of_blocks
 
@@ -105,6 +105,65 @@ def test_ddrgf_schur_complement_exact():
     for (t, u), blk in S.items():
         approx[so[t]:so[t + 1], so[u]:so[u + 1]] = blk
     assert rel_fro(approx, exact) < ROUNDOFF64 * 2.5e5
+
+
+@pytest.mark.parametrize("npl,b,d1s", [(128, 6, [4, 3]), (64, 8, [3, 1, 1]), (40, 10, [3, 1, 2]), (128, 6, [7, 7])])
+def test_ddrgf_multilevel_vs_sequential(npl, b, d1s):
+    # the Schur complement recursion (matinvertndiag_ddrgf_core.jl:656-680):
+    # every level's partition is possible, the result matches sequential RGF
+    # at test_matinvertndiag_ddrgf.jl's tolerance (2.5e-10)
+    n = npl
+    for d1 in d1s:
+        nr, _ = ddrgf.get_nr_tasks(n, d1)
+        assert nr >= 2
+        n = nr
+    M = bm_create_synthetic_random(npl, b, seed=npl + sum(d1s))
+    Gs = bm_convert_dense(rgf.bndiag_of_inv_rgf_local(M))
+    Gp, _ = ddrgf.bndiag_of_inv_ddrgf(M, d1s)
+    assert rel_fro(bm_convert_dense(Gp), Gs) < ROUNDOFF64 * 2.5e5
+
+
+def test_ddrgf_cost_model_known_answers():
+    # worked by hand from matinvertndiag_ddrgf_utils.jl:221-276, :357-465:
+    # cost_rgf(3, full): 4*2 + 3 GEMMs + 2*3 LU + 1.5*7 solves = 27.5
+    assert ddrgf.cost_rgf(3, 2.0, 1.5, True) == 27.5
+    # cost_rgf(4, coarse): 12 GEMMs + 2*4 + 1.5*10 = 35
+    assert ddrgf.cost_rgf(4, 2.0, 1.5, False) == 35.0
+    # 4 tasks on 8 threads: check_nr_threads settles at 4 threads, 1 task each
+    assert ddrgf.check_nr_threads(8, 4) == (4, 1, 1)
+    assert ddrgf.check_nr_threads(3, 10) == (3, 4, 2)
+    # npl = 16: D1 = 4 is impossible (get_nr_tasks = -1), D1 = 3 gives 4 tasks
+    # at 73.5 + coarse 35 = 108.5; smaller level-1 sizes are pruned after that
+    assert ddrgf.cost_ddrgf(2.0, 1.5, 4, 4, 3) == 73.5
+    assert ddrgf.opt_params(16, 2.0, 1.5, 1.0, 8) == (1, [4], [3], 108.5)
+    # allocate_aux_data_DDRGF builds max(1, nrLevels - 1) levels (setup.jl:36-48)
+    assert ddrgf.levels_used(1, [3]) == [3]
+    assert ddrgf.levels_used(2, [4, 3]) == [4]
+    assert ddrgf.levels_used(4, [4, 1, 1, 2]) == [4, 1, 1]
+
+
+def test_library_ddrgf_partition_search_matches_oracle():
+    # host-only entry points: negf_ddrgf_opt_params against the oracle's
+    # restatement; negf_ddrgf_choose_levels gives possible partitions
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "libnegf.jl_b200"))
+    import libnegf_b200 as L
+    for npl in list(range(2, 40)) + [64, 128, 500, 2048]:
+        for thr in (1, 3, 8, 64):
+            for r in ((2.0, 1.5, 1.0), (0.5, 3.0, 0.3), (7.0, 0.2, 4.0)):
+                a = L.opt_params(npl, *r, nrThreads=thr)
+                o = ddrgf.opt_params(npl, *r, thr)
+                assert a[:3] == o[:3], (npl, thr, r)
+                assert abs(a[3] - o[3]) <= 1e-12 * abs(o[3])
+    for npl, b in ((64, 512), (128, 64), (1024, 32), (4096, 32), (7, 16)):
+        n = npl
+        d1s = L.choose_levels(npl, b)
+        assert len(d1s) <= 6
+        for d1 in d1s:
+            nr, _ = ddrgf.get_nr_tasks(n, d1)
+            assert nr >= 2
+            n = nr
+    assert L.choose_levels(4096, 32), "a long device with small blocks should decompose"
 
 
 @pytest.mark.parametrize("npl,d1,expect", [(64, 15, (4, 0)), (128, 15, (8, 0)), (40, 6, (6, 4)), (17, 3, (-1, 0)),
@@ -237,3 +296,19 @@ def test_oracle_overlap_and_energy_dependent_sigma_vs_dense():
         g1n = G[off[0]:off[1], off[4]:off[5]]
         T = np.real(np.trace(s.gamma(sL) @ g1n @ s.gamma(sR) @ np.conj(g1n).T))
         assert abs(T - r["T"]) < 1e-11 * max(1.0, abs(T))
+
+
+def test_direct_oracle_band_and_outside_entries():
+    # bndiag_of_inv_direct! (matinvertndiag_direct.jl:17-61): the out band of
+    # inv(M) written into M; M's entries outside the band stay
+    M = bm_create_synthetic_random(6, 8, seed=2, ndiag=5)
+    D = bm_convert_dense(M)
+    out, inv = direct.bndiag_of_inv_direct(D, M.blockSizes, {"in": 5, "out": 3})
+    band = band_of_dense(inv, M.blockSizes, {"in": 3, "out": 3})
+    assert np.array_equal(out[band != 0], band[band != 0])
+    off = np.concatenate([[0], np.cumsum(M.blockSizes)])
+    assert np.array_equal(out[0:off[1], off[2]:off[3]], D[0:off[1], off[2]:off[3]])
+    # on a tridiagonal matrix the band agrees with sequential RGF
+    T = bm_create_synthetic_random(6, 8, seed=3)
+    out3, _ = direct.bndiag_of_inv_direct(bm_convert_dense(T), T.blockSizes, {"in": 3, "out": 3})
+    assert rel_fro(out3, bm_convert_dense(rgf.bndiag_of_inv_rgf_local(T))) < 1e-12
