@@ -304,6 +304,15 @@ int negf_solver_outputs(negf_solver_t s, void** gr_dev, void** gl_dev, double** 
 /* Copy the resident outputs into host buffers (pinned for full speed) on
  * `stream` and wait: gr/gl as in negf_solve, t as 2*nE doubles (re, im). */
 int negf_solver_download(negf_solver_t s, void* gr_host, void* gl_host, double* t_host, void* stream);
+/* One pass with the downloads overlapped: each diagonal G^R block layer is
+ * copied to the host as soon as the downward RGF pass has finished it, each
+ * G^< layer as soon as the last RKD pass has, on a copy stream of the solver
+ * that runs beside the remaining launches (the pass replays launch by launch
+ * instead of as a graph).  Same outputs and layout as negf_solver_run +
+ * negf_solver_download; waits for everything and checks the pivot flags
+ * before returning.  Host buffers that are not pinned fall back to run, then
+ * download. */
+int negf_solver_run_download(negf_solver_t s, void* gr_host, void* gl_host, double* t_host, void* stream);
 /* Synchronous check of the zero-pivot flags of the last run. */
 int negf_solver_check(negf_solver_t s);
 /* One pass launch by launch (no graph) with a CUDA event recorded after every

@@ -480,6 +480,20 @@ cudaError_t Plan::run_events(cudaStream_t stream, const std::vector<cudaEvent_t>
   return cudaSuccess;
 }
 
+cudaError_t Plan::run_marked(cudaStream_t stream, const std::function<cudaError_t(int)>& at_mark) {
+  cudaError_t e = finalize();
+  if (e != cudaSuccess) return e;
+  const unsigned char* base = static_cast<const unsigned char*>(dblob_);
+  size_t m = 0;
+  for (size_t i = 0; i <= steps.size(); ++i) {
+    for (; m < marks_.size() && marks_[m].first == i; ++m)
+      if ((e = at_mark(marks_[m].second)) != cudaSuccess) return e;
+    if (i == steps.size()) break;
+    if ((e = launch_step(steps[i], base, stream)) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 cudaError_t Plan::run(cudaStream_t stream, bool use_graph) {
   cudaError_t e = finalize();
   if (e != cudaSuccess) return e;
@@ -646,7 +660,7 @@ void build_rgf_upward(Plan& plan, const std::vector<TriSystem>& sys, std::vector
 }
 
 void build_rgf_downward(Plan& plan, const std::vector<TriSystem>& sys, std::vector<RgfWork>& work,
-                        std::vector<TriOut>& out) {
+                        std::vector<TriOut>& out, const std::function<void(int)>& on_final) {
   int maxN = 0;
   for (const auto& s : sys) maxN = std::max(maxN, s.npl());
   // G_11 = X_1^{-1}  (rgf.jl:169)
@@ -662,6 +676,7 @@ void build_rgf_downward(Plan& plan, const std::vector<TriSystem>& sys, std::vect
     }
     plan.blockops(ops);
   }
+  if (on_final && maxN > 0) on_final(0);
   for (int i = 1; i < maxN; ++i) {
     // G[i-1,i] = -G[i-1,i-1] R_{i-1};  G[i,i-1] = -L_i G[i-1,i-1]  (rgf.jl:174,177)
     std::vector<ZGemmProblem> pr;
@@ -687,6 +702,7 @@ void build_rgf_downward(Plan& plan, const std::vector<TriSystem>& sys, std::vect
                       MONE, w.g[i], s.b[i], ONE));
     }
     plan.gemm('N', 'N', dp);
+    if (on_final) on_final(i);
   }
 }
 
@@ -721,7 +737,7 @@ void build_rgf_full_inverse(Plan& plan, const std::vector<TriSystem>& sys, std::
 // be_mldivide!('N', ., ., LU(X_i)) applied as a product with g_i = X_i^{-1}.
 
 void build_rkd(Plan& plan, const std::vector<TriSystem>& sys, std::vector<RgfWork>& work,
-               std::vector<HermBlocks>& S) {
+               std::vector<HermBlocks>& S, const std::function<void(int)>& on_final) {
   int maxN = 0;
   for (const auto& s : sys) maxN = std::max(maxN, s.npl());
   // workspace: xb diagonal chain (npl blocks), m2/t temporaries (npl blocks each)
@@ -860,7 +876,10 @@ void build_rkd(Plan& plan, const std::vector<TriSystem>& sys, std::vector<RgfWor
                        MONE, h.d[i + 1], h.ldd[i + 1], ONE));
     }
     plan.gemm('N', 'N', d3v);
+    // iteration i last reads S[i,i] (d2)
+    if (on_final) on_final(i);
   }
+  if (on_final && maxN > 0) on_final(maxN - 1);
 }
 
 }  // namespace negf

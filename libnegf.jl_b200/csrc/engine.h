@@ -10,6 +10,7 @@
 #pragma once
 
 #include <string>
+#include <functional>
 #include <vector>
 #include <cstddef>
 
@@ -168,6 +169,13 @@ class Plan {
   // Launch-by-launch replay with a CUDA event recorded after every launch
   // (events[0] before the first); events must hold steps.size() + 1 events.
   cudaError_t run_events(cudaStream_t stream, const std::vector<cudaEvent_t>& events);
+  // Markers: mark(tag) notes that everything built so far is done at this
+  // point of the pass; run_marked replays launch by launch (no graph) and
+  // calls at_mark(tag) in stream order at every marker, so the caller can
+  // record an event there and start work that depends on it.
+  void mark(int tag) { marks_.push_back({steps.size(), tag}); }
+  const std::vector<std::pair<size_t, int>>& marks() const { return marks_; }
+  cudaError_t run_marked(cudaStream_t stream, const std::function<cudaError_t(int)>& at_mark);
 
   double flops() const;
   size_t num_launches() const;
@@ -183,6 +191,7 @@ class Plan {
   void* dblob_ = nullptr;
   std::vector<void*> owned_;
   size_t owned_bytes_ = 0;
+  std::vector<std::pair<size_t, int>> marks_;
   unsigned char* chunk_ = nullptr;  // bump pointer into the current chunk
   size_t chunk_left_ = 0, chunk_size_ = 0;
   bool finalized_ = false;
@@ -243,8 +252,10 @@ void build_rgf_upward(Plan& plan, const std::vector<TriSystem>& sys, std::vector
 // Downward pass (src/matinvertndiag_rgf.jl:166-182) writing the tridiagonal of
 // M^{-1}; with full_rows/full_cols the whole inverse (rgf.jl:185-199) is
 // written into full[s][i*npl+j] (null = skip).
+// on_final(i), when given, is called once layer i's diagonal output is final
+// for every system (in layer order).
 void build_rgf_downward(Plan& plan, const std::vector<TriSystem>& sys, std::vector<RgfWork>& work,
-                        std::vector<TriOut>& out);
+                        std::vector<TriOut>& out, const std::function<void(int)>& on_final = {});
 void build_rgf_full_inverse(Plan& plan, const std::vector<TriSystem>& sys, std::vector<RgfWork>& work,
                             std::vector<std::vector<cplx*>>& full);
 // RKD passes (src/keldyshndiag.jl:221-317).  S holds the Hermitian middle
@@ -253,8 +264,10 @@ struct HermBlocks {
   std::vector<cplx*> d, u;
   std::vector<int> ldd, ldu;
 };
+// on_final(i), when given, is called once G^n's diagonal block i is final
+// (no later step of the pass reads or writes it) for every system.
 void build_rkd(Plan& plan, const std::vector<TriSystem>& sys, std::vector<RgfWork>& work,
-               std::vector<HermBlocks>& S);
+               std::vector<HermBlocks>& S, const std::function<void(int)>& on_final = {});
 
 std::string& last_error();
 void set_error(const std::string& msg);

@@ -160,11 +160,19 @@ struct negf_solver_s {
   size_t per_energy = 0;   // sum b_i^2 (single-device solvers; 0 for a multi-device batch)
   std::vector<std::vector<cudaEvent_t>> ev_sets;  // one event set per profiled pass
   size_t ev_used = 0;
+  cudaStream_t copy_stream = nullptr;  // overlapped downloads (negf_solver_run_download)
+  cudaEvent_t mark_ev = nullptr, join_ev = nullptr;
   ~negf_solver_s() {
     for (auto& v : ev_sets)
       for (cudaEvent_t e : v) cudaEventDestroy(e);
+    if (mark_ev) cudaEventDestroy(mark_ev);
+    if (join_ev) cudaEventDestroy(join_ev);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
   }
 };
+
+// Plan marker tags of the solver pass: output layer i final.
+constexpr int kMarkGR = 0, kMarkGL = 1 << 20;
 
 namespace {
 
@@ -401,21 +409,22 @@ int build_solver(negf_solver_s& S) {
         o.ldl.push_back(d.b[i + 1]);
       }
     }
-    build_rgf_downward(plan, sys, work, out);
+    build_rgf_downward(plan, sys, work, out, [&](int i) { plan.mark(kMarkGR + i); });
   }
   if (S.opts.want_gl) {
-    build_rkd(plan, sys, work, herm);
-    // G^< = i G^n
-    std::vector<ZBlockOp> sc;
-    for (int e = 0; e < nE; ++e) {
-      const negf_device_s& d = *items[e].d;
-      for (int i = 0; i < d.npl; ++i) {
+    // G^< = i G^n, layer by layer as soon as G^n's layer is final
+    build_rkd(plan, sys, work, herm, [&](int i) {
+      std::vector<ZBlockOp> sc;
+      for (int e = 0; e < nE; ++e) {
+        const negf_device_s& d = *items[e].d;
+        if (i >= d.npl) continue;
         ZBlockOp o{}; o.A = herm[e].d[i]; o.lda = d.b[i]; o.C = herm[e].d[i]; o.ldc = d.b[i];
         o.m = o.n = d.b[i]; o.kind = ZOP_AXPBY; o.alpha_ptr = S.params + 3 * nE; o.beta = make_double2(0.0, 0.0);
         sc.push_back(o);
       }
-    }
-    plan.blockops(sc);
+      plan.blockops(sc);
+      plan.mark(kMarkGL + i);
+    });
   }
   if (S.opts.want_t) {
     // G^R_{1N} by G_{1,j} = -G_{1,j-1} R_{j-1}, G_{1,1} = g_1 (rgf.jl:169, :185-199)
@@ -989,6 +998,65 @@ int negf_solver_download(negf_solver_t s, void* gr_host, void* gl_host, double* 
   return NEGF_SUCCESS;
 }
 
+int negf_solver_run_download(negf_solver_t s, void* gr_host, void* gl_host, double* t_host, void* stream) {
+  if (!s) return fail(NEGF_ERR_INVALID, "NULL solver");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // copies into pageable memory would block the host between launches: then
+  // run the pass and download after it
+  auto pinned = [](const void* p) {
+    cudaPointerAttributes a{};
+    return p == nullptr || (cudaPointerGetAttributes(&a, p) == cudaSuccess && a.type == cudaMemoryTypeHost);
+  };
+  if (!pinned(gr_host) || !pinned(gl_host)) {
+    cudaGetLastError();  // clear a lookup error of an unregistered pointer
+    if (int r = negf_solver_run(s, stream)) return r;
+    if (int r = negf_solver_download(s, gr_host, gl_host, t_host, stream)) return r;
+    return negf_solver_check(s);
+  }
+  if (!s->copy_stream) {
+    NEGF_TRY_CUDA(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking), "run_download");
+    NEGF_TRY_CUDA(cudaEventCreateWithFlags(&s->mark_ev, cudaEventDisableTiming), "run_download");
+    NEGF_TRY_CUDA(cudaEventCreateWithFlags(&s->join_ev, cudaEventDisableTiming), "run_download");
+  }
+  // energies are device-major: one pitched copy per (device group, layer)
+  struct Group { const negf_device_s* d; size_t base, per; int count; std::vector<size_t> off; };
+  std::vector<Group> groups;
+  {
+    size_t base = 0;
+    for (size_t k = 0; k < s->devs.size(); ++k) {
+      Group g{s->devs[k], base, 0, s->dev_nE[k], {}};
+      for (int x : g.d->b) { g.off.push_back(g.per); g.per += (size_t)x * x; }
+      base += g.per * (size_t)g.count;
+      if (g.count > 0) groups.push_back(std::move(g));
+    }
+  }
+  auto at_mark = [&](int tag) -> cudaError_t {
+    const bool gl = tag >= kMarkGL;
+    const int layer = gl ? tag - kMarkGL : tag - kMarkGR;
+    char* host = static_cast<char*>(gl ? gl_host : gr_host);
+    const cplx* dev = gl ? s->gl : s->gr;
+    if (!host || !dev) return cudaSuccess;
+    cudaError_t e = cudaEventRecord(s->mark_ev, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s->copy_stream, s->mark_ev, 0);
+    for (const Group& g : groups) {
+      if (e != cudaSuccess || layer >= g.d->npl) continue;
+      const size_t o = (g.base + g.off[layer]) * sizeof(cplx), pitch = g.per * sizeof(cplx);
+      const size_t width = (size_t)g.d->b[layer] * g.d->b[layer] * sizeof(cplx);
+      e = cudaMemcpy2DAsync(host + o, pitch, reinterpret_cast<const char*>(dev) + o, pitch, width, g.count,
+                            cudaMemcpyDeviceToHost, s->copy_stream);
+    }
+    return e;
+  };
+  NEGF_TRY_CUDA(s->plan->run_marked(st, at_mark), "run_download");
+  if (t_host && s->t2)
+    NEGF_TRY_CUDA(cudaMemcpyAsync(t_host, s->t2, 2 * sizeof(double) * s->nE, cudaMemcpyDeviceToHost, st),
+                  "run_download");
+  NEGF_TRY_CUDA(cudaEventRecord(s->join_ev, s->copy_stream), "run_download");
+  NEGF_TRY_CUDA(cudaStreamWaitEvent(st, s->join_ev, 0), "run_download");
+  NEGF_TRY_CUDA(cudaStreamSynchronize(st), "run_download");
+  return negf_solver_check(s);
+}
+
 int negf_solver_outputs(negf_solver_t s, void** gr_dev, void** gl_dev, double** t_dev) {
   if (!s) return fail(NEGF_ERR_INVALID, "NULL solver");
   if (gr_dev) *gr_dev = s->gr;
@@ -1064,6 +1132,16 @@ int negf_solve(negf_device_t dev, int32_t nE, const double* energies, const negf
     int cnt = std::min(chunk, nE - e0);
     for (int e = 0; e < chunk; ++e) eb[e] = energies[e0 + std::min(e, cnt - 1)];
     if (int r = negf_solver_set_energies(s, eb.data(), stream)) return r;
+    if (!out_on_device && cnt == chunk) {
+      // host outputs of a full chunk: downloads overlap the pass
+      if (int r = negf_solver_run_download(s, gr_out ? static_cast<cplx*>(gr_out) + (size_t)e0 * per : nullptr,
+                                           gl_out ? static_cast<cplx*>(gl_out) + (size_t)e0 * per : nullptr,
+                                           t_out ? t2.data() : nullptr, stream))
+        return r;
+      if (t_out)
+        for (int e = 0; e < cnt; ++e) t_out[e0 + e] = t2[2 * e];
+      continue;
+    }
     if (int r = negf_solver_run(s, stream)) return r;
     if (gr_out)
       NEGF_TRY_CUDA(cudaMemcpyAsync(static_cast<cplx*>(gr_out) + (size_t)e0 * per, s->gr, (size_t)cnt * per * sizeof(cplx),

@@ -859,7 +859,10 @@ CCscMatrix run_bndiag_wrapper(int32_t m, int32_t n, int32_t nnz_in, int32_t* col
       return bad;
     }
   }
-  int rc = negf_ddrgf(1, npl, b.data(), Md.data(), Mu.data(), Ml.data(), 0, Gd.data(), Gu.data(), Gl.data(), nullptr);
+  // levels from the GPU cost model, as the reference's wrapper takes them
+  // from allocate_aux_data_DDRGF (libnegf_c_interface.jl:119)
+  int rc = negf_ddrgf_levels(1, npl, b.data(), Md.data(), Mu.data(), Ml.data(), 0, nullptr, Gd.data(), Gu.data(),
+                             Gl.data(), nullptr);
   if (rc != NEGF_SUCCESS) { cleanup(); return bad; }
   // output: the input's "out" band; DDRGF fills the tridiagonal, wider bands keep
   // the input blocks as the reference's bm_copy(MbmIN) + bm_copy!(MbmOUT,

@@ -107,6 +107,8 @@ PROTOTYPES = {
     "negf_solver_check": (ctypes.c_int, [ctypes.c_void_p]),
     "negf_solver_download": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, c_double_p,
                                             ctypes.c_void_p]),
+    "negf_solver_run_download": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, c_double_p,
+                                            ctypes.c_void_p]),
     "negf_solver_run_profiled": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "negf_solver_profile_read": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_double_p,
                                                 ctypes.POINTER(ctypes.c_int64), ctypes.c_int32]),

@@ -171,6 +171,13 @@ class Solver:
         check(load().negf_solver_download(self._h, gr_ptr, gl_ptr,
                                           ctypes.cast(t_ptr, _lib.c_double_p) if t_ptr else None, stream))
 
+    def run_download(self, gr_ptr, gl_ptr, t_ptr, stream=None):
+        """One pass with the downloads into host memory at the given addresses
+        (pinned; None: skip) overlapped with it, layer by layer; returns when
+        done (negf_solver_run_download)."""
+        check(load().negf_solver_run_download(self._h, gr_ptr, gl_ptr,
+                                              ctypes.cast(t_ptr, _lib.c_double_p) if t_ptr else None, stream))
+
     def outputs(self):
         gr = ctypes.c_void_p()
         gl = ctypes.c_void_p()
