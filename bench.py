@@ -249,13 +249,19 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # GPU arm
 
-def load_traffic():
-    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
-    try:
-        with open(p) as f:
-            return json.load(f)
-    except (OSError, ValueError):
+# DRAM bytes (read + write) per launch of ozaki_mma_kernel, measured by ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum over one pass of the mixed
+# solver, N = 32, b = 256, 32 energies: 469 launches, 67.0 GB); recorded in
+# profiles/ozaki_mixed_cfg2_traffic.md.  A launch's tiles scale with the number
+# of energies, so a full launch of E energies moves E / 32 times as much.
+OZ_MMA_TRAFFIC_32 = {"npl": 32, "b": 256, "energies": 32, "bytes_per_launch": 142.7e6}
+
+
+def oz_mma_traffic(npl, b, ne):
+    t = OZ_MMA_TRAFFIC_32
+    if npl != t["npl"] or b != t["b"]:
         return None
+    return t["bytes_per_launch"] * ne / t["energies"]
 
 
 def run_ours(args):
@@ -403,8 +409,10 @@ def run_ours(args):
         achieved = (k_fl / k_n) / ((k_ms / k_n) / 1000.0) / 1e12 if k_n else 0.0
         roof = {"kernel": kind, "bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                 "frac": achieved / fp64_peak if fp64_peak else None}
-    traffic = load_traffic()
-    roof["traffic"] = traffic.get("oz_mma_bytes_per_launch") if traffic else None
+    roof["traffic"] = oz_mma_traffic(args.npl, args.b, args.ne) if kind == "oz_mma" else None
+    if roof["traffic"] is not None:
+        roof["traffic_note"] = ("ncu DRAM bytes per launch at 32 energies (profiles/ozaki_mixed_cfg2_traffic.md) "
+                                "scaled by energies / 32")
     roof["share"] = k_ms / sum(v[0] for v in prof.values())
     roof["launch_ms"] = k_ms / max(1, k_n)
     whole = {"algorithmic_tflops": step_flops / ((ms / args.steps) / 1000.0) / 1e12,

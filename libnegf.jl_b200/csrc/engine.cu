@@ -173,7 +173,7 @@ void Plan::gemm_mixed(char opA, char opB, const std::vector<ZGemmProblem>& probs
     oz_pool_bytes_ = need;
   }
   std::vector<OzSplitProblem> sp(keys.size());
-  int max_rows = 0;
+  int max_rows = 0, max_kpad = 0;
   for (size_t i = 0; i < keys.size(); ++i) {
     OzSplitProblem& s = sp[i];
     s.X = keys[i].X; s.sr = keys[i].sr; s.sk = keys[i].sk;
@@ -182,12 +182,14 @@ void Plan::gemm_mixed(char opA, char opB, const std::vector<ZGemmProblem>& probs
     s.slices = reinterpret_cast<int8_t*>(oz_pool_ + off_s[i]);
     s.exps = reinterpret_cast<int*>(oz_pool_ + off_e[i]);
     max_rows = std::max(max_rows, rpad[i]);
+    max_kpad = std::max(max_kpad, kpad[i]);
   }
   Step s1;
   s1.kind = Step::OZ_SPLIT;
   s1.off = push_bytes(sp.data(), sp.size() * sizeof(OzSplitProblem));
   s1.count = (int)sp.size();
   s1.max_m = max_rows;
+  s1.max_n = max_kpad;
   steps.push_back(s1);
   std::vector<OzMmaProblem> mp;
   std::vector<int> tmap;  // 4 ints per output tile, see launch_ozaki_mma
@@ -557,7 +559,7 @@ cudaError_t Plan::launch_step(const Step& s, const unsigned char* base, cudaStre
         e = launch_ztrtri_diag(base + s.off, s.count, s.nb, s.blocked, s.max_n, s.smem, stream);
         break;
       case Step::OZ_SPLIT:
-        e = launch_ozaki_split(base + s.off, s.count, s.max_m, stream);
+        e = launch_ozaki_split(base + s.off, s.count, s.max_m, s.max_n, stream);
         break;
       case Step::OZ_MMA:
         e = launch_ozaki_mma(base + s.off, base + s.tiles_off, s.total_tiles, err_, stream);

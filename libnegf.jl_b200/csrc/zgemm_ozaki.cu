@@ -108,6 +108,131 @@ __device__ __forceinline__ uint32_t oz_gather(uint32_t w0, uint32_t w1, uint32_t
   return __byte_perm(__byte_perm(w0, w1, sel), __byte_perm(w2, w3, sel), 0x5410);
 }
 
+// Digit store of one lane: 4 consecutive k of row `grow` in each K half of
+// chunk c (row[16h + j] = element c*32 + 16h + 4kq + j, in shared memory), as
+// 3 real operands x 7 byte slices in the product kernel's core-matrix layout.
+// A warp whose lanes are (row % 8) * 4 + kq covers one 128-byte core matrix
+// per store.
+__device__ __forceinline__ void oz_store_digits(const OzSplitProblem& q, int grow, int kq, int c, const cplx* row,
+                                                double f1, double fi, double f2) {
+  const int TR = q.tile_rows;
+  const int t = grow / TR, rt = grow % TR;
+  const int kch = q.k_pad / oz::KC;
+  // left operand (128-row tiles): slice i at i * 4096, K halves 2048 apart;
+  // right operand (64-row tiles): the seven slices form one 448-row K-major
+  // matrix (row = 64 i + r), so slice i starts at i * 1024, K halves 7168 apart
+  const size_t slice = TR == oz::TM ? (size_t)TR * oz::KC : (size_t)TR * 16;
+  const size_t half = TR == oz::TM ? (size_t)TR * 16 : (size_t)oz::S * TR * 16;
+  const size_t block = (size_t)oz::S * TR * oz::KC;
+  const int ntiles = q.rows_pad / TR;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    // offset fixed-point values x + C6 of re, im and re + im of 4 consecutive
+    // k: byte 6 is the top digit, bytes 5..0 are the lower digits + 128
+    uint32_t lo[3][4], hi[3][4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const cplx v = row[16 * h + j];
+      const long long xr = oz_rint54(v.x * f1 * f2);
+      const long long xi = oz_rint54(v.y * fi * f2);
+      const long long x3[3] = {xr + oz::C6, xi + oz::C6, xr + xi + oz::C6};
+#pragma unroll
+      for (int p = 0; p < 3; ++p) {
+        lo[p][j] = (uint32_t)x3[p];
+        hi[p][j] = (uint32_t)((unsigned long long)x3[p] >> 32);
+      }
+    }
+    const size_t inrow = (size_t)h * half + (size_t)(rt >> 3) * 128 + (rt & 7) * 16 + 4 * kq;
+#pragma unroll
+    for (int p = 0; p < 3; ++p) {
+      uint8_t* base = reinterpret_cast<uint8_t*>(q.slices) + ((size_t)(p * ntiles + t) * kch + c) * block + inrow;
+#pragma unroll
+      for (int i = 0; i < oz::S; ++i) {
+        const int bi = oz::S - 1 - i;  // byte of digit slice i
+        uint32_t w = bi < 4 ? oz_gather(lo[p][0], lo[p][1], lo[p][2], lo[p][3], bi)
+                            : oz_gather(hi[p][0], hi[p][1], hi[p][2], hi[p][3], bi - 4);
+        if (i > 0) w ^= 0x80808080u;  // lower digits: byte - 128
+        *reinterpret_cast<uint32_t*>(base + i * slice) = w;
+      }
+    }
+  }
+}
+
+// Scale factors of a row with exponent e: x = rint(v 2^(54 - e)) through two
+// exact power-of-two factors (|x| <= 2^54); fi carries the conjugation.
+__device__ __forceinline__ void oz_row_factors(int e, int conj, double& f1, double& fi, double& f2) {
+  const int sh = 54 - e;
+  f1 = ldexp(1.0, sh / 2);
+  f2 = ldexp(1.0, sh - sh / 2);
+  fi = conj ? -f1 : f1;
+}
+
+// Single-read split: the CTA stages R whole rows (all k_pad columns) in shared
+// memory once, takes the row maxima there and writes the digits from there,
+// so each operand element is read from memory once.  For k_pad <= 512
+// (R = 32, 16, 8 rows for k_pad <= 128, 256, 512; <= 66 KB of staging).
+template <int R>
+__global__ void __launch_bounds__(256, 3) ozaki_split1_kernel(const OzSplitProblem* __restrict__ probs, int ldt) {
+  const OzSplitProblem q = probs[blockIdx.y];
+  const int r0 = blockIdx.x * R;
+  if (r0 >= q.rows_pad) return;
+  extern __shared__ __align__(16) unsigned char split_smem[];
+  cplx* tile = reinterpret_cast<cplx*>(split_smem);  // R rows x ldt (>= k_pad + 1)
+  __shared__ int sh_e[R];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int kp = q.k_pad;
+  // stage: zero-filled outside Y; consecutive threads take the contiguous index
+  if (q.sr == 1) {
+    for (int idx = tid; idx < R * kp; idx += 256) {
+      const int r = idx % R, k = idx / R, gr = r0 + r;
+      const bool in = gr < q.rows && k < q.cols;
+      const void* src = in ? (const void*)(q.X + (long long)gr + (long long)k * q.sk) : (const void*)probs;
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(oz_smem(tile + (size_t)r * ldt + k)),
+                   "l"(src), "r"(in ? 16 : 0)
+                   : "memory");
+    }
+  } else {
+    for (int idx = tid; idx < R * kp; idx += 256) {
+      const int k = idx % kp, r = idx / kp, gr = r0 + r;
+      const bool in = gr < q.rows && k < q.cols;
+      const void* src = in ? (const void*)(q.X + (long long)gr * q.sr + k) : (const void*)probs;
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(oz_smem(tile + (size_t)r * ldt + k)),
+                   "l"(src), "r"(in ? 16 : 0)
+                   : "memory");
+    }
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  __syncthreads();
+  // row maxima of |re| + |im| (bounds |re|, |im| and |re + im|), a warp per row
+  for (int r = warp; r < R; r += 8) {
+    double mx = 0.0;
+    for (int k = lane; k < kp; k += 32) {
+      const cplx v = tile[(size_t)r * ldt + k];
+      mx = fmax(mx, fabs(v.x) + fabs(v.y));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) {
+      int e = 0;
+      if (mx > 0.0) frexp(mx, &e);  // mx < 2^e
+      sh_e[r] = e;
+      q.exps[r0 + r] = e;
+    }
+  }
+  __syncthreads();
+  // digits: work items (group of 8 rows, 32-wide K chunk), a warp each
+  const int kch = kp / oz::KC;
+  const int kq = lane & 3;
+  for (int item = warp; item < (R / 8) * kch; item += 8) {
+    const int g = item % (R / 8), c = item / (R / 8);
+    const int rl = g * 8 + (lane >> 2);
+    double f1, fi, f2;
+    oz_row_factors(sh_e[rl], q.conj, f1, fi, f2);
+    oz_store_digits(q, r0 + rl, kq, c, tile + (size_t)rl * ldt + c * oz::KC + 4 * kq, f1, fi, f2);
+  }
+}
+
 __global__ void __launch_bounds__(256, 3) ozaki_split_kernel(const OzSplitProblem* __restrict__ probs) {
   const OzSplitProblem q = probs[blockIdx.y];
   const int r0 = blockIdx.x * oz::SPLIT_ROWS;
@@ -167,21 +292,8 @@ __global__ void __launch_bounds__(256, 3) ozaki_split_kernel(const OzSplitProble
   // store covers a 128-byte core matrix of one digit slice
   const int rl = warp * 8 + (lane >> 2);
   const int kq = lane & 3;
-  const int e = sh_e[rl];
-  // x = rint(v 2^(54 - e)), |x| <= 2^54, scaled in two exact power-of-two factors
-  const int sh = 54 - e;
-  const double f1 = ldexp(1.0, sh / 2), f2 = ldexp(1.0, sh - sh / 2);
-  const double fi = q.conj ? -f1 : f1;
-  const int TR = q.tile_rows;
-  const int grow = r0 + rl;
-  const int t = grow / TR, rt = grow % TR;
-  // left operand (128-row tiles): slice i at i * 4096, K halves 2048 apart;
-  // right operand (64-row tiles): the seven slices form one 448-row K-major
-  // matrix (row = 64 i + r), so slice i starts at i * 1024, K halves 7168 apart
-  const size_t slice = TR == oz::TM ? (size_t)TR * oz::KC : (size_t)TR * 16;
-  const size_t half = TR == oz::TM ? (size_t)TR * 16 : (size_t)oz::S * TR * 16;
-  const size_t block = (size_t)oz::S * TR * oz::KC;
-  const int ntiles = q.rows_pad / TR;
+  double f1, fi, f2;
+  oz_row_factors(sh_e[rl], q.conj, f1, fi, f2);
   // asynchronous staging of chunk c into buffer b (zero-filled outside Y)
   auto stage = [&](int c, int b) {
     const int kbase = c * oz::KC;
@@ -220,37 +332,7 @@ __global__ void __launch_bounds__(256, 3) ozaki_split_kernel(const OzSplitProble
       asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     }
     __syncthreads();
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      // offset fixed-point values x + C6 of re, im and re + im of 4 consecutive
-      // k: byte 6 is the top digit, bytes 5..0 are the lower digits + 128
-      uint32_t lo[3][4], hi[3][4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const cplx v = tile[b][rl][16 * h + 4 * kq + j];
-        const long long xr = oz_rint54(v.x * f1 * f2);
-        const long long xi = oz_rint54(v.y * fi * f2);
-        const long long x3[3] = {xr + oz::C6, xi + oz::C6, xr + xi + oz::C6};
-#pragma unroll
-        for (int p = 0; p < 3; ++p) {
-          lo[p][j] = (uint32_t)x3[p];
-          hi[p][j] = (uint32_t)((unsigned long long)x3[p] >> 32);
-        }
-      }
-      const size_t inrow = (size_t)h * half + (size_t)(rt >> 3) * 128 + (rt & 7) * 16 + 4 * kq;
-#pragma unroll
-      for (int p = 0; p < 3; ++p) {
-        uint8_t* base = reinterpret_cast<uint8_t*>(q.slices) + ((size_t)(p * ntiles + t) * kch + c) * block + inrow;
-#pragma unroll
-        for (int i = 0; i < oz::S; ++i) {
-          const int bi = oz::S - 1 - i;  // byte of digit slice i
-          uint32_t w = bi < 4 ? oz_gather(lo[p][0], lo[p][1], lo[p][2], lo[p][3], bi)
-                              : oz_gather(hi[p][0], hi[p][1], hi[p][2], hi[p][3], bi - 4);
-          if (i > 0) w ^= 0x80808080u;  // lower digits: byte - 128
-          *reinterpret_cast<uint32_t*>(base + i * slice) = w;
-        }
-      }
-    }
+    oz_store_digits(q, r0 + rl, kq, c, &tile[b][rl][4 * kq], f1, fi, f2);
     __syncthreads();
   }
 }
@@ -783,17 +865,47 @@ size_t ozaki_mma_smem_bytes() { return (size_t)oz::STAGES * oz::STAGE; }
 
 constexpr size_t kSplitSmem = 2 * oz::SPLIT_ROWS * 33 * sizeof(cplx);
 
+// single-read split: rows per CTA for a step whose largest k_pad is kp (0: two-pass kernel)
+constexpr int split1_rows(int kp) { return kp <= 128 ? 32 : kp <= 256 ? 16 : kp <= 512 ? 8 : 0; }
+constexpr size_t split1_smem(int kp) { return (size_t)split1_rows(kp) * (kp + 1) * sizeof(cplx); }
+constexpr size_t kSplit1SmemMax = 32 * 129 * sizeof(cplx);  // the largest of the three cases (66,048 B)
+static_assert(split1_smem(128) <= kSplit1SmemMax && split1_smem(256) <= kSplit1SmemMax &&
+                  split1_smem(512) <= kSplit1SmemMax,
+              "single-read split staging");
+
 cudaError_t ozaki_prepare() {
   cudaError_t e = cudaFuncSetAttribute(ozaki_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)ozaki_mma_smem_bytes());
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(ozaki_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSplitSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ozaki_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSplitSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ozaki_split1_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kSplit1SmemMax);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ozaki_split1_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kSplit1SmemMax);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ozaki_split1_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kSplit1SmemMax);
+  return e;
 }
 
-cudaError_t launch_ozaki_split(const void* probs, int nprob, int max_rows_pad, cudaStream_t st) {
+cudaError_t launch_ozaki_split(const void* probs, int nprob, int max_rows_pad, int max_k_pad, cudaStream_t st) {
   if (nprob <= 0) return cudaSuccess;
-  dim3 grid((max_rows_pad + oz::SPLIT_ROWS - 1) / oz::SPLIT_ROWS, nprob);
-  ozaki_split_kernel<<<grid, 256, kSplitSmem, st>>>(static_cast<const OzSplitProblem*>(probs));
+  const OzSplitProblem* p = static_cast<const OzSplitProblem*>(probs);
+  const int R = split1_rows(max_k_pad);
+  if (R == 0) {
+    dim3 grid((max_rows_pad + oz::SPLIT_ROWS - 1) / oz::SPLIT_ROWS, nprob);
+    ozaki_split_kernel<<<grid, 256, kSplitSmem, st>>>(p);
+    return cudaGetLastError();
+  }
+  // rows_pad is a multiple of 64, so of R; every problem's k_pad <= max_k_pad
+  dim3 grid(max_rows_pad / R, nprob);
+  const int ldt = max_k_pad + 1;
+  const size_t smem = split1_smem(max_k_pad);
+  if (R == 32) ozaki_split1_kernel<32><<<grid, 256, smem, st>>>(p, ldt);
+  else if (R == 16) ozaki_split1_kernel<16><<<grid, 256, smem, st>>>(p, ldt);
+  else ozaki_split1_kernel<8><<<grid, 256, smem, st>>>(p, ldt);
   return cudaGetLastError();
 }
 

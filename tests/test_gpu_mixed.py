@@ -22,7 +22,7 @@ def _rand(rng, m, n, scale=1.0):
 
 @pytest.mark.parametrize("ops", ["NN", "NC", "CN", "CC", "TN", "NT"])
 @pytest.mark.parametrize("shape", [(128, 64, 32), (256, 256, 256), (37, 45, 29), (130, 70, 257), (1, 1, 1),
-                                   (200, 300, 1024)])
+                                   (200, 300, 1024), (70, 90, 512), (33, 65, 130)])
 def test_mixed_gemm_vs_fp64(negf, ops, shape):
     rng = np.random.default_rng(abs(hash((ops, shape))) % 2 ** 32)
     m, n, k = shape
