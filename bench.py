@@ -257,6 +257,16 @@ def run_reference(args):
 OZ_MMA_TRAFFIC_32 = {"npl": 32, "b": 256, "energies": 32, "bytes_per_launch": 142.7e6}
 
 
+def measured_hbm_gbs():
+    """HBM copy bandwidth of this pool's B200s (MEASURED_PEAKS.json at the
+    repository root), else the pool's earlier measurement."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json)"
+    except (OSError, ValueError, KeyError):
+        return 6650.0, "fallback (6.65 TB/s)"
+
+
 def oz_mma_traffic(npl, b, ne):
     t = OZ_MMA_TRAFFIC_32
     if npl != t["npl"] or b != t["b"]:
@@ -340,11 +350,23 @@ def run_ours(args):
         stream.synchronize()
         return solver.profile_read(reset=True)
 
+    hbm_peak, hbm_src = measured_hbm_gbs()
+
     def breakdown_of(prof):
         tot = sum(v[0] for v in prof.values()) or 1.0
-        return {k: {"ms": v[0], "launches": v[2], "share": v[0] / tot,
-                    "tflops": (v[1] / (v[0] / 1000.0) / 1e12) if v[0] > 0 and v[1] > 0 else None}
-                for k, v in prof.items() if v[2]}
+        out = {}
+        for k, v in prof.items():
+            if not v[2]:
+                continue
+            e = {"ms": v[0], "launches": v[2], "share": v[0] / tot}
+            if k == "oz_split":  # HBM-bound: the library reports its algorithmic bytes
+                gbs = v[1] / (v[0] / 1000.0) / 1e9 if v[0] > 0 else None
+                e.update({"bytes_per_launch": v[1] / v[2], "gbs": gbs, "hbm_peak_gbs": hbm_peak,
+                          "hbm_frac": gbs / hbm_peak if gbs else None, "hbm_peak_source": hbm_src})
+            else:
+                e["tflops"] = (v[1] / (v[0] / 1000.0) / 1e12) if v[0] > 0 and v[1] > 0 else None
+            out[k] = e
+        return out
 
     # ---- FP64 path (reference precision): timing, breakdown, reference outputs
     solver = negf.Solver(dev, args.ne, eta=sysm.eta)

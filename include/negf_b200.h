@@ -322,7 +322,9 @@ int negf_solver_run_profiled(negf_solver_t s, void* stream);
  * copies, 4 trace, 5 LU panel, 6 LU row swaps, 7 triangular diagonal blocks,
  * 8 INT8 digit split, 9 INT8 tensor-core product (mixed precision); the
  * arrays hold NEGF_PROFILE_KINDS entries. Synchronises and writes, per
- * kind, the summed milliseconds, real flops and launch counts of the
+ * kind, the summed milliseconds, real flops (for kind 8, the digit split,
+ * its algorithmic bytes instead: operands read once, 21 digit bytes per
+ * complex element and a scale per row written) and launch counts of the
  * profiled passes since the last reset (reset != 0 starts a new
  * accumulation). */
 #define NEGF_PROFILE_KINDS 10

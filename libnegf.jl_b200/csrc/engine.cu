@@ -174,6 +174,7 @@ void Plan::gemm_mixed(char opA, char opB, const std::vector<ZGemmProblem>& probs
   }
   std::vector<OzSplitProblem> sp(keys.size());
   int max_rows = 0, max_kpad = 0;
+  double split_bytes = 0.0;
   for (size_t i = 0; i < keys.size(); ++i) {
     OzSplitProblem& s = sp[i];
     s.X = keys[i].X; s.sr = keys[i].sr; s.sk = keys[i].sk;
@@ -183,6 +184,7 @@ void Plan::gemm_mixed(char opA, char opB, const std::vector<ZGemmProblem>& probs
     s.exps = reinterpret_cast<int*>(oz_pool_ + off_e[i]);
     max_rows = std::max(max_rows, rpad[i]);
     max_kpad = std::max(max_kpad, kpad[i]);
+    split_bytes += 16.0 * keys[i].rows * keys[i].cols + 21.0 * rpad[i] * kpad[i] + 4.0 * rpad[i];
   }
   Step s1;
   s1.kind = Step::OZ_SPLIT;
@@ -190,6 +192,7 @@ void Plan::gemm_mixed(char opA, char opB, const std::vector<ZGemmProblem>& probs
   s1.count = (int)sp.size();
   s1.max_m = max_rows;
   s1.max_n = max_kpad;
+  s1.bytes = split_bytes;
   steps.push_back(s1);
   std::vector<OzMmaProblem> mp;
   std::vector<int> tmap;  // 4 ints per output tile, see launch_ozaki_mma

@@ -131,6 +131,7 @@ struct Step {
   int form = 0;          // GEMM: 0 default, 1 four real products, 2 3M
   size_t smem = 0;
   double flops = 0.0;    // real flops of the step (8mnk per complex GEMM)
+  double bytes = 0.0;    // OZ_SPLIT: algorithmic bytes (operands read once, digit slices and scales written)
 };
 
 class Plan {

@@ -973,7 +973,7 @@ int negf_solver_profile_read(negf_solver_t s, double* ms, double* flops, int64_t
       NEGF_TRY_CUDA(cudaEventElapsedTime(&x, ev[i], ev[i + 1]), "profile read");
       int k = static_cast<int>(steps[i].kind);
       t[k] += x;
-      f[k] += steps[i].flops;
+      f[k] += steps[i].kind == Step::OZ_SPLIT ? steps[i].bytes : steps[i].flops;
       n[k] += 1;
     }
   }
