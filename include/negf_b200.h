@@ -208,6 +208,15 @@ int negf_ddrgf_choose_levels(int32_t npl, int32_t b, int32_t nsys, int32_t max_l
  * max(1, nr_levels - 1) DDRGF levels from these (setup.jl:36-48).  Host only. */
 int negf_ddrgf_opt_params(int32_t npl, int32_t nr_threads, double r_lu, double r_mldiv, double damp_rgf,
                           int32_t* nr_levels, int32_t* nr_tasks, int32_t* block_size_d1, double* cost);
+/* The pieces of that search (host only): cost_rgf (src/matinvertndiag_ddrgf_
+ * utils.jl:221-247; do_full needs L <= 4), cost_ddrgf (:249-276; D1 <= 4) and
+ * bndiag_of_inv_ddrgf_check_nr_threads (:455-465: threads actually used,
+ * tasks per thread, tasks of the last thread). */
+int negf_ddrgf_cost_rgf(int32_t L, double r_lu, double r_mldiv, int32_t do_full, double* cost);
+int negf_ddrgf_cost_ddrgf(double r_lu, double r_mldiv, int32_t nr_tasks, int32_t nr_threads, int32_t block_size_d1,
+                          double* cost);
+int negf_ddrgf_check_nr_threads(int32_t nr_threads, int32_t nr_tasks, int32_t* threads, int32_t* max_per_thread,
+                                int32_t* last_per_thread);
 
 /* ------------------------------------------------------------------------
  * Batched-energy NEGF solver (the reference has no energy loop; this is the

@@ -728,6 +728,33 @@ int negf_ddrgf_choose_levels(int32_t npl, int32_t b, int32_t nsys, int32_t max_l
   return NEGF_SUCCESS;
 }
 
+int negf_ddrgf_cost_rgf(int32_t L, double r_lu, double r_mldiv, int32_t do_full, double* cost) {
+  if (L <= 0 || !cost) return fail(NEGF_ERR_INVALID, "bad arguments");
+  if (do_full && L > 4) return fail(NEGF_ERR_INVALID, "cost_rgf: a full inverse by RGF is modelled for L <= 4 only");
+  *cost = ref_cost_rgf(L, r_lu, r_mldiv, do_full != 0);
+  return NEGF_SUCCESS;
+}
+
+int negf_ddrgf_cost_ddrgf(double r_lu, double r_mldiv, int32_t nr_tasks, int32_t nr_threads, int32_t block_size_d1,
+                          double* cost) {
+  if (nr_tasks <= 0 || nr_threads <= 0 || block_size_d1 <= 0 || block_size_d1 > 4 || !cost)
+    return fail(NEGF_ERR_INVALID, "bad arguments");
+  *cost = ref_cost_ddrgf(r_lu, r_mldiv, nr_tasks, nr_threads, block_size_d1);
+  return NEGF_SUCCESS;
+}
+
+int negf_ddrgf_check_nr_threads(int32_t nr_threads, int32_t nr_tasks, int32_t* threads, int32_t* max_per_thread,
+                                int32_t* last_per_thread) {
+  if (nr_threads <= 0 || nr_tasks <= 0 || !threads || !max_per_thread || !last_per_thread)
+    return fail(NEGF_ERR_INVALID, "bad arguments");
+  const int thr = ref_check_nr_threads(nr_threads, nr_tasks);
+  const int per = (nr_tasks + thr - 1) / thr;
+  *threads = thr;
+  *max_per_thread = per;
+  *last_per_thread = nr_tasks - (thr - 1) * per;
+  return NEGF_SUCCESS;
+}
+
 int negf_ddrgf_opt_params(int32_t npl, int32_t nr_threads, double r_lu, double r_mldiv, double damp_rgf,
                           int32_t* nr_levels, int32_t* nr_tasks, int32_t* block_size_d1, double* cost) {
   if (npl <= 0 || nr_threads <= 0 || !nr_levels || !nr_tasks || !block_size_d1)

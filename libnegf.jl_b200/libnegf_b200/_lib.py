@@ -83,6 +83,12 @@ PROTOTYPES = {
                                          ctypes.c_int32, c_int32_p, c_void_pp, c_void_pp, c_void_pp, ctypes.c_void_p]),
     "negf_ddrgf_choose_levels": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                                 c_int32_p, c_int32_p]),
+    "negf_ddrgf_cost_rgf": (ctypes.c_int, [ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
+                                           c_double_p]),
+    "negf_ddrgf_cost_ddrgf": (ctypes.c_int, [ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_int32,
+                                             ctypes.c_int32, c_double_p]),
+    "negf_ddrgf_check_nr_threads": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, c_int32_p, c_int32_p,
+                                                   c_int32_p]),
     "negf_ddrgf_opt_params": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
                                              ctypes.c_double, c_int32_p, c_int32_p, c_int32_p, c_double_p]),
     "negf_device_create": (ctypes.c_int, [ctypes.c_int32, c_int32_p, c_void_pp, c_void_pp, ctypes.c_void_p,

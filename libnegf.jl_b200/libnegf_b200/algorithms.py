@@ -245,6 +245,12 @@ def Block_factorization_(A, td=None, cd=None):
     return _selinv(A, 1)
 
 
+def Block_factorization_noT_(A):
+    """Block_factorization_noT! (selected_inverse.jl:57-104): the same block LU
+    without the timing / counting wrappers."""
+    return _selinv(A, 1)
+
+
 def Block_factorization(A, td=None, cd=None):
     """selected_inverse.jl:124-128."""
     return Block_factorization_(_copy_blocks(A), td, cd)
@@ -287,6 +293,11 @@ class AuxDataDDRGF:
         self.blockSizeD1 = int(blockSizeD1)
         self.blockSizeD2 = 1
         self.nrTasks, self.lastSizeD1 = bndiag_of_inv_ddrgf_get_nr_tasks(len(self.blockSizes), self.blockSizeD1)
+        self.permVecInv, self.sizeDomains, self.permVec = [], [], []
+        if self.nrTasks >= 1 and self.blockSizeD1 < len(self.blockSizes):
+            self.permVecInv, self.sizeDomains = bndiag_of_inv_ddrgf_create_permutation_vector(
+                len(self.blockSizes), self.blockSizeD1)
+            self.permVec = bndiag_of_inv_ddrgf_transpose_permutation_vector(self.permVecInv)
         self.buffMout = None
         if level == 1:
             self.buffMout = BlockMatrix(self.blockSizes, None, {"in": 3, "out": 3}, False, False)
@@ -297,6 +308,129 @@ class AuxDataDDRGF:
         if self.nrTasks < 1:
             return []
         return [self.blockSizes[t * (self.blockSizeD1 + 1)] for t in range(self.nrTasks)]
+
+
+def bndiag_of_inv_ddrgf_create_permutation_vector(M, nrBlocksInNonPivots):
+    """bndiag_of_inv_ddrgf_create_permutation_vector (ddrgf_utils.jl:478-575),
+    0-based: permVecInv lists the old layer index of every new position --
+    first the separators ("D2", one layer at the start of each task), then
+    the interior layers ("D1") task by task -- and sizeDomains the sizes of
+    those subdomains in the same order.  M: a BlockMatrix or its layer count."""
+    npl = M if isinstance(M, int) else len(M.blockSizes)
+    d1 = int(nrBlocksInNonPivots)
+    nr, last = bndiag_of_inv_ddrgf_get_nr_tasks(npl, d1)
+    if nr < 1:
+        raise ValueError("DDRGF partition impossible for %d layers and interior size %d" % (npl, d1))
+    sizes1 = [d1] * nr
+    if last:
+        sizes1[-1] = last
+    perm_inv, size_domains = [], []
+    x = 0
+    for t in range(nr):  # region 2: the pivots
+        perm_inv.append(x)
+        size_domains.append(1)
+        x += 1 + sizes1[t]
+    x = 0
+    for t in range(nr):  # region 1: the interiors
+        x += 1
+        perm_inv.extend(range(x, x + sizes1[t]))
+        size_domains.append(sizes1[t])
+        x += sizes1[t]
+    return perm_inv, size_domains
+
+
+def bndiag_of_inv_ddrgf_transpose_permutation_vector(permVec):
+    """ddrgf_utils.jl:579-587: the inverse permutation (0-based)."""
+    inv = list(permVec)
+    for i, p in enumerate(permVec):
+        inv[p] = i
+    return inv
+
+
+def bndiag_of_inv_ddrgf_create_permuted_matrix(M, permVec):
+    """ddrgf_utils.jl:591-624: the block matrix P M P^T whose blocks are the
+    blocks of M (references, no copies): block (i, j) of the band of M lands
+    at (permVec[i], permVec[j]), and the block sizes move with it."""
+    sizes = [0] * len(M.blockSizes)
+    for i, b in enumerate(M.blockSizes):
+        sizes[permVec[i]] = b
+    Mhat = BlockMatrix(sizes, None, M.ndiag, False, M.isHermitian)
+    for (i, j) in M.pattern("out"):
+        if (i, j) in M.M:
+            Mhat.M[(permVec[i], permVec[j])] = M.M[(i, j)]
+    return Mhat
+
+
+def bndiag_of_inv_ddrgf_check_nr_threads(nrThreads, nrTasks):
+    """bndiag_of_inv_ddrgf_check_nr_threads (ddrgf_utils.jl:455-465):
+    (threads used, tasks per thread, tasks of the last thread)."""
+    t, m, l = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+    check(load().negf_ddrgf_check_nr_threads(int(nrThreads), int(nrTasks), ctypes.byref(t), ctypes.byref(m),
+                                             ctypes.byref(l)))
+    return t.value, m.value, l.value
+
+
+def cost_rgf(L, rLU, rMLDIV, doFull):
+    """cost_rgf (ddrgf_utils.jl:221-247), in units of one GEMM."""
+    c = ctypes.c_double()
+    check(load().negf_ddrgf_cost_rgf(int(L), float(rLU), float(rMLDIV), int(bool(doFull)), ctypes.byref(c)))
+    return c.value
+
+
+def cost_ddrgf(rLU, rMLDIV, nrTasks, nrThreads, blockSizeD1):
+    """cost_ddrgf (ddrgf_utils.jl:249-276), in units of one GEMM."""
+    c = ctypes.c_double()
+    check(load().negf_ddrgf_cost_ddrgf(float(rLU), float(rMLDIV), int(nrTasks), int(nrThreads), int(blockSizeD1),
+                                       ctypes.byref(c)))
+    return c.value
+
+
+def allocate_aux_data_DDRGF_single_level(M, nrBlocksInNonPivots, auxDataSeq=None, nrTasks=None):
+    """allocate_aux_data_DDRGF_single_level (ddrgf_setup.jl:63-220): one level's
+    partition, permutation and (for a BlockMatrix input) output buffer."""
+    sizes = M.blockSizes if hasattr(M, "blockSizes") else list(M)
+    a = AuxDataDDRGF(sizes, nrBlocksInNonPivots, level=1)
+    if nrTasks is not None and nrTasks != a.nrTasks:
+        raise ValueError("nrTasks %d does not match the partition (%d)" % (nrTasks, a.nrTasks))
+    return a
+
+
+def bndiag_of_inv_ddrgf_error_inv_of_T11(Min, Mout, auxData, td=None, cd=None):
+    """bndiag_of_inv_ddrgf_error_inv_of_T11 (ddrgf_utils.jl:776-824): the
+    diagnostic sqrt(sum ||(T11 T11^{-1})_{ij} - delta_ij I||_F^2 / sum_i b_i)
+    over the interior domains of auxData's partition.  The domains' full
+    inverses are recomputed by the library's RGF (buildFullInv); Mout is not
+    needed (the reference uses one of its blocks as scratch).  Unlike the
+    reference's rough version, domains of different sizes are handled."""
+    from .blockmatrix import be_gemm_
+    perm_inv, sizes = auxData.permVecInv, auxData.sizeDomains
+    nr = auxData.nrTasks
+    layers1 = perm_inv[nr:]
+    num, den, o = 0.0, 0.0, 0
+    for nd in sizes[nr:]:
+        d = layers1[o:o + nd]
+        o += nd
+        bs = [Min.blockSizes[i] for i in d]
+        full = {(a, b): dzeros(bs[a], bs[b]) for a in range(nd) for b in range(nd)}
+        Gd = [full[(a, a)] for a in range(nd)]
+        check(load().negf_rgf(1, nd, int_array(bs), ptr_array([dptr(Min.M[(i, i)]) for i in d]),
+                              ptr_array([dptr(Min.M[(d[a], d[a + 1])]) for a in range(nd - 1)]),
+                              ptr_array([dptr(Min.M[(d[a + 1], d[a])]) for a in range(nd - 1)]),
+                              ptr_array([dptr(g) for g in Gd]), None, None,
+                              ptr_array([dptr(full[(a, b)]) for a in range(nd) for b in range(nd)]),
+                              stream_handle()))
+        for a in range(nd):
+            for b in range(nd):
+                acc = dzeros(bs[a], bs[b])
+                for k in (a - 1, a, a + 1):
+                    if 0 <= k < nd:
+                        be_gemm_("N", "N", 1.0, Min.M[(d[a], d[k])], full[(k, b)], 1.0, acc)
+                x = to_host(acc)
+                if a == b:
+                    x = x - np.eye(bs[a])
+                    den += bs[a]
+                num += float(np.linalg.norm(x)) ** 2
+    return float(np.sqrt(num / den)) if den else 0.0
 
 
 def _probe_samples(M):
@@ -485,3 +619,15 @@ def bndiag_of_inv_direct_(M, blockSizes, ndiag):
     R = _csc_direct(M, blockSizes, ndiag)
     M.data, M.indices, M.indptr = R.data, R.indices, R.indptr
     M.has_sorted_indices = True
+
+
+# --------------------------------------------------------------------------
+# Input preparation (src/matloader.jl)
+
+def build_M_from_HS(H, S, Se, energVal):
+    """build_M_from_HS (matloader.jl:85-95): M = E S - H - S_e for host
+    matrices (scipy sparse or dense), as the reference's loader prepares the
+    input of the direct / C-interface paths.  The batched solver assembles
+    M(E) = (E + i eta) S - H - Sigma(E) on the device instead
+    (Device.set_overlap, Solver.set_self_energies)."""
+    return energVal * S - H - Se

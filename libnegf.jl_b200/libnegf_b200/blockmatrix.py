@@ -257,6 +257,38 @@ def be_inv_batched_(As, outs):
                                    stream_handle()))
 
 
+def be_getrf_(A, td=None, cd=None):
+    """be_getrf! (backend_cpu.jl:255-265): LU with partial pivoting in place,
+    the pivots discarded as the reference does (its callers, the selected
+    inverse, treat the factors as unpivoted).  Returns LAPACK's info (0, or
+    the first zero pivot, 1-based)."""
+    info = (ctypes.c_int32 * 1)()
+    check(load().negf_zgetrf_batched(1, int_array([A.shape[0]]), ptr_array([dptr(A)]), int_array([ld(A)]),
+                                     ptr_array([None]), info, stream_handle()))
+    return int(info[0])
+
+
+def be_trsm_(side, ul, tA, dA, alpha, A, B, td=None, cd=None):
+    """be_trsm! (backend_cpu.jl:241-253): B = alpha op(T)^{-1} B (side 'L') or
+    alpha B op(T)^{-1} (side 'R') with T the 'U' or 'L' triangle of A,
+    unit ('U') or non-unit ('N') diagonal; op = 'N' (the form the selected
+    inverse uses)."""
+    if tA != "N":
+        raise ValueError("be_trsm_: only tA = 'N' is supported (the reference's callers use 'N')")
+    a = complex(alpha)
+    al = (ctypes.c_double * 2)(a.real, a.imag)
+    check(load().negf_ztrsm_batched(side.encode(), ul.encode(), b"N", dA.encode(), al, 1, int_array([B.shape[0]]),
+                                    int_array([B.shape[1]]), ptr_array([dptr(A)]), int_array([ld(A)]),
+                                    ptr_array([dptr(B)]), int_array([ld(B)]), stream_handle()))
+
+
+def be_getri_(A, td=None, cd=None):
+    """be_getri! (backend_cpu.jl:229-239): the inverse from L\\U factors with
+    identity pivots, in place."""
+    check(load().negf_zgetri_nopiv_batched(1, int_array([A.shape[0]]), ptr_array([dptr(A)]), int_array([ld(A)]),
+                                           stream_handle()))
+
+
 def be_mul(M1, M2):
     """be_mul (backend_cpu.jl:221-223)."""
     out = dzeros(M1.shape[0], M2.shape[1])
@@ -341,6 +373,17 @@ def bm_similar(bm, filling, rng=None):
 def bm_empty(blockSizes, npl, ndiag, isArrayOrLU, isHermitian):
     """blockmatrix.jl:321-323."""
     return BlockMatrix(blockSizes, None, {"in": ndiag, "out": ndiag}, isArrayOrLU, isHermitian)
+
+
+def bm_reference_(M, B, iOffset=0, jOffset=0):
+    """bm_reference! (blockmatrix.jl:974-998, :1011-1040): the band of M
+    (ndiag["out"], diagonal and upper only when Hermitian) refers to the
+    blocks B[(i + iOffset, j + jOffset)] -- no copies, as in the reference.
+    B: a block table (dict keyed by (i, j)) or a BlockMatrix."""
+    table = B.M if isinstance(B, BlockMatrix) else B
+    for (i, j) in M.pattern("out"):
+        M.M[(i, j)] = table[(i + iOffset, j + jOffset)]
+    return M
 
 
 def bm_blocks_define_identity_(bm):

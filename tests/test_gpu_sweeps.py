@@ -393,3 +393,37 @@ def test_bndiag_of_inv_direct_rejects_bad_input(negf):
         negf.bndiag_of_inv_direct(sp.csc_matrix(D), [4, 3], {"out": 3})  # sizes do not add up
     with pytest.raises(NegfError):
         negf.bndiag_of_inv_direct(sp.csc_matrix(D), [4, 4], {"out": 4})  # even band
+
+
+def test_backend_getrf_trsm_getri_mirror(negf):
+    # be_getrf! / be_trsm! / be_getri! (backend_cpu.jl:229-265) through the mirror
+    import scipy.linalg as sla
+    rng = np.random.default_rng(12)
+    n = 70
+    A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)) + 12 * np.eye(n)
+    lu_ref, piv_ref = sla.lu_factor(A)
+    dA = negf.to_device(A)
+    assert negf.be_getrf_(dA) == 0
+    assert rel_fro(negf.to_host(dA), lu_ref) < 1e-13
+    assert np.array_equal(piv_ref, np.arange(n))  # diagonally dominant: no interchanges
+    B = rng.standard_normal((n, 30)) + 1j * rng.standard_normal((n, 30))
+    dB = negf.to_device(B)
+    negf.be_trsm_("L", "L", "N", "U", 1.0, dA, dB)
+    L = np.tril(lu_ref, -1) + np.eye(n)
+    assert rel_fro(negf.to_host(dB), np.linalg.solve(L, B)) < 1e-12
+    negf.be_getri_(dA)
+    assert rel_fro(negf.to_host(dA), np.linalg.inv(A)) < 1e-12
+
+
+@pytest.mark.parametrize("npl,b,d1", [(24, 12, 4), (19, 9, 3)])
+def test_ddrgf_error_inv_of_T11(negf, npl, b, d1):
+    # ddrgf_utils.jl:776-824: the interior domains' inverses reproduce the identity
+    M = bm_create_synthetic_random(npl, b, seed=npl + d1)
+    dM = _to_gpu_bm(negf, M)
+    aux = negf.allocate_aux_data_DDRGF(dM, blockSizeD1=d1)
+    a = aux[0]
+    assert a.permVecInv == o_dd.partition(npl, d1)[2]
+    err = negf.bndiag_of_inv_ddrgf_error_inv_of_T11(dM, a.buffMout, a)
+    assert 0.0 < err < 1e-12
+    single = negf.allocate_aux_data_DDRGF_single_level(dM, d1)
+    assert single.nrTasks == a.nrTasks and single.permVec == a.permVec
