@@ -312,3 +312,51 @@ def test_direct_oracle_band_and_outside_entries():
     T = bm_create_synthetic_random(6, 8, seed=3)
     out3, _ = direct.bndiag_of_inv_direct(bm_convert_dense(T), T.blockSizes, {"in": 3, "out": 3})
     assert rel_fro(out3, bm_convert_dense(rgf.bndiag_of_inv_rgf_local(T))) < 1e-12
+
+
+def test_golden_ddrgf_multilevel():
+    g = _gold("ddrgf_ml_npl40_b8")
+    M = bm_from_dense(g["M"], list(g["sizes"]), {"in": 3, "out": 3})
+    G, _ = ddrgf.bndiag_of_inv_ddrgf(M, [int(x) for x in g["d1"]])
+    assert rel_fro(bm_convert_dense(G), g["G"]) < 1e-14
+    exact = band_of_dense(np.linalg.inv(g["M"]), list(g["sizes"]), {"in": 3, "out": 3})
+    assert rel_fro(g["G"], exact) < ROUNDOFF64 * 2.5e5
+
+
+def test_golden_opt_params_grid():
+    # the reference's search (matinvertndiag_ddrgf_utils.jl:357-453), frozen; the
+    # library's restatement gives the same rows
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "libnegf.jl_b200"))
+    import libnegf_b200 as L
+    for row in _gold("ddrgf_opt_params_grid")["grid"]:
+        npl, thr, rlu, rml, damp, lev, cost = int(row[0]), int(row[1]), row[2], row[3], row[4], int(row[5]), row[6]
+        d1s = [int(x) for x in row[7:7 + lev]]
+        tasks = [int(x) for x in row[13:13 + lev]]
+        assert ddrgf.opt_params(npl, rlu, rml, damp, thr) == (lev, tasks, d1s, cost)
+        a = L.opt_params(npl, rlu, rml, damp, nrThreads=thr)
+        assert a[:3] == (lev, tasks, d1s) and abs(a[3] - cost) <= 1e-12 * cost
+
+
+def test_golden_direct():
+    g = _gold("direct_npl6_b8_in5_out3")
+    sizes = [int(x) for x in g["sizes"]]
+    R, inv = direct.bndiag_of_inv_direct(g["M"], sizes, {"in": 5, "out": 3})
+    assert np.array_equal(R, g["R"])
+    band = band_of_dense(np.ones_like(g["M"]), sizes, {"in": 3, "out": 3}) != 0
+    assert np.array_equal(g["R"][~band], g["M"][~band])
+    assert rel_fro(g["R"][band], np.linalg.inv(g["M"])[band]) < 1e-13
+
+
+def test_golden_overlap_sigma_of_E():
+    g = _gold("negf_overlap_sigmaE_npl5_b16")
+    Es = list(g["E"])
+    sig = {float(E): (g["sigL"][k], g["sigR"][k]) for k, E in enumerate(Es)}
+    sysm = physics.DeviceSystem(list(g["Hd"]), list(g["Hu"]), g["sigL"][0], g["sigR"][0], eta=float(g["eta"]),
+                                Sd=list(g["Sd"]), Su=list(g["Su"]), sigma_fn=lambda E: sig[float(E)])
+    for k, E in enumerate(Es):
+        r = physics.solve_energy(sysm, E)
+        for i in range(5):
+            assert rel_fro(r["GR"].M[(i, i)], g["GR"][k][i]) < 1e-14
+            assert rel_fro(1j * r["Gn"].M[(i, i)], g["GL"][k][i]) < 1e-14
+        assert abs(r["T"] - g["T"][k]) <= 1e-14 * max(1.0, abs(g["T"][k]))
