@@ -51,3 +51,59 @@ def test_halve_conserves_and_orders():
         got.setdefault(k, []).append((s, c))
     assert got == {0: [(0, 3)], 1: [(2, 1), (3, 4)], 2: [(0, 1)]}
     assert sum(c for _, _, c in a) == 4
+
+
+class _Req:
+    def __init__(self, n, per):
+        self.energies = list(range(n))
+        self.per_energy = per
+
+
+class _Queue:
+    """Stand-in for the server's state that _take_group reads and updates."""
+
+    def __init__(self, reqs, budget):
+        import collections
+        self._queue = collections.deque((r, 0, len(r.energies)) for r in reqs)
+        self.budget = budget
+
+
+def test_server_takes_fifo_groups_and_splits_the_last_request():
+    # NegfServer._take_group: the head of the queue under the budget, the last
+    # request possibly in part; the rest stays queued in order
+    from libnegf_b200.server import NegfServer
+    a, b, c = _Req(4, 10), _Req(6, 10), _Req(3, 10)
+    q = _Queue([a, b, c], budget=70)
+    g1 = NegfServer._take_group(q)
+    assert g1 == [(a, 0, 4), (b, 0, 3)]
+    assert list(q._queue) == [(b, 3, 3), (c, 0, 3)]
+    g2 = NegfServer._take_group(q)
+    assert g2 == [(b, 3, 3), (c, 0, 3)]
+    assert not q._queue
+
+
+def test_server_takes_a_single_energy_larger_than_the_budget():
+    from libnegf_b200.server import NegfServer
+    big = _Req(2, 500)
+    q = _Queue([big], budget=100)
+    assert NegfServer._take_group(q) == [(big, 0, 1)]
+    assert list(q._queue) == [(big, 1, 1)]
+    assert NegfServer._take_group(q) == [(big, 1, 1)]
+    assert not q._queue
+
+
+def test_autotune_candidates_and_signature():
+    from libnegf_b200.autotune import candidates, signature
+
+    class D:
+        def __init__(self, sizes):
+            self.sizes = sizes
+
+    small = [D([32, 64]), D([100])]
+    assert candidates(small) == [dict(gemm_form=2, gj_nb=0), dict(gemm_form=1, gj_nb=0)]
+    big = [D([256, 256])]
+    c = candidates(big)
+    assert dict(gemm_form=2, gj_nb=32) in c and dict(gemm_form=1, gj_nb=8) in c
+    # panels that do not fit shared memory are not candidates (n = 1024: nb = 32 needs 512 KiB)
+    assert all(x["gj_nb"] != 32 for x in candidates([D([1024])]))
+    assert signature(small, "fp64") == ("fp64", 128) and signature(big, "mixed") == ("mixed", 256)
