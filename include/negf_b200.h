@@ -264,9 +264,10 @@ typedef struct {
 
 /* Precision modes.  FP64: every product in FP64 on the DMMA tensor path.
  * MIXED: the Schur-complement products run on the INT8 tensor cores
- * (tcgen05) with FP64-accurate digit splitting (7 digits of 7 bits per
- * operand, exact int32 accumulation, ~1e-13 relative per product); the
- * diagonal-block inversions stay in FP64. */
+ * (tcgen05) with FP64-accurate digit splitting (per row a 54-bit fixed-point
+ * value as 7 base-256 digits, the 34 digit pairs of weight >= 2^-59 formed
+ * with exact int32 accumulation: ~1e-15 relative to |op(A)| |op(B)| per
+ * product); the diagonal-block inversions stay in FP64. */
 #define NEGF_PREC_FP64 0
 #define NEGF_PREC_MIXED 1
 
