@@ -38,6 +38,7 @@ extern "C" {
 #define NEGF_ERR_CUDA 2      /* CUDA runtime error / no device */
 #define NEGF_ERR_SINGULAR 3  /* zero pivot in a diagonal block */
 #define NEGF_ERR_NOMEM 4     /* device allocation failed */
+#define NEGF_ERR_TIMEOUT 5   /* a bounded wait ran out (negf_server_wait) */
 
 /* Message of the last failure on this thread ("" when none). */
 const char* negf_last_error(void);
@@ -390,6 +391,46 @@ int negf_bndiag_of_inv_direct(int32_t n, int32_t nnz, const int32_t* colptr, con
  * ---------------------------------------------------------------------- */
 int negf_probe_fp64_peak(double* dmma_tflops, double* dfma_tflops);
 int negf_probe_int8_peak(double* tops);
+
+/* ------------------------------------------------------------------------
+ * Request server.  The reference has no request loop (one system and one
+ * energy per call); this batches whole NEGF solves (RGF + RKD +
+ * transmission: src/matinvertndiag_rgf.jl:114-200, src/keldyshndiag.jl:
+ * 120-317) submitted from any thread of any host language.  A worker thread
+ * takes the queued requests first in, first out, as many as fit an HBM budget
+ * (negf_batch_bytes estimates; budget_gb <= 0: 80 % of free memory when a
+ * group forms) and solves them as one batch plan.  A group that fails to
+ * allocate is halved, one that fails otherwise is re-solved request by
+ * request, and a single request above the budget goes through negf_solve,
+ * which splits its energies.  opts gives eta, mu_l, mu_r, kT, precision and
+ * the schedule knobs; the want_* flags follow each request's non-NULL
+ * outputs; sigma_per_energy must be 0.
+ * ---------------------------------------------------------------------- */
+typedef struct negf_server_s* negf_server_t;
+int negf_server_create(const negf_solve_opts* opts, double budget_gb, negf_server_t* out);
+/* Upload the device (host blocks as negf_device_create; the caller may free
+ * them on return) and queue nE energies.  gr_out / gl_out (nE * sum b_i^2
+ * complex128, energy-major then layer, each block column-major) and t_out
+ * (nE doubles) are host buffers, any of them NULL, that must stay valid until
+ * the request is done.  Call with the server's device current. */
+int negf_server_submit(negf_server_t srv, int32_t npl, const int32_t* block_sizes, const void* const* Hd,
+                       const void* const* Hu, const void* sigL, const void* sigR, int32_t nE, const double* energies,
+                       void* gr_out, void* gl_out, double* t_out, int64_t* ticket);
+/* done = 1 once the request's outputs are written; the return value is then
+ * the request's status (NEGF_SUCCESS while pending). */
+int negf_server_poll(negf_server_t srv, int64_t ticket, int32_t* done);
+/* Wait at most timeout_s seconds: the request's status, or NEGF_ERR_TIMEOUT;
+ * latency_s (may be NULL) receives submission-to-completion seconds. */
+int negf_server_wait(negf_server_t srv, int64_t ticket, double timeout_s, double* latency_s);
+/* Completed requests, groups solved, and the p50 / p99 latency (seconds) of
+ * the completed requests. */
+int negf_server_stats(negf_server_t srv, int64_t* completed, int64_t* groups, double* p50_s, double* p99_s);
+/* Finish the queued requests, stop the worker, free the server. */
+int negf_server_destroy(negf_server_t srv);
+/* The worker's grouping rule (host only): requests in order, each group as
+ * many as fit budget bytes (a request above it alone); sizes receives the
+ * group sizes (room for nreq), ngroups their count. */
+int negf_server_group_sizes(int32_t nreq, const int64_t* bytes, double budget, int32_t* sizes, int32_t* ngroups);
 
 #ifdef __cplusplus
 }

@@ -16,6 +16,7 @@ NEGF_ERR_INVALID = 1
 NEGF_ERR_CUDA = 2
 NEGF_ERR_SINGULAR = 3
 NEGF_ERR_NOMEM = 4
+NEGF_ERR_TIMEOUT = 5
 NEGF_DDRGF_MAX_LEVELS = 6
 
 c_int32_p = ctypes.POINTER(ctypes.c_int32)
@@ -83,6 +84,18 @@ PROTOTYPES = {
                                          ctypes.c_int32, c_int32_p, c_void_pp, c_void_pp, c_void_pp, ctypes.c_void_p]),
     "negf_ddrgf_choose_levels": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                                 c_int32_p, c_int32_p]),
+    "negf_server_create": (ctypes.c_int, [ctypes.POINTER(SolveOpts), ctypes.c_double, ctypes.POINTER(ctypes.c_void_p)]),
+    "negf_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, c_int32_p, c_void_pp, c_void_pp,
+                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, c_double_p,
+                                          ctypes.c_void_p, ctypes.c_void_p, c_double_p,
+                                          ctypes.POINTER(ctypes.c_int64)]),
+    "negf_server_poll": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, c_int32_p]),
+    "negf_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, c_double_p]),
+    "negf_server_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64),
+                                         ctypes.POINTER(ctypes.c_int64), c_double_p, c_double_p]),
+    "negf_server_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "negf_server_group_sizes": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(ctypes.c_int64), ctypes.c_double,
+                                               c_int32_p, c_int32_p]),
     "negf_ddrgf_cost_rgf": (ctypes.c_int, [ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
                                            c_double_p]),
     "negf_ddrgf_cost_ddrgf": (ctypes.c_int, [ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_int32,

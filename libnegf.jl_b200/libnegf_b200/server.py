@@ -209,3 +209,100 @@ class NegfServer:
             r.device.close()
             self.completed.append(r)
             r._event.set()
+
+
+class NativeServer:
+    """The library's own request server (negf_server_*): the same FIFO,
+    budget-packed batching as ``NegfServer`` but run by a native worker
+    thread, so C and Julia callers get it too.  ``submit`` returns a ticket
+    object whose ``wait()`` gives (gr, gl, t) as host arrays."""
+
+    def __init__(self, budget_gb=0.0, **opts):
+        import ctypes
+        from . import _lib
+        from .negf import make_opts
+        self._lib = _lib
+        o = make_opts(**opts)
+        self._h = ctypes.c_void_p()
+        _lib.check(_lib.load().negf_server_create(ctypes.byref(o), float(budget_gb), ctypes.byref(self._h)))
+
+    class Ticket:
+        def __init__(self, server, tid, sizes, nE, keep):
+            self.server, self.id, self.sizes, self.nE, self._keep = server, tid, sizes, nE, keep
+
+        def done(self):
+            import ctypes
+            d = ctypes.c_int32()
+            self.server._lib.check(self.server._lib.load().negf_server_poll(self.server._h, self.id, ctypes.byref(d)))
+            return bool(d.value)
+
+        def wait(self, timeout=600.0):
+            """Block until done (at most ``timeout`` seconds); returns (gr, gl, t)
+            with gr[e][i] the diagonal block i of energy e."""
+            import ctypes
+            lat = ctypes.c_double()
+            self.server._lib.check(self.server._lib.load().negf_server_wait(self.server._h, self.id, float(timeout),
+                                                                            ctypes.byref(lat)))
+            self.latency = lat.value
+            gr, gl, t = self._keep[:3]
+
+            def split(flat):
+                if flat is None:
+                    return None
+                out, o = [], 0
+                for _ in range(self.nE):
+                    row = []
+                    for b in self.sizes:
+                        row.append(flat[o:o + b * b].reshape(b, b, order="F"))
+                        o += b * b
+                    out.append(row)
+                return out
+            return split(gr), split(gl), t
+
+    def submit(self, Hd, Hu, sigL, sigR, energies, want_blocks=True):
+        import ctypes
+        from .negf import _host_blocks
+        E = np.ascontiguousarray(np.asarray(energies, dtype=np.float64))
+        sizes = [int(h.shape[0]) for h in Hd]
+        per = sum(b * b for b in sizes)
+        gr = np.empty(len(E) * per, dtype=np.complex128) if want_blocks else None
+        gl = np.empty(len(E) * per, dtype=np.complex128) if want_blocks else None
+        t = np.empty(len(E), dtype=np.float64)
+        kd, pd = _host_blocks(Hd)
+        ku, pu = _host_blocks(Hu)
+        sl = np.asfortranarray(np.asarray(sigL, dtype=np.complex128))
+        sr = np.asfortranarray(np.asarray(sigR, dtype=np.complex128))
+        lib, L = self._lib, self._lib.load()
+        tid = ctypes.c_int64()
+        lib.check(L.negf_server_submit(self._h, len(sizes), lib.int_array(sizes), lib.ptr_array(pd),
+                                       lib.ptr_array(pu), sl.ctypes.data, sr.ctypes.data, len(E),
+                                       E.ctypes.data_as(lib.c_double_p), gr.ctypes.data if gr is not None else None,
+                                       gl.ctypes.data if gl is not None else None,
+                                       t.ctypes.data_as(lib.c_double_p), ctypes.byref(tid)))
+        # the output buffers (and energies) stay referenced until the ticket is dropped
+        return NativeServer.Ticket(self, tid.value, sizes, len(E), (gr, gl, t, E))
+
+    def stats(self):
+        import ctypes
+        c, g = ctypes.c_int64(), ctypes.c_int64()
+        p50, p99 = ctypes.c_double(), ctypes.c_double()
+        self._lib.check(self._lib.load().negf_server_stats(self._h, ctypes.byref(c), ctypes.byref(g),
+                                                           ctypes.byref(p50), ctypes.byref(p99)))
+        return {"requests": c.value, "groups": g.value, "p50_s": p50.value, "p99_s": p99.value}
+
+    def close(self):
+        if self._h:
+            self._lib.load().negf_server_destroy(self._h)
+            self._h = None
+
+
+def group_sizes(bytes_per_request, budget):
+    """The native worker's grouping rule (negf_server_group_sizes)."""
+    import ctypes
+    from . import _lib
+    n = len(bytes_per_request)
+    b = (ctypes.c_int64 * max(1, n))(*[int(x) for x in bytes_per_request])
+    sizes = (ctypes.c_int32 * max(1, n))()
+    ng = ctypes.c_int32()
+    _lib.check(_lib.load().negf_server_group_sizes(n, b, float(budget), sizes, ctypes.byref(ng)))
+    return list(sizes[:ng.value])

@@ -107,3 +107,23 @@ def test_autotune_candidates_and_signature():
     # panels that do not fit shared memory are not candidates (n = 1024: nb = 32 needs 512 KiB)
     assert all(x["gj_nb"] != 32 for x in candidates([D([1024])]))
     assert signature(small, "fp64") == ("fp64", 128) and signature(big, "mixed") == ("mixed", 256)
+
+
+def test_native_server_grouping_rule():
+    # negf_server_group_sizes: the native worker's FIFO grouping under a budget
+    from libnegf_b200.server import group_sizes
+    assert group_sizes([10, 20, 30, 100, 5, 5], 50) == [2, 1, 1, 2]
+    assert group_sizes([], 10) == []
+    assert group_sizes([200], 10) == [1]
+    assert group_sizes([5] * 7, 15) == [3, 3, 1]
+    assert sum(group_sizes(list(range(1, 30)), 40)) == 29
+
+
+def test_native_server_needs_a_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    from libnegf_b200 import NegfError
+    from libnegf_b200.server import NativeServer
+    with pytest.raises(NegfError):
+        NativeServer()

@@ -66,3 +66,31 @@ def test_server_requests_of_different_sizes(negf):
         assert stats["requests"] == 3 and stats["p99_s"] >= stats["p50_s"] > 0
     finally:
         srv.close()
+
+
+@pytest.mark.parametrize("budget_gb", [0.0, 1e-6])
+def test_native_server_matches_oracle(negf, budget_gb):
+    # negf_server_*: three requests of different shapes from the host; with the
+    # default budget they share one batch plan, with a tiny one each request is
+    # solved alone (through negf_solve)
+    from libnegf_b200.server import NativeServer
+    systems = _systems([(4, 32, 11), (6, 24, 12), (3, 48, 13)])
+    energies = [np.linspace(-0.6, 0.5, n) for n in (3, 4, 2)]
+    srv = NativeServer(budget_gb=budget_gb, eta=systems[0].eta)
+    try:
+        tickets = [srv.submit(s.Hd, s.Hu, s.sigL, s.sigR, E) for s, E in zip(systems, energies)]
+        for s, E, tk in zip(systems, energies, tickets):
+            gr, gl, t = tk.wait(timeout=120.0)
+            assert tk.latency > 0.0
+            for e, En in enumerate(E):
+                r = o_phys.solve_energy(s, En)
+                for i in range(s.npl):
+                    assert rel_fro(gr[e][i], r["GR"].M[(i, i)]) < 1e-12
+                    assert rel_fro(gl[e][i], 1j * r["Gn"].M[(i, i)]) < 1e-12
+                assert abs(t[e] - r["T"]) <= 1e-12 * max(1.0, abs(r["T"]))
+        st = srv.stats()
+        assert st["requests"] == 3 and st["p99_s"] >= st["p50_s"] > 0.0
+        # requests submitted while the worker is busy join one group; the first may go alone
+        assert st["groups"] == 3 if budget_gb > 0.0 else 1 <= st["groups"] <= 3
+    finally:
+        srv.close()
