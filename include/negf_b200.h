@@ -404,7 +404,8 @@ int negf_probe_int8_peak(double* tops);
  * request, and a single request above the budget goes through negf_solve,
  * which splits its energies.  opts gives eta, mu_l, mu_r, kT, precision and
  * the schedule knobs; the want_* flags follow each request's non-NULL
- * outputs; sigma_per_energy must be 0.
+ * outputs; sigma_per_energy must be 0.  The server keeps a few bytes per
+ * ticket (status, latency) until it is destroyed.
  * ---------------------------------------------------------------------- */
 typedef struct negf_server_s* negf_server_t;
 int negf_server_create(const negf_solve_opts* opts, double budget_gb, negf_server_t* out);
