@@ -93,7 +93,7 @@ int negf_zinv_batched(int32_t nprob, const int32_t* n, void* const* A, const int
  * negf_zinv_batched; all scratch (block copies, rank-nb update buffers,
  * pivots, flags, launch descriptors) lives in one fixed 64 MiB __device__
  * array that every GPU loading the library keeps until the process exits.
- * A request whose scratch exceeds 64 MiB (about 60 blocks of 256 or 15 of 512
+ * A request whose scratch exceeds 64 MiB (more than 51 blocks of 256 or 15 of 512
  * per call) is rejected with NEGF_ERR_INVALID.  The first call on a device
  * looks up the array's address and sets kernel attributes: make it before
  * any stream capture.  All calls share the array, so calls that overlap on

@@ -132,7 +132,7 @@ extern "C" int negf_zinv_batched_noalloc(int32_t nprob, const int32_t* n, void* 
     char buf[256];
     std::snprintf(buf, sizeof buf,
                   "negf_zinv_batched_noalloc: the request needs %zu bytes of scratch, more than the fixed %zu "
-                  "(for example at most 60 blocks of 256 or 15 blocks of 512 per call)",
+                  "(at most 51 blocks of 256 or 15 blocks of 512 per call)",
                   L.off, kNoAllocScratchBytes);
     return fail(NEGF_ERR_INVALID, buf);
   }

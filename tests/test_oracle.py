@@ -360,3 +360,38 @@ def test_golden_overlap_sigma_of_E():
             assert rel_fro(r["GR"].M[(i, i)], g["GR"][k][i]) < 1e-14
             assert rel_fro(1j * r["Gn"].M[(i, i)], g["GL"][k][i]) < 1e-14
         assert abs(r["T"] - g["T"][k]) <= 1e-14 * max(1.0, abs(g["T"][k]))
+
+
+# ---------------------------------------------------------------------------
+# the double-double truth (oracle/ddtruth.py) used by the configuration parity tests
+
+def test_ddtruth_products_and_inverse_are_exact_to_dd_level():
+    from oracle import ddtruth as dd
+    rng = np.random.default_rng(7)
+    A = dd.DD(rng.standard_normal((48, 48)) + 1j * rng.standard_normal((48, 48)))
+    X = dd.inv(A)
+    R = dd.sub(dd.identity(48), dd.matmul(A, X))
+    assert np.abs(R.hi).max() < 1e-28
+    # a product of exactly representable integer matrices is exact
+    B = dd.DD(np.round(64 * rng.standard_normal((48, 20))) + 1j * np.round(64 * rng.standard_normal((48, 20))))
+    C = dd.DD(np.round(64 * rng.standard_normal((20, 30))) + 0j)
+    P = dd.matmul(B, C)
+    assert np.array_equal(P.hi, B.hi @ C.hi) and not np.any(P.lo)
+
+
+@pytest.mark.parametrize("npl,b", [(5, 12), (1, 9), (3, 20)])
+def test_ddtruth_vs_dense_and_oracle(npl, b):
+    from oracle import ddtruth as dd
+    sysm = physics.physics_system(npl, b, seed=npl + b)
+    E = 0.21
+    t = dd.physics_truth(sysm, E)
+    r = physics.solve_energy(sysm, E)
+    D = bm_convert_dense(sysm.M_of_E(E))
+    Gd = np.linalg.inv(D)
+    o = 0
+    for i, bi in enumerate(sysm.sizes):
+        assert rel_fro(t["GR"][i], Gd[o:o + bi, o:o + bi]) < 1e-13
+        assert rel_fro(t["GR"][i], r["GR"].M[(i, i)]) < 1e-13
+        assert rel_fro(t["GL"][i], 1j * r["Gn"].M[(i, i)]) < 1e-13
+        o += bi
+    assert abs(t["T"] - r["T"]) < 1e-12 * max(1.0, abs(r["T"]))

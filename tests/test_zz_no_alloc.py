@@ -52,6 +52,28 @@ def test_noalloc_matches_allocating_entry_point_twice(negf, sizes):
             assert rel_fro(x, np.linalg.inv(a)) < TOL * max(1.0, np.linalg.cond(a) / 1e2)
 
 
+@pytest.mark.parametrize("b,limit", [(256, 51), (512, 15)])
+def test_noalloc_documented_limit(negf, b, limit):
+    """The header's limit: `limit` blocks of size b run and match the allocating
+    entry point; one block more is refused."""
+    from libnegf_b200._lib import int_array, ptr_array, check, NEGF_ERR_INVALID
+    lib = negf.load()
+    rng = np.random.default_rng(b)
+    base = [rng.standard_normal((b, b)) + 1j * rng.standard_normal((b, b)) + 4.0 * np.sqrt(b) * np.eye(b)
+            for _ in range(3)]
+    mats = [base[i % 3] for i in range(limit)]
+    ref, na = _inv_both(negf, mats)
+    for r, x in zip(ref, na):
+        assert rel_fro(x, r) < TOL
+    n = [b] * (limit + 1)
+    dA = negf.to_device(base[0])
+    dO = [negf.dzeros(b, b) for _ in n]
+    rc = lib.negf_zinv_batched_noalloc(len(n), int_array(n), ptr_array([dA.data_ptr()] * len(n)), int_array(n),
+                                       ptr_array([o.data_ptr() for o in dO]), int_array(n), None, None)
+    assert rc == NEGF_ERR_INVALID
+    assert b"scratch" in lib.negf_last_error()
+
+
 def test_noalloc_rejects_oversized_request(negf):
     from libnegf_b200._lib import int_array, ptr_array, NEGF_ERR_INVALID
     lib = negf.load()
