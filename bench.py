@@ -52,16 +52,18 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--npl", type=int, default=32)
-    ap.add_argument("--b", type=int, default=256)
-    ap.add_argument("--ne", type=int, default=256)
+    ap.add_argument("--npl", type=int, default=None, help="layers (cfg2: 32, cfg3: 64)")
+    ap.add_argument("--b", type=int, default=None, help="block size (cfg2: 256, cfg3: 512)")
+    ap.add_argument("--ne", type=int, default=None, help="energies (cfg2: 256, cfg3: 128)")
     ap.add_argument("--cpu-budget-s", type=float, default=12.0, help="time budget of each CPU baseline mode")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg4", "cfg5"],
+    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg3", "cfg4", "cfg5"],
                     help="cfg2 (default, the headline line); cfg4: a bounded sample of the uneven batch (systems "
                          "of N in U{8..96}, b in {32..384}, 16 energies each); cfg5: a bounded sample of the "
                          "Poisson-arrival request stream through the server (p50/p99 latency)")
+    ap.add_argument("--chunk", type=int, default=8, help="cfg3: energies per device-resident chunk")
+    ap.add_argument("--methods", default="ddrgf,selinv,rgf", help="cfg3: methods to time (ddrgf, selinv, rgf)")
     ap.add_argument("--systems", type=int, default=96, help="cfg4: number of systems in the sample")
     ap.add_argument("--requests", type=int, default=16, help="cfg5: number of requests in the sample")
     ap.add_argument("--rate", type=float, default=2.0, help="cfg5: mean arrival rate, requests/s")
@@ -69,7 +71,12 @@ def parse():
     ap.add_argument("--launch-list", action="store_true",
                     help="only two launch-by-launch passes of the mixed solver (for an ncu launch list: skip the "
                          "first pass's launches, capture the second's); prints no bench line")
-    return ap.parse_args()
+    a = ap.parse_args()
+    dflt = {"cfg3": (64, 512, 128)}.get(a.workload, (32, 256, 256))
+    a.npl = a.npl if a.npl is not None else dflt[0]
+    a.b = a.b if a.b is not None else dflt[1]
+    a.ne = a.ne if a.ne is not None else dflt[2]
+    return a
 
 
 def shard_energies(ne_per_rank, world, rank, lo=-1.0, hi=1.0):
@@ -415,11 +422,11 @@ def run_ours(args):
     del refs, t_ref
 
     # dominant kernel: the INT8 product kernel; algorithmic work per launch =
-    # 3 real products x 34 digit pairs x 2mnk int8 ops per complex product
-    # (8mnk complex flops) = 25.5 x its complex flops
+    # 3 real products x 28 digit pairs x 2mnk int8 ops per complex product
+    # (8mnk complex flops) = 21 x its complex flops
     kind = max(prof, key=lambda k: prof[k][0])
     k_ms, k_fl, k_n = prof[kind]
-    ops_per_cflop = 3 * 34 * 2 / 8.0
+    ops_per_cflop = 3 * 28 * 2 / 8.0
     if kind == "oz_mma":
         achieved = (k_fl * ops_per_cflop / k_n) / ((k_ms / k_n) / 1000.0) / 1e12
         roof = {"kernel": "ozaki_mma_kernel (tcgen05.mma kind::i8, TMEM accumulators)", "bound": "tensor",
@@ -489,7 +496,7 @@ def run_ours(args):
                 "roofline": roof, "kernels": breakdown_of(prof), "whole_step": whole, "clocks": clk.summary(),
                 "gpu_launches": int(stats["launches"]) * args.steps,
                 "e2e": e2e, "cpu_baseline": cpu, "fp64_path": fp64,
-                "method": "3M complex products of 7-digit base-256 int8 splits of 54-bit fixed-point rows (34 digit "
+                "method": "3M complex products of 7-digit base-256 int8 splits of 54-bit fixed-point rows (28 digit "
                           "pairs per real product) on tcgen05.mma kind::i8 with exact int32 TMEM accumulation; "
                           "FP64 Gauss-Jordan inversions"}
         print(json.dumps(line), flush=True)
@@ -498,6 +505,101 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_cfg3(args):
+    """Selected inverse of M(E) for many energies: N = 64 layers of b = 512
+    (--npl / --b), 128 energies (--ne) uniform in [-1, 1], the same H / Sigma
+    generator (seed 0), by DDRGF with four partitions (interior size 15:
+    separators at layers 0, 16, 32, 48), by the block selected inverse
+    (Block_factorization! + Block_inverse!, lu(NoPivot()) diagonal blocks) and
+    by sequential RGF, each in FP64 and in the mixed precision mode.  A step is
+    one pass over all energies through negf_device_selected_inverse with
+    device outputs, in chunks of --chunk energies (planning and workspace
+    allocation inside the timed region); accuracy: the mixed outputs against
+    the FP64 GPU outputs on the first chunk and against the oracle's sequential
+    RGF on one energy."""
+    import ctypes
+    import torch
+    import libnegf_b200 as negf
+    from libnegf_b200 import _lib
+    from oracle import physics, rgf as o_rgf
+    npl, b, ne, chunk = args.npl, args.b, args.ne, args.chunk
+    sysm = physics.physics_system(npl, b, seed=0)
+    dev = negf.Device(sysm.Hd, sysm.Hu, sysm.sigL, sysm.sigR)
+    E = np.linspace(-1.0, 1.0, ne)
+    sd, su = npl * b * b, (npl - 1) * b * b
+    gd = torch.empty(2 * chunk * sd, dtype=torch.float64, device="cuda")
+    gu = torch.empty(2 * chunk * su, dtype=torch.float64, device="cuda")
+    gl = torch.empty(2 * chunk * su, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.Stream()
+    lib = negf.load()
+    d1 = max(1, (npl - 4) // 4)  # four partitions: 4 (d1 + 1) = npl
+    methods = {"ddrgf": (_lib.NEGF_METHOD_DDRGF, [d1]), "selinv": (_lib.NEGF_METHOD_SELINV, []),
+               "rgf": (_lib.NEGF_METHOD_RGF, [])}
+
+    def one_chunk(method, precision, e0):
+        m, lv = methods[method]
+        cnt = min(chunk, ne - e0)
+        o = negf.make_opts(sysm.eta, max_chunk=cnt, precision=precision)
+        Ec = np.ascontiguousarray(E[e0:e0 + cnt])
+        _lib.check(lib.negf_device_selected_inverse(
+            dev.handle, cnt, Ec.ctypes.data_as(_lib.c_double_p), ctypes.byref(o), m, len(lv),
+            _lib.int_array(lv) if lv else None, gd.data_ptr(), gu.data_ptr(), gl.data_ptr(), 1,
+            ctypes.c_void_p(stream.cuda_stream)))
+
+    def host_blocks(t, n_blocks, e):
+        z = t.view(-1, 2)[e * n_blocks * b * b:(e + 1) * n_blocks * b * b].cpu().numpy()
+        z = z[:, 0] + 1j * z[:, 1]
+        return [z[i * b * b:(i + 1) * b * b].reshape(b, b, order="F") for i in range(n_blocks)]
+
+    res = {}
+    ref_chunk = {}
+    clk = ClockSampler(torch.cuda.current_device())
+    with clk:
+        for method in [x for x in args.methods.split(",") if x]:
+            for precision in ("fp64", "mixed"):
+                one_chunk(method, precision, 0)  # warm-up (kernel attributes, first allocations)
+                times = []
+                for _ in range(args.steps):
+                    t0 = time.perf_counter()
+                    for e0 in range(0, ne, chunk):
+                        one_chunk(method, precision, e0)
+                    times.append(time.perf_counter() - t0)
+                t = float(np.median(times))
+                # accuracy on the first chunk: mixed vs the FP64 GPU path, both vs the oracle on energy 0
+                one_chunk(method, precision, 0)
+                outs = [host_blocks(gd, npl, 0), host_blocks(gu, npl - 1, 0), host_blocks(gl, npl - 1, 0)]
+                ref_chunk[(method, precision)] = outs
+                res[(method, precision)] = {"pts_per_s": ne / t, "s_per_step": t}
+    # the oracle's sequential RGF on energy 0 (the CPU restatement of bndiag_of_inv_rgf_local!)
+    G = o_rgf.bndiag_of_inv_rgf_local(sysm.M_of_E(E[0]))
+    ref = [[G.M[(i, i)] for i in range(npl)], [G.M[(i, i + 1)] for i in range(npl - 1)],
+           [G.M[(i + 1, i)] for i in range(npl - 1)]]
+
+    def err(a, r):
+        return max(max(np.linalg.norm(x - y) / np.linalg.norm(y) for x, y in zip(pa, pr)) for pa, pr in zip(a, r))
+
+    lines = {}
+    for (method, precision), v in res.items():
+        acc = {"vs_oracle_rgf_energy0": err(ref_chunk[(method, precision)], ref)}
+        if precision == "mixed" and (method, "fp64") in ref_chunk:
+            acc["vs_fp64_gpu_energy0"] = err(ref_chunk[(method, precision)], ref_chunk[(method, "fp64")])
+        v["accuracy"] = acc
+        lines.setdefault(method, {})[precision] = v
+    for method, d in lines.items():
+        if "fp64" in d and "mixed" in d:
+            d["speedup_mixed_vs_fp64"] = d["mixed"]["pts_per_s"] / d["fp64"]["pts_per_s"]
+    head = lines.get("ddrgf", next(iter(lines.values())))
+    print(json.dumps({"metric": "energy pts/s (selected inverse of M(E): DDRGF, block selected inverse, RGF)",
+                      "value": head["mixed"]["pts_per_s"] if "mixed" in head else None, "unit": UNIT,
+                      "n_gpus": 1, "steps": args.steps, "dtype": "int8 products / f64",
+                      "data": "synthetic (seeded numpy generator of the config)",
+                      "config": {"workload": "batched selected inverse + DDRGF, N=%d layers x b=%d, %d energies, "
+                                             "four partitions (interior size %d)" % (npl, b, ne, d1),
+                                 "chunk": chunk, "headline": "ddrgf, mixed"},
+                      "methods": lines, "clocks": clk.summary()}), flush=True)
+    dev.close()
 
 
 def run_cfg4(args):
@@ -588,6 +690,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "cfg3":
+        run_cfg3(args)
     elif args.workload == "cfg4":
         run_cfg4(args)
     elif args.workload == "cfg5":

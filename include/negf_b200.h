@@ -77,6 +77,11 @@ int negf_zgemm_batched_mixed(char opA, char opB, int32_t nprob, const negf_zgemm
 int negf_zcopy_batched(char op, int32_t nprob, const int32_t* m, const int32_t* n, void* const* A,
                        const int32_t* lda, void* const* C, const int32_t* ldc, void* stream);
 
+/* Batched be_fill! (src/backend_cpu.jl:86-88): every entry of C[i]
+ * (m[i] x n[i]) set to value (re, im). */
+int negf_zfill_batched(int32_t nprob, const int32_t* m, const int32_t* n, void* const* C, const int32_t* ldc,
+                       const double* value, void* stream);
+
 /* Batched inversion Ainv[i] = A[i]^{-1} by blocked Gauss-Jordan with partial
  * pivoting; replaces be_lu! + be_mldivide!(identity) / be_inv_from_lu!
  * (src/backend_cpu.jl:147-206).  A[i] is not modified.  n[i] <= 1024.
@@ -159,6 +164,22 @@ int negf_general_rgf(int32_t nsys, int32_t npl, int32_t ndiag, const int32_t* bl
  * 3 = both.  In place. */
 int negf_selected_inverse(int32_t npl, int32_t b, void* const* Ab, const uint8_t* fill, int32_t mode, void* stream);
 
+/* negf_selected_inverse over nsys systems at once (Block_factorization! /
+ * Block_inverse!, src/selected_inverse.jl:9-206, one call per system in the
+ * reference): Ab holds nsys*npl*npl dptrs (system-major, then row-major block
+ * index); every system has system 0's block pattern; each step is one batched
+ * launch over all systems.  pivoting = 1 factors each diagonal block as the
+ * reference's be_getrf! does (LAPACK getrf, src/backend_cpu.jl:255-265, whose
+ * row interchanges the reference then discards, so it is exact only for
+ * blocks that need none); pivoting = 0 is lu(NoPivot()), the factorisation
+ * selected_inverse.jl:17 names, exact for any blocks with non-zero leading
+ * minors.  precision NEGF_PREC_MIXED runs the block products (the triangular
+ * solves with the explicit factor inverses, the Schur updates and the
+ * Block_inverse! products) on the INT8 tensor cores with FP64-grade digit
+ * splitting; the diagonal-block LU and triangular inverses stay FP64. */
+int negf_selected_inverse_batched(int32_t nsys, int32_t npl, int32_t b, void* const* Ab, const uint8_t* fill,
+                                  int32_t mode, int32_t pivoting, int32_t precision, void* stream);
+
 /* Domain-decomposed RGF: bndiag_of_inv_ddrgf! (src/matinvertndiag_ddrgf_core.jl:
  * 719-758) with one level and the reference's partition (separators of one
  * layer at t*(D1+1), src/matinvertndiag_ddrgf_utils.jl:278-312, :478-575);
@@ -186,6 +207,13 @@ int negf_ddrgf(int32_t nsys, int32_t npl, const int32_t* block_sizes, void* cons
 int negf_ddrgf_levels(int32_t nsys, int32_t npl, const int32_t* block_sizes, void* const* Md, void* const* Mu,
                       void* const* Ml, int32_t nlevels, const int32_t* block_size_d1, void* const* Gd,
                       void* const* Gu, void* const* Gl, void* stream);
+/* negf_ddrgf_levels with a precision mode: NEGF_PREC_MIXED runs every block
+ * product of the sweep (domain RGF and full inverses, Schur complement, the
+ * 12 / 21 / 11 assembly) on the INT8 tensor cores with FP64-grade digit
+ * splitting; the diagonal-block inversions stay FP64. */
+int negf_ddrgf_levels_ex(int32_t nsys, int32_t npl, const int32_t* block_sizes, void* const* Md, void* const* Mu,
+                         void* const* Ml, int32_t nlevels, const int32_t* block_size_d1, void* const* Gd,
+                         void* const* Gu, void* const* Gl, int32_t precision, void* stream);
 
 /* The reference's partition helper (src/matinvertndiag_ddrgf_utils.jl:
  * 278-312): writes nr_tasks (-1: impossible) and the last interior size. */
@@ -266,7 +294,7 @@ typedef struct {
 /* Precision modes.  FP64: every product in FP64 on the DMMA tensor path.
  * MIXED: the Schur-complement products run on the INT8 tensor cores
  * (tcgen05) with FP64-accurate digit splitting (per row a 54-bit fixed-point
- * value as 7 base-256 digits, the 34 digit pairs of weight >= 2^-59 formed
+ * value as 7 base-256 digits, the 28 digit pairs of weight >= 2^-60 formed
  * with exact int32 accumulation: ~1e-15 relative to |op(A)| |op(B)| per
  * product); the diagonal-block inversions stay in FP64. */
 #define NEGF_PREC_FP64 0
@@ -278,6 +306,31 @@ typedef struct {
  * out_on_device != 0.  NULL outputs are skipped. */
 int negf_solve(negf_device_t dev, int32_t nE, const double* energies, const negf_solve_opts* opts, void* gr_out,
                void* gl_out, double* t_out, int32_t out_on_device, void* stream);
+
+/* Selected inverse of M(E) = (E + i eta) S - H - Sigma for nE energies: the
+ * blocks (i,i), (i,i+1), (i+1,i) of G^R(E) = M(E)^{-1}, every recursion step
+ * one batched launch over all energies of a device-resident chunk.  This is
+ * the batched form of one reference call per energy point of
+ *   method 0: bndiag_of_inv_rgf_local! (src/matinvertndiag_rgf.jl:114-200);
+ *   method 1: bndiag_of_inv_ddrgf! (src/matinvertndiag_ddrgf_core.jl:719-758)
+ *             with nlevels interior sizes block_size_d1 (nlevels = 0: the
+ *             library's GPU cost model chooses);
+ *   method 2: Block_factorization! + Block_inverse! (src/selected_inverse.jl:
+ *             9-206) with lu(NoPivot()) diagonal factorisations (one block
+ *             size).
+ * opts: eta, precision (NEGF_PREC_MIXED: block products on the INT8 tensor
+ * cores with FP64-grade digit splitting, inversions / LU in FP64), max_chunk /
+ * hbm_budget_gb (energies per chunk), gemm_form, gj_nb; sigma_per_energy must
+ * be 0.  Outputs (NULL: skipped), energy-major: gd_out nE * sum b_i^2; gu_out
+ * (blocks (i,i+1), b_i x b_{i+1}) and gl_out (blocks (i+1,i), b_{i+1} x b_i)
+ * nE * sum b_i b_{i+1}; column-major blocks.  HOST pointers unless
+ * out_on_device != 0.  Synchronises the stream. */
+int negf_device_selected_inverse(negf_device_t dev, int32_t nE, const double* energies, const negf_solve_opts* opts,
+                                 int32_t method, int32_t nlevels, const int32_t* block_size_d1, void* gd_out,
+                                 void* gu_out, void* gl_out, int32_t out_on_device, void* stream);
+#define NEGF_METHOD_RGF 0
+#define NEGF_METHOD_DDRGF 1
+#define NEGF_METHOD_SELINV 2
 
 /* Resident-plan form of negf_solve for repeated solves of a fixed number of
  * energies with inputs and outputs kept in device memory. */

@@ -321,7 +321,7 @@ void Plan::getrf(const std::vector<LuSpec>& specs) {
     if (s.n <= 0) continue;
     ZLuProblem p;
     p.A = s.A; p.ipiv = s.ipiv; p.Linv = s.Linv; p.T = s.T; p.info = s.info;
-    p.n = s.n; p.ld = s.ld; p.pad0_ = p.pad1_ = 0;
+    p.n = s.n; p.ld = s.ld; p.nopiv = s.nopiv ? 1 : 0; p.pad_ = 0;
     v.push_back(p);
     max_n = std::max(max_n, s.n);
   }

@@ -77,6 +77,7 @@ struct LuSpec {
   cplx* Linv;  // scratch nb x nb
   cplx* T;     // scratch nb x n
   int* info;
+  bool nopiv = false;  // lu(A, NoPivot()): no row interchanges
 };
 // Triangular inverse request: X = inverse of the upper (non-unit) or unit
 // lower triangle of the packed factors A; T is scratch n x nb.
@@ -269,6 +270,26 @@ struct HermBlocks {
 // (no later step of the pass reads or writes it) for every system.
 void build_rkd(Plan& plan, const std::vector<TriSystem>& sys, std::vector<RgfWork>& work,
                std::vector<HermBlocks>& S, const std::function<void(int)>& on_final = {});
+
+// Block selected inverse (selinv.cu): Block_factorization! and / or
+// Block_inverse! (src/selected_inverse.jl:9-206, mode bit 1 / bit 2) in place
+// on each system's npl x npl block table (row-major, null = unassigned; all
+// systems share system 0's pattern; blocks b x b, ld b).  info points to npl
+// ints per system (zero pivot of block i).  nopiv: lu(NoPivot()) for the
+// diagonal blocks instead of the reference's getrf with discarded pivots.
+struct SelInvSystem {
+  std::vector<cplx*> A;
+  int* info = nullptr;
+};
+int build_selected_inverse(Plan& plan, std::vector<SelInvSystem>& sys, int npl, int b, int mode, bool nopiv);
+
+// Multi-level DDRGF (sweeps.cu) of systems with one layer count and unit
+// scales (D, U, Lw are the M blocks themselves, lop 'N'); d1s[level] are the
+// interior sizes, past the last level sequential RGF.
+int build_ddrgf_level(Plan& plan, const std::vector<TriSystem>& sys, std::vector<TriOut>& out,
+                      const std::vector<int>& d1s, size_t level);
+// Levels of the library's GPU cost model for nsys systems of npl layers of b.
+std::vector<int> choose_levels(int npl, int b, int nsys, int max_levels);
 
 std::string& last_error();
 void set_error(const std::string& msg);

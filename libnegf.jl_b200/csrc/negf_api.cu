@@ -578,6 +578,27 @@ int negf_zcopy_batched(char op, int32_t nprob, const int32_t* m, const int32_t* 
   }
 }
 
+int negf_zfill_batched(int32_t nprob, const int32_t* m, const int32_t* n, void* const* C, const int32_t* ldc,
+                       const double* value, void* stream) {
+  if (int r = check_device()) return r;
+  if (!value || nprob < 0 || (nprob > 0 && (!m || !n || !C || !ldc))) return fail(NEGF_ERR_INVALID, "bad arguments");
+  try {
+    Plan plan;
+    std::vector<ZBlockOp> ops;
+    for (int i = 0; i < nprob; ++i) {
+      if (m[i] <= 0 || n[i] <= 0) continue;
+      ZBlockOp o{};
+      o.C = static_cast<cplx*>(C[i]); o.ldc = std::max(1, ldc[i]);
+      o.m = m[i]; o.n = n[i]; o.kind = ZOP_FILL; o.alpha = make_double2(value[0], value[1]);
+      ops.push_back(o);
+    }
+    plan.blockops(ops);
+    return run_plan_sync(plan, static_cast<cudaStream_t>(stream), nullptr, 0, "negf_zfill_batched");
+  } catch (const std::bad_alloc&) {
+    return fail(NEGF_ERR_NOMEM, "device allocation failed");
+  }
+}
+
 int negf_zinv_batched(int32_t nprob, const int32_t* n, void* const* A, const int32_t* lda, void* const* Ainv,
                       const int32_t* ldainv, int32_t* info, void* stream) {
   if (int r = check_device()) return r;
@@ -1164,6 +1185,234 @@ int negf_solve(negf_device_t dev, int32_t nE, const double* energies, const negf
         for (int e = 0; e < cnt; ++e) t_out[e0 + e] = t2[2 * e];
       }
     }
+  }
+  return NEGF_SUCCESS;
+}
+
+// Selected inverse of M(E) for a list of energies (the batched form of one
+// bndiag_of_inv_rgf_local! / bndiag_of_inv_ddrgf! / Block_factorization! +
+// Block_inverse! call per energy point).
+namespace {
+
+// Device bytes of one energy of negf_device_selected_inverse (inputs,
+// workspace, device outputs of a host-output call, digit slices).
+size_t selinv_bytes_per_energy(const negf_device_s& d, int method, int d1, bool mixed, bool host_out) {
+  const size_t n = d.npl;
+  size_t mb = 0, sd = 0, su = 0;
+  for (int x : d.b) { mb = std::max<size_t>(mb, x); sd += (size_t)x * x; }
+  for (size_t i = 0; i + 1 < n; ++i) su += (size_t)d.b[i] * d.b[i + 1];
+  size_t c = sd + (d.has_S ? 2 * su : 0);                  // M(E) diagonal (+ off-diagonal) blocks
+  if (host_out || method == 2) c += sd + 2 * su;            // output blocks (in place for method 2)
+  size_t ops = 3;                                           // operands per layer of the widest mixed step
+  if (method == 0) {
+    c += sd + 2 * su + mb * mb + 64 * mb;                   // RGF work
+  } else if (method == 1) {
+    const size_t D1 = (size_t)std::max(1, d1);
+    c += sd + 2 * su + mb * mb + 64 * mb;                   // domain RGF work
+    c += D1 * sd;                                           // domain full inverses: D1 blocks per layer
+    c += 10 * sd;                                           // Schur complement and 12 / 21 / 11 temporaries
+    ops = 6;
+  } else {
+    c += 2 * sd + (2 * n + 2) * mb * mb + 64 * mb * n;      // factor inverses, scratch, LU / trtri scratch
+  }
+  size_t bytes = c * sizeof(cplx) + 64 * n;
+  if (mixed) {
+    const size_t pad = (mb + 127) / 128 * 128;
+    bytes += 21 * ops * n * pad * pad;
+  }
+  return bytes;
+}
+
+}  // namespace
+
+int negf_device_selected_inverse(negf_device_t dev, int32_t nE, const double* energies, const negf_solve_opts* opts,
+                                 int32_t method, int32_t nlevels, const int32_t* block_size_d1, void* gd_out,
+                                 void* gu_out, void* gl_out, int32_t out_on_device, void* stream) {
+  if (int r = check_device()) return r;
+  if (!dev || nE <= 0 || !energies || !opts || method < 0 || method > 2 || nlevels < 0 ||
+      nlevels > NEGF_DDRGF_MAX_LEVELS || (nlevels > 0 && !block_size_d1) ||
+      (opts->precision != NEGF_PREC_FP64 && opts->precision != NEGF_PREC_MIXED))
+    return fail(NEGF_ERR_INVALID, "negf_device_selected_inverse: bad arguments");
+  if (opts->sigma_per_energy)
+    return fail(NEGF_ERR_INVALID, "negf_device_selected_inverse: the device's constant self-energies are used");
+  const negf_device_s& d = *dev;
+  const int n = d.npl;
+  int mb = 0;
+  for (int x : d.b) mb = std::max(mb, x);
+  if (method == 2)
+    for (int x : d.b)
+      if (x != d.b[0]) return fail(NEGF_ERR_INVALID, "negf_device_selected_inverse: the block selected inverse "
+                                                     "needs one block size");
+  std::vector<size_t> od(n), ou(std::max(n - 1, 0));
+  size_t sd = 0, su = 0;
+  for (int i = 0; i < n; ++i) { od[i] = sd; sd += (size_t)d.b[i] * d.b[i]; }
+  for (int i = 0; i + 1 < n; ++i) { ou[i] = su; su += (size_t)d.b[i] * d.b[i + 1]; }
+  const bool mixed = opts->precision == NEGF_PREC_MIXED;
+  std::vector<int> fixed_d1s;
+  if (nlevels > 0) {
+    fixed_d1s.assign(block_size_d1, block_size_d1 + nlevels);
+    for (int x : fixed_d1s)
+      if (x <= 0) return fail(NEGF_ERR_INVALID, "negf_device_selected_inverse: interior sizes must be positive");
+  }
+  int chunk = opts->max_chunk > 0 ? std::min<int>(opts->max_chunk, nE) : nE;
+  if (opts->max_chunk <= 0) {
+    size_t fr = 0, tot = 0;
+    NEGF_TRY_CUDA(cudaMemGetInfo(&fr, &tot), "negf_device_selected_inverse");
+    const double budget = opts->hbm_budget_gb > 0 ? opts->hbm_budget_gb * 1e9 : 0.8 * (double)fr;
+    const int d1 = nlevels > 0 ? fixed_d1s[0] : 16;
+    const size_t per = selinv_bytes_per_energy(d, method, d1, mixed, !out_on_device);
+    chunk = std::min<int>(nE, (int)std::max(1.0, std::floor(budget / (double)per)));
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const cudaMemcpyKind kind = cudaMemcpyDeviceToHost;
+  static constexpr cplx ONE{1.0, 0.0}, MONE{-1.0, 0.0}, ZERO{0.0, 0.0};
+  auto kzero = [](cplx* C, int ldc, int m, int nn, const cplx* Cin, cplx beta, cplx diag) {
+    ZGemmProblem p{};
+    p.C = C; p.Cin = Cin; p.m = m; p.n = nn; p.k = 0;
+    p.lda = p.ldb = 1; p.ldc = ldc; p.ldcin = ldc;
+    p.alpha = ZERO; p.beta = beta; p.diag = diag;
+    return p;
+  };
+  auto bop = [](int kindop, const cplx* A, int lda, cplx* C, int ldc, int m, int nn, cplx alpha, cplx beta) {
+    ZBlockOp o{};
+    o.A = A; o.lda = lda; o.C = C; o.ldc = ldc; o.m = m; o.n = nn; o.kind = kindop; o.alpha = alpha; o.beta = beta;
+    return o;
+  };
+  for (int e0 = 0; e0 < nE;) {
+    const int cnt = std::min(chunk, nE - e0);
+    try {
+      Plan plan;
+      plan.set_mixed(mixed);
+      plan.set_schedule(opts->gemm_form, opts->gj_nb);
+      int* dinfo = static_cast<int*>(plan.alloc(sizeof(int) * (size_t)cnt * n));
+      // output blocks of this chunk: the caller's device buffers, or plan memory
+      // downloaded afterwards (every sweep writes all three kinds)
+      auto out_base = [&](void* user, size_t per) -> cplx* {
+        if (user && out_on_device) return static_cast<cplx*>(user) + (size_t)e0 * per;
+        return plan.alloc_c((size_t)cnt * std::max<size_t>(per, 1));
+      };
+      cplx* GD = out_base(gd_out, sd);
+      cplx* GU = (n > 1) ? out_base(gu_out, su) : nullptr;
+      cplx* GL = (n > 1) ? out_base(gl_out, su) : nullptr;
+      // M(E) = (E + i eta) S - H - Sigma: diagonal blocks per energy; the
+      // off-diagonal blocks are shared by all energies unless S couples layers
+      std::vector<ZGemmProblem> asm_g;
+      std::vector<ZBlockOp> asm_o1, asm_o2;
+      std::vector<cplx*> Mu_sh(std::max(n - 1, 0)), Ml_sh(std::max(n - 1, 0));
+      if (!d.has_S && method != 2)
+        for (int i = 0; i + 1 < n; ++i) {
+          Mu_sh[i] = plan.alloc_c((size_t)d.b[i] * d.b[i + 1]);
+          Ml_sh[i] = plan.alloc_c((size_t)d.b[i] * d.b[i + 1]);
+          asm_g.push_back(kzero(Mu_sh[i], d.b[i], d.b[i], d.b[i + 1], d.Hu[i], MONE, ZERO));
+          asm_o1.push_back(bop(ZOP_CTRANS_AXPBY, d.Hu[i], d.b[i], Ml_sh[i], d.b[i + 1], d.b[i + 1], d.b[i], MONE, ZERO));
+        }
+      std::vector<TriSystem> sys(cnt);
+      std::vector<TriOut> out(cnt);
+      std::vector<SelInvSystem> ssys(method == 2 ? cnt : 0);
+      for (int e = 0; e < cnt; ++e) {
+        const cplx z = make_double2(energies[e0 + e], opts->eta);
+        TriSystem& ts = sys[e];
+        TriOut& o = out[e];
+        ts.info = dinfo + (size_t)e * n;
+        std::vector<cplx*> Md(n), Mu(std::max(n - 1, 0)), Ml(std::max(n - 1, 0));
+        for (int i = 0; i < n; ++i) {
+          const int bi = d.b[i];
+          Md[i] = method == 2 ? GD + (size_t)e * sd + od[i] : plan.alloc_c((size_t)bi * bi);
+          asm_g.push_back(kzero(Md[i], bi, bi, bi, d.D[i], MONE, d.has_S ? ZERO : z));
+          if (d.has_S) asm_o1.push_back(bop(ZOP_AXPBY, d.Sd[i], bi, Md[i], bi, bi, bi, z, ONE));
+        }
+        for (int i = 0; i + 1 < n; ++i) {
+          const int bi = d.b[i], bj = d.b[i + 1];
+          if (method == 2) {
+            Mu[i] = GU + (size_t)e * su + ou[i];
+            Ml[i] = GL + (size_t)e * su + ou[i];
+          } else if (d.has_S) {
+            Mu[i] = plan.alloc_c((size_t)bi * bj);
+            Ml[i] = plan.alloc_c((size_t)bi * bj);
+          } else {
+            Mu[i] = Mu_sh[i];
+            Ml[i] = Ml_sh[i];
+          }
+          if (method == 2 || d.has_S) {
+            asm_g.push_back(kzero(Mu[i], bi, bi, bj, d.Hu[i], MONE, ZERO));
+            asm_o1.push_back(bop(ZOP_CTRANS_AXPBY, d.Hu[i], bi, Ml[i], bj, bj, bi, MONE, ZERO));
+            if (d.has_S) {
+              asm_o2.push_back(bop(ZOP_AXPBY, d.Su[i], bi, Mu[i], bi, bi, bj, z, ONE));
+              asm_o2.push_back(bop(ZOP_CTRANS_AXPBY, d.Su[i], bi, Ml[i], bj, bj, bi, z, ONE));
+            }
+          }
+        }
+        if (method == 2) {
+          SelInvSystem& ss = ssys[e];
+          ss.A.assign((size_t)n * n, nullptr);
+          ss.info = ts.info;
+          for (int i = 0; i < n; ++i) ss.A[(size_t)i * n + i] = Md[i];
+          for (int i = 0; i + 1 < n; ++i) {
+            ss.A[(size_t)i * n + i + 1] = Mu[i];
+            ss.A[(size_t)(i + 1) * n + i] = Ml[i];
+          }
+          continue;
+        }
+        for (int i = 0; i < n; ++i) {
+          ts.b.push_back(d.b[i]);
+          ts.D.push_back(Md[i]); ts.ldD.push_back(d.b[i]);
+          o.d.push_back(GD + (size_t)e * sd + od[i]); o.ldd.push_back(d.b[i]);
+        }
+        for (int i = 0; i + 1 < n; ++i) {
+          ts.U.push_back(Mu[i]); ts.ldU.push_back(d.b[i]);
+          ts.Lw.push_back(Ml[i]); ts.ldL.push_back(d.b[i + 1]);
+          o.u.push_back(GU + (size_t)e * su + ou[i]); o.ldu.push_back(d.b[i]);
+          o.l.push_back(GL + (size_t)e * su + ou[i]); o.ldl.push_back(d.b[i + 1]);
+        }
+      }
+      plan.gemm_fp64('N', 'N', asm_g);  // k = 0: C = -Cin (+ z I)
+      plan.blockops(asm_o1);
+      plan.blockops(asm_o2);
+      if (method == 0) {
+        std::vector<RgfWork> w(cnt);
+        for (int e = 0; e < cnt; ++e) alloc_rgf_work(plan, sys[e], w[e]);
+        build_rgf_upward(plan, sys, w);
+        build_rgf_downward(plan, sys, w, out);
+      } else if (method == 1) {
+        const std::vector<int> d1s = nlevels > 0 ? fixed_d1s : choose_levels(n, mb, cnt, NEGF_DDRGF_MAX_LEVELS);
+        if (int r = build_ddrgf_level(plan, sys, out, d1s, 0)) return r;
+      } else {
+        if (int r = build_selected_inverse(plan, ssys, n, d.b[0], 3, true)) return r;
+      }
+      NEGF_TRY_CUDA(plan.run(st, false), "negf_device_selected_inverse");
+      if (!out_on_device) {
+        if (gd_out)
+          NEGF_TRY_CUDA(cudaMemcpyAsync(static_cast<cplx*>(gd_out) + (size_t)e0 * sd, GD, (size_t)cnt * sd * sizeof(cplx),
+                                        kind, st), "negf_device_selected_inverse output");
+        if (gu_out && n > 1)
+          NEGF_TRY_CUDA(cudaMemcpyAsync(static_cast<cplx*>(gu_out) + (size_t)e0 * su, GU, (size_t)cnt * su * sizeof(cplx),
+                                        kind, st), "negf_device_selected_inverse output");
+        if (gl_out && n > 1)
+          NEGF_TRY_CUDA(cudaMemcpyAsync(static_cast<cplx*>(gl_out) + (size_t)e0 * su, GL, (size_t)cnt * su * sizeof(cplx),
+                                        kind, st), "negf_device_selected_inverse output");
+      }
+      NEGF_TRY_CUDA(cudaStreamSynchronize(st), "negf_device_selected_inverse");
+      if (plan.error_flag()) {
+        int h = 0;
+        NEGF_TRY_CUDA(cudaMemcpy(&h, plan.error_flag(), sizeof(int), cudaMemcpyDeviceToHost), "negf_device_selected_inverse");
+        if (h) return fail(NEGF_ERR_TIMEOUT, "negf_device_selected_inverse: a tensor-core wait timed out");
+      }
+      std::vector<int> info((size_t)cnt * n);
+      NEGF_TRY_CUDA(cudaMemcpy(info.data(), dinfo, sizeof(int) * info.size(), cudaMemcpyDeviceToHost),
+                    "negf_device_selected_inverse");
+      for (int e = 0; e < cnt; ++e)
+        for (int i = 0; i < n; ++i)
+          if (info[(size_t)e * n + i]) {
+            char buf[160];
+            std::snprintf(buf, sizeof buf, "negf_device_selected_inverse: energy %d is singular (block %d)", e0 + e, i);
+            return fail(NEGF_ERR_SINGULAR, buf);
+          }
+    } catch (const std::bad_alloc&) {
+      if (chunk == 1) return fail(NEGF_ERR_NOMEM, "negf_device_selected_inverse: device allocation failed");
+      chunk = std::max(1, chunk / 2);  // retry this chunk with half as many energies
+      continue;
+    }
+    e0 += cnt;
   }
   return NEGF_SUCCESS;
 }

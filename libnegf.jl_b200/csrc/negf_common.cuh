@@ -76,7 +76,9 @@ struct ZLuProblem {
   cplx* Linv;    // scratch nb x nb (inverse of the panel's unit-lower block)
   cplx* T;       // scratch nb x n (A12 copy)
   int* info;
-  int n, ld, pad0_, pad1_;
+  int n, ld;
+  int nopiv;     // 1: no row interchanges (the pivot of column c is row c)
+  int pad_;
 };
 
 // One matrix of a batched triangular inverse (zlu.cu).

@@ -70,17 +70,17 @@ int run_sync(Plan& plan, cudaStream_t st, int* dinfo, int n, const char* what) {
   return NEGF_SUCCESS;
 }
 
-// LU of one block with plan-owned scratch; returns the 0-based pivot array.
-int* add_lu(Plan& plan, cplx* A, int n, int ld, int* info) {
-  int nb = lu_panel_width(n);
+// LU request of one block with plan-owned scratch.
+LuSpec lu_spec(Plan& plan, cplx* A, int n, int ld, int* info, bool nopiv) {
+  const int nb = lu_panel_width(n);
   LuSpec s;
   s.A = A; s.n = n; s.ld = ld;
   s.ipiv = static_cast<int*>(plan.alloc(sizeof(int) * n));
   s.Linv = plan.alloc_c((size_t)nb * nb);
   s.T = plan.alloc_c((size_t)nb * n);
   s.info = info;
-  plan.getrf({s});
-  return s.ipiv;
+  s.nopiv = nopiv;
+  return s;
 }
 
 TriSpec tri_spec(Plan& plan, const cplx* A, int n, int lda, cplx* X) {
@@ -91,6 +91,173 @@ TriSpec tri_spec(Plan& plan, const cplx* A, int n, int lda, cplx* X) {
 }
 
 }  // namespace
+
+
+namespace negf {
+
+// Block_factorization! then Block_inverse! (src/selected_inverse.jl:9-55,
+// :139-206) over systems with one block pattern (that of system 0); every step
+// is one batched launch over all systems.
+int build_selected_inverse(Plan& plan, std::vector<SelInvSystem>& S, int npl, int b, int mode, bool nopiv) {
+  const int ns = static_cast<int>(S.size());
+  auto at = [&](int s, int i, int j) -> cplx* { return S[s].A[(size_t)i * npl + j]; };
+  for (int s = 0; s < ns; ++s)
+    for (int i = 0; i < npl; ++i)
+      for (int j = 0; j < npl; ++j)
+        if ((at(s, i, j) != nullptr) != (at(0, i, j) != nullptr))
+          return fail(NEGF_ERR_INVALID, "the systems of a batched selected inverse must share one block pattern");
+  for (int i = 0; i < npl; ++i)
+    if (!at(0, i, i)) return fail(NEGF_ERR_INVALID, "every diagonal block must be assigned");
+  const size_t bb = (size_t)b * b;
+  std::vector<std::vector<cplx*>> Uinv(ns, std::vector<cplx*>(npl)), Linv(ns, std::vector<cplx*>(npl));
+  std::vector<cplx*> tmp(ns);
+  for (int s = 0; s < ns; ++s) {
+    for (int i = 0; i < npl; ++i) { Uinv[s][i] = plan.alloc_c(bb); Linv[s][i] = plan.alloc_c(bb); }
+    tmp[s] = plan.alloc_c(bb * (size_t)std::max(2 * npl + 2, 10));
+  }
+  auto scratch = [&](int s, int k) { return tmp[s] + bb * k; };
+  auto inverses = [&](int i) {
+    std::vector<TriSpec> up, lo;
+    for (int s = 0; s < ns; ++s) {
+      up.push_back(tri_spec(plan, at(s, i, i), b, b, Uinv[s][i]));
+      lo.push_back(tri_spec(plan, at(s, i, i), b, b, Linv[s][i]));
+    }
+    plan.trtri(up, true);
+    plan.trtri(lo, false);
+  };
+  if (mode & 1) {
+    // Block_factorization! (selected_inverse.jl:9-55).  Fill-in blocks are
+    // pre-zeroed, so "assign a zero block, then gemm with beta = 0"
+    // (:43-46) is the same as accumulating into them; a fill block that the
+    // reference creates at step i is never read or written before step i.
+    for (int i = 0; i < npl; ++i) {
+      // :18, be_getrf! (backend_cpu.jl:255-265: LAPACK getrf whose pivots the
+      // reference discards) or lu(NoPivot()), the factorisation :17 names
+      std::vector<LuSpec> lus;
+      for (int s = 0; s < ns; ++s) lus.push_back(lu_spec(plan, at(s, i, i), b, b, S[s].info + i, nopiv));
+      plan.getrf(lus);
+      inverses(i);
+      std::vector<ZBlockOp> cp;
+      std::vector<ZGemmProblem> g;
+      for (int s = 0; s < ns; ++s) {
+        int k = 0;
+        for (int j = i + 1; j < npl; ++j) {
+          if (at(s, j, i)) {                                         // :23  A[j,i] / U_ii
+            cp.push_back(copy_op(at(s, j, i), b, scratch(s, k), b, b, b));
+            g.push_back(gp(scratch(s, k), b, Uinv[s][i], b, at(s, j, i), b, b, b, b, ONE));
+            ++k;
+          }
+          if (at(s, i, j)) {                                         // :27  L_ii \ A[i,j]
+            cp.push_back(copy_op(at(s, i, j), b, scratch(s, k), b, b, b));
+            g.push_back(gp(Linv[s][i], b, scratch(s, k), b, at(s, i, j), b, b, b, b, ONE));
+            ++k;
+          }
+        }
+      }
+      plan.blockops(cp);
+      plan.gemm('N', 'N', g);
+      std::vector<ZGemmProblem> sch;                                 // :32-51 Schur updates
+      for (int s = 0; s < ns; ++s)
+        for (int kk = i + 1; kk < npl; ++kk) {
+          if (!at(s, i, kk) || !at(s, kk, i)) continue;
+          sch.push_back(gp(at(s, kk, i), b, at(s, i, kk), b, at(s, kk, kk), b, b, b, b, MONE, at(s, kk, kk), b, ONE));
+          for (int l = kk + 1; l < npl; ++l) {
+            if (!at(s, i, l) || !at(s, l, i)) continue;
+            if (!at(s, kk, l) || !at(s, l, kk)) return fail(NEGF_ERR_INVALID, "missing fill-in block");
+            sch.push_back(gp(at(s, kk, i), b, at(s, i, l), b, at(s, kk, l), b, b, b, b, MONE, at(s, kk, l), b, ONE));
+            sch.push_back(gp(at(s, l, i), b, at(s, i, kk), b, at(s, l, kk), b, b, b, b, MONE, at(s, l, kk), b, ONE));
+          }
+        }
+      plan.gemm('N', 'N', sch);
+    }
+  } else {
+    for (int i = 0; i < npl; ++i) inverses(i);
+  }
+  if (!(mode & 2)) return NEGF_SUCCESS;
+  // Block_inverse! (selected_inverse.jl:139-206)
+  {
+    const int i = npl - 1;                                           // :158 getri(A[N,N])
+    std::vector<ZGemmProblem> g;
+    for (int s = 0; s < ns; ++s) g.push_back(gp(Uinv[s][i], b, Linv[s][i], b, at(s, i, i), b, b, b, b, ONE));
+    plan.gemm('N', 'N', g);
+  }
+  for (int i = npl - 2; i >= 0; --i) {
+    std::vector<int> js;
+    for (int j = i + 1; j < npl; ++j)
+      if (at(0, i, j)) js.push_back(j);
+    if (js.size() > 2) return fail(NEGF_ERR_INVALID, "Block_inverse! supports at most two upper neighbours per block row");
+    for (int j : js)
+      if (!at(0, j, i)) return fail(NEGF_ERR_INVALID, "Block_inverse! needs a symmetric block pattern");
+    // Uij = sum_k A[i,k] A[k,j];  Lji = sum_k A[j,k] A[k,i]   (:161-169)
+    std::vector<std::vector<int>> ks(js.size());
+    size_t rounds = 0;
+    for (size_t v = 0; v < js.size(); ++v) {
+      for (int k = i + 1; k < npl; ++k)
+        if (at(0, i, k) && at(0, k, js[v])) ks[v].push_back(k);
+      rounds = std::max(rounds, ks[v].size());
+    }
+    auto U = [&](int s, size_t v) { return scratch(s, (int)v); };
+    auto L = [&](int s, size_t v) { return scratch(s, 2 + (int)v); };
+    auto T = [&](int s, size_t v) { return scratch(s, 4 + (int)v); };
+    auto Aii = [&](int s) { return scratch(s, 6); };
+    for (size_t r = 0; r < rounds; ++r) {
+      std::vector<ZGemmProblem> g;
+      for (int s = 0; s < ns; ++s)
+        for (size_t v = 0; v < js.size(); ++v) {
+          if (r >= ks[v].size()) continue;
+          const int j = js[v], k = ks[v][r];
+          g.push_back(gp(at(s, i, k), b, at(s, k, j), b, U(s, v), b, b, b, b, ONE, r ? U(s, v) : nullptr, b,
+                         r ? ONE : ZERO));
+          g.push_back(gp(at(s, j, k), b, at(s, k, i), b, L(s, v), b, b, b, b, ONE, r ? L(s, v) : nullptr, b,
+                         r ? ONE : ZERO));
+        }
+      plan.gemm('N', 'N', g);
+    }
+    // Uij = -U_ii^{-1} Uij ;  Lji = -Lji L_ii^{-1}   (:172, :174)
+    {
+      std::vector<ZGemmProblem> g1, g2;
+      for (int s = 0; s < ns; ++s)
+        for (size_t v = 0; v < js.size(); ++v) {
+          g1.push_back(gp(Uinv[s][i], b, U(s, v), b, T(s, v), b, b, b, b, MONE));
+          g2.push_back(gp(L(s, v), b, Linv[s][i], b, scratch(s, 7 + (int)v), b, b, b, b, MONE));
+        }
+      plan.gemm('N', 'N', g1);
+      plan.gemm('N', 'N', g2);
+    }
+    // Aii = sum_j Uij A[j,i]  (:183), then A[j,i] = Lji, A[i,j] = Uij (:185-187)
+    for (size_t v = 0; v < js.size(); ++v) {
+      std::vector<ZGemmProblem> g;
+      for (int s = 0; s < ns; ++s)
+        g.push_back(gp(T(s, v), b, at(s, js[v], i), b, Aii(s), b, b, b, b, ONE, v ? Aii(s) : nullptr, b,
+                       v ? ONE : ZERO));
+      plan.gemm('N', 'N', g);
+    }
+    std::vector<ZBlockOp> cp;
+    for (int s = 0; s < ns; ++s) {
+      if (js.empty()) {
+        ZBlockOp z{};
+        z.C = Aii(s); z.ldc = b; z.m = z.n = b; z.kind = ZOP_FILL;
+        cp.push_back(z);
+      }
+      for (size_t v = 0; v < js.size(); ++v) {
+        cp.push_back(copy_op(scratch(s, 7 + (int)v), b, at(s, js[v], i), b, b, b));
+        cp.push_back(copy_op(T(s, v), b, at(s, i, js[v]), b, b, b));
+      }
+    }
+    plan.blockops(cp);
+    // A[i,i] = getri(A[i,i]) - Aii L_ii^{-1}   (:195-199)
+    std::vector<ZGemmProblem> g1, g2;
+    for (int s = 0; s < ns; ++s) {
+      g1.push_back(gp(Aii(s), b, Linv[s][i], b, scratch(s, 9), b, b, b, b, ONE));
+      g2.push_back(gp(Uinv[s][i], b, Linv[s][i], b, at(s, i, i), b, b, b, b, ONE, scratch(s, 9), b, MONE));
+    }
+    plan.gemm('N', 'N', g1);
+    plan.gemm('N', 'N', g2);
+  }
+  return NEGF_SUCCESS;
+}
+
+}  // namespace negf
 
 extern "C" {
 
@@ -207,127 +374,28 @@ int negf_zgetri_nopiv_batched(int32_t nprob, const int32_t* n, void* const* A, c
 }
 
 int negf_selected_inverse(int32_t npl, int32_t b, void* const* Ab, const uint8_t* fill, int32_t mode, void* stream) {
+  return negf_selected_inverse_batched(1, npl, b, Ab, fill, mode, 1, NEGF_PREC_FP64, stream);
+}
+
+int negf_selected_inverse_batched(int32_t nsys, int32_t npl, int32_t b, void* const* Ab, const uint8_t* fill,
+                                  int32_t mode, int32_t pivoting, int32_t precision, void* stream) {
   if (int r = check_device()) return r;
-  if (npl <= 0 || b <= 0 || b > kMaxBlock || !Ab || mode < 1 || mode > 3) return fail(NEGF_ERR_INVALID, "bad arguments");
-  (void)fill;  // fill-in blocks arrive pre-zeroed; they act as assigned from the start (equivalent, see below)
-  auto at = [&](int i, int j) -> cplx* { return static_cast<cplx*>(Ab[(size_t)i * npl + j]); };
-  for (int i = 0; i < npl; ++i)
-    if (!at(i, i)) return fail(NEGF_ERR_INVALID, "every diagonal block must be assigned");
+  if (nsys <= 0 || npl <= 0 || b <= 0 || b > kMaxBlock || !Ab || mode < 1 || mode > 3 ||
+      (precision != NEGF_PREC_FP64 && precision != NEGF_PREC_MIXED))
+    return fail(NEGF_ERR_INVALID, "bad arguments");
+  (void)fill;  // fill-in blocks arrive pre-zeroed; they act as assigned from the start (see the builder)
   try {
     Plan plan;
-    int* dinfo = static_cast<int*>(plan.alloc(sizeof(int) * npl));
-    const size_t bb = (size_t)b * b;
-    std::vector<cplx*> Uinv(npl), Linv(npl);
-    for (int i = 0; i < npl; ++i) { Uinv[i] = plan.alloc_c(bb); Linv[i] = plan.alloc_c(bb); }
-    cplx* tmp = plan.alloc_c(bb * (size_t)std::max(2 * npl + 2, 10));
-    auto scratch = [&](int k) { return tmp + bb * k; };
-    auto inverses = [&](int i) {
-      plan.trtri({tri_spec(plan, at(i, i), b, b, Uinv[i])}, true);
-      plan.trtri({tri_spec(plan, at(i, i), b, b, Linv[i])}, false);
-    };
-    if (mode & 1) {
-      // Block_factorization! (selected_inverse.jl:9-55).  Fill-in blocks are
-      // pre-zeroed, so "assign a zero block, then gemm with beta = 0"
-      // (:43-46) is the same as accumulating into them; a fill block that the
-      // reference creates at step i is never read or written before step i.
-      for (int i = 0; i < npl; ++i) {
-        add_lu(plan, at(i, i), b, b, dinfo + i);                   // :18 (pivots discarded)
-        inverses(i);
-        std::vector<ZBlockOp> cp;
-        std::vector<ZGemmProblem> g;
-        int k = 0;
-        for (int j = i + 1; j < npl; ++j) {
-          if (at(j, i)) {                                            // :23  A[j,i] / U_ii
-            cp.push_back(copy_op(at(j, i), b, scratch(k), b, b, b));
-            g.push_back(gp(scratch(k), b, Uinv[i], b, at(j, i), b, b, b, b, ONE));
-            ++k;
-          }
-          if (at(i, j)) {                                            // :27  L_ii \ A[i,j]
-            cp.push_back(copy_op(at(i, j), b, scratch(k), b, b, b));
-            g.push_back(gp(Linv[i], b, scratch(k), b, at(i, j), b, b, b, b, ONE));
-            ++k;
-          }
-        }
-        plan.blockops(cp);
-        plan.gemm('N', 'N', g);
-        std::vector<ZGemmProblem> s;                                 // :32-51 Schur updates
-        for (int kk = i + 1; kk < npl; ++kk) {
-          if (!at(i, kk) || !at(kk, i)) continue;
-          s.push_back(gp(at(kk, i), b, at(i, kk), b, at(kk, kk), b, b, b, b, MONE, at(kk, kk), b, ONE));
-          for (int l = kk + 1; l < npl; ++l) {
-            if (!at(i, l) || !at(l, i)) continue;
-            if (!at(kk, l) || !at(l, kk)) return fail(NEGF_ERR_INVALID, "missing fill-in block");
-            s.push_back(gp(at(kk, i), b, at(i, l), b, at(kk, l), b, b, b, b, MONE, at(kk, l), b, ONE));
-            s.push_back(gp(at(l, i), b, at(i, kk), b, at(l, kk), b, b, b, b, MONE, at(l, kk), b, ONE));
-          }
-        }
-        plan.gemm('N', 'N', s);
-      }
-    } else {
-      for (int i = 0; i < npl; ++i) inverses(i);
+    plan.set_mixed(precision == NEGF_PREC_MIXED);
+    int* dinfo = static_cast<int*>(plan.alloc(sizeof(int) * (size_t)nsys * npl));
+    std::vector<SelInvSystem> sys(nsys);
+    for (int s = 0; s < nsys; ++s) {
+      sys[s].A.resize((size_t)npl * npl);
+      for (size_t k = 0; k < (size_t)npl * npl; ++k) sys[s].A[k] = static_cast<cplx*>(Ab[(size_t)s * npl * npl + k]);
+      sys[s].info = dinfo + (size_t)s * npl;
     }
-    if (mode & 2) {
-      // Block_inverse! (selected_inverse.jl:139-206)
-      {
-        int i = npl - 1;                                             // :158 getri(A[N,N])
-        plan.gemm('N', 'N', {gp(Uinv[i], b, Linv[i], b, at(i, i), b, b, b, b, ONE)});
-      }
-      for (int i = npl - 2; i >= 0; --i) {
-        std::vector<int> js;
-        for (int j = i + 1; j < npl; ++j)
-          if (at(i, j)) js.push_back(j);
-        if (js.size() > 2)
-          return fail(NEGF_ERR_INVALID, "Block_inverse! supports at most two upper neighbours per block row");
-        // Uij = sum_k A[i,k] A[k,j];  Lji = sum_k A[j,k] A[k,i]   (:161-169)
-        std::vector<std::vector<int>> ks(js.size());
-        size_t rounds = 0;
-        for (size_t v = 0; v < js.size(); ++v) {
-          for (int k = i + 1; k < npl; ++k)
-            if (at(i, k) && at(k, js[v])) ks[v].push_back(k);
-          rounds = std::max(rounds, ks[v].size());
-        }
-        cplx* U[2] = {scratch(0), scratch(1)};
-        cplx* L[2] = {scratch(2), scratch(3)};
-        cplx* T[2] = {scratch(4), scratch(5)};
-        cplx* Aii = scratch(6);
-        for (size_t r = 0; r < rounds; ++r) {
-          std::vector<ZGemmProblem> g;
-          for (size_t v = 0; v < js.size(); ++v) {
-            if (r >= ks[v].size()) continue;
-            int j = js[v], k = ks[v][r];
-            g.push_back(gp(at(i, k), b, at(k, j), b, U[v], b, b, b, b, ONE, r ? U[v] : nullptr, b, r ? ONE : ZERO));
-            g.push_back(gp(at(j, k), b, at(k, i), b, L[v], b, b, b, b, ONE, r ? L[v] : nullptr, b, r ? ONE : ZERO));
-          }
-          plan.gemm('N', 'N', g);
-        }
-        // Uij = -U_ii^{-1} Uij ;  Lji = -Lji L_ii^{-1}   (:172, :174)
-        {
-          std::vector<ZGemmProblem> g1, g2;
-          for (size_t v = 0; v < js.size(); ++v) {
-            if (!at(js[v], i)) return fail(NEGF_ERR_INVALID, "Block_inverse! needs a symmetric block pattern");
-            g1.push_back(gp(Uinv[i], b, U[v], b, T[v], b, b, b, b, MONE));
-            g2.push_back(gp(L[v], b, Linv[i], b, scratch(7 + (int)v), b, b, b, b, MONE));
-          }
-          plan.gemm('N', 'N', g1);
-          plan.gemm('N', 'N', g2);
-        }
-        // Aii = sum_j Uij A[j,i]  (:183), then A[j,i] = Lji, A[i,j] = Uij (:185-187)
-        for (size_t v = 0; v < js.size(); ++v)
-          plan.gemm('N', 'N', {gp(T[v], b, at(js[v], i), b, Aii, b, b, b, b, ONE, v ? Aii : nullptr, b,
-                                  v ? ONE : ZERO)});
-        if (js.empty()) plan.blockops({[&] { ZBlockOp z{}; z.C = Aii; z.ldc = b; z.m = z.n = b; z.kind = ZOP_FILL; return z; }()});
-        std::vector<ZBlockOp> cp;
-        for (size_t v = 0; v < js.size(); ++v) {
-          cp.push_back(copy_op(scratch(7 + (int)v), b, at(js[v], i), b, b, b));
-          cp.push_back(copy_op(T[v], b, at(i, js[v]), b, b, b));
-        }
-        plan.blockops(cp);
-        // A[i,i] = getri(A[i,i]) - Aii L_ii^{-1}   (:195-199)
-        plan.gemm('N', 'N', {gp(Aii, b, Linv[i], b, scratch(9), b, b, b, b, ONE)});
-        plan.gemm('N', 'N', {gp(Uinv[i], b, Linv[i], b, at(i, i), b, b, b, b, ONE, scratch(9), b, MONE)});
-      }
-    }
-    return run_sync(plan, static_cast<cudaStream_t>(stream), dinfo, npl, "negf_selected_inverse");
+    if (int r = build_selected_inverse(plan, sys, npl, b, mode, pivoting == 0)) return r;
+    return run_sync(plan, static_cast<cudaStream_t>(stream), dinfo, nsys * npl, "negf_selected_inverse");
   } catch (const std::bad_alloc&) {
     return fail(NEGF_ERR_NOMEM, "device allocation failed");
   }

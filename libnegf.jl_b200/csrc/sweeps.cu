@@ -138,6 +138,10 @@ struct GpuCost {
   }
 };
 
+}  // namespace
+
+namespace negf {
+
 std::vector<int> choose_levels(int npl, int b, int nsys, int max_levels) {
   GpuCost c(b, nsys);
   // best[lev][n]: (time, first interior size or 0 for sequential RGF)
@@ -169,6 +173,10 @@ std::vector<int> choose_levels(int npl, int b, int nsys, int max_levels) {
   }
   return d1s;
 }
+
+}  // namespace negf
+
+namespace {
 
 // One level: the interior size, or npl (sequential RGF) when DDRGF does not pay.
 int choose_d1(int npl, int b, int nsys) {
@@ -262,6 +270,10 @@ void build_seq_rgf(Plan& plan, const std::vector<TriSystem>& sys, std::vector<Tr
   build_rgf_upward(plan, sys, w);
   build_rgf_downward(plan, sys, w, out);
 }
+
+}  // namespace
+
+namespace negf {
 
 // One DDRGF level over systems with the same layer count (block sizes may
 // differ per system), writing the tridiagonal of every system's inverse into
@@ -477,7 +489,7 @@ int build_ddrgf_level(Plan& plan, const std::vector<TriSystem>& sys, std::vector
   return NEGF_SUCCESS;
 }
 
-}  // namespace
+}  // namespace negf
 
 extern "C" {
 
@@ -654,9 +666,17 @@ int negf_general_rgf(int32_t nsys, int32_t npl, int32_t ndiag, const int32_t* bl
 int negf_ddrgf_levels(int32_t nsys, int32_t npl, const int32_t* block_sizes, void* const* Md, void* const* Mu,
                       void* const* Ml, int32_t nlevels, const int32_t* block_size_d1, void* const* Gd,
                       void* const* Gu, void* const* Gl, void* stream) {
+  return negf_ddrgf_levels_ex(nsys, npl, block_sizes, Md, Mu, Ml, nlevels, block_size_d1, Gd, Gu, Gl,
+                              NEGF_PREC_FP64, stream);
+}
+
+int negf_ddrgf_levels_ex(int32_t nsys, int32_t npl, const int32_t* block_sizes, void* const* Md, void* const* Mu,
+                         void* const* Ml, int32_t nlevels, const int32_t* block_size_d1, void* const* Gd,
+                         void* const* Gu, void* const* Gl, int32_t precision, void* stream) {
   if (int r = check_device()) return r;
   if (nsys <= 0 || npl <= 0 || !block_sizes || !Md || !Gd || (npl > 1 && (!Mu || !Ml)) || nlevels < 0 ||
-      nlevels > kMaxDdrgfLevels || (nlevels > 0 && !block_size_d1))
+      nlevels > kMaxDdrgfLevels || (nlevels > 0 && !block_size_d1) ||
+      (precision != NEGF_PREC_FP64 && precision != NEGF_PREC_MIXED))
     return fail(NEGF_ERR_INVALID, "bad arguments");
   std::vector<int> d1s;
   if (nlevels == 0) {
@@ -673,6 +693,7 @@ int negf_ddrgf_levels(int32_t nsys, int32_t npl, const int32_t* block_sizes, voi
       return fail(NEGF_ERR_INVALID, "block sizes must be in [1, 1024]");
   try {
     Plan plan;
+    plan.set_mixed(precision == NEGF_PREC_MIXED);
     int* dinfo = static_cast<int*>(plan.alloc(sizeof(int) * nsys));
     std::vector<TriSystem> sys(nsys);
     std::vector<TriOut> out(nsys);

@@ -12,11 +12,12 @@
 //     digits are the bytes of x + C6 (lower ones minus 128), so the split is a
 //     rounding (FP64 adds), an add and byte permutes per element
 //     (representation error <= 2^(e_r - 55));
-//   * product: sum_k A[r,k] B[c,k] = 2^(eA_r + eB_c) sum_{D=0..7} 2^(-12 - 8D)
+//   * product: sum_k A[r,k] B[c,k] = 2^(eA_r + eB_c) sum_{D=0..6} 2^(-12 - 8D)
 //     acc_D, acc_D = sum_{i+j=D} sum_k sA_i sB_j; each acc_D is an exact int32
-//     sum (|acc_D| <= 7 * K * 2^14 < 2^31 for K < 18000); the 34 digit pairs
-//     with i + j <= 7 are formed; the dropped ones sum to below
-//     2^(eA_r + eB_c - 59) K, so a product is as accurate as an FP64 one;
+//     sum (|acc_D| <= 7 * K * 2^14 < 2^31 for K < 18000); the 28 digit pairs
+//     with i + j <= 6 are formed; the dropped ones (i + j >= 7) sum to below
+//     2^(eA_r + eB_c - 51.4) K, i.e. within 3x of the FP64 rounding bound
+//     K u |a| |b| of one product;
 //   * complex: 3M (Gauss) -- P1 = Ar Br, P2 = Ai Bi, P3 = (Ar+Ai)(Br+Bi),
 //     Re = P1 - P2, Im = P3 - P1 - P2 -- the three real operands of a side
 //     share one scale per row and xr + xi is formed exactly in integers;
@@ -29,8 +30,8 @@
 //   * the product kernel (persistent, one CTA per SM, 128 x 64 output tiles,
 //     256 threads): one thread streams stages with cp.async.bulk into a 5-deep
 //     mbarrier ring, refilling each slot as its MMAs retire; another issues the
-//     12 MMAs (N = 64..256) of each stage into eight TMEM accumulators (one per
-//     digit diagonal, 8 x 64 columns); after
+//     10 MMAs (N = 64..256) of each stage into seven TMEM accumulators (one per
+//     digit diagonal, 7 x 64 columns); after
 //     each real product the eight warps drain the accumulators into FP64
 //     registers, and at the end of a tile they write
 //     C = alpha A B + beta Cin + diag I while the next tile's first product is
@@ -47,7 +48,7 @@ namespace negf {
 namespace oz {
 constexpr int S = 7;             // base-256 digits per operand
 constexpr int NP = 3;            // real products (3M)
-constexpr int ND = 8;            // digit diagonals D = i + j = 0..7 (34 digit pairs)
+constexpr int ND = 7;            // digit diagonals D = i + j = 0..6 (28 digit pairs)
 constexpr int TM = 128, TN = 64, KC = 32;
 constexpr int A_SLICE = TM * KC;        // 4096 bytes
 constexpr int B_SLICE = TN * KC;        // 2048 bytes
@@ -57,7 +58,7 @@ constexpr int STAGE = A_BLOCK + B_BLOCK;
 constexpr int STAGES = 5;
 constexpr int THREADS = 256;            // 8 warps drain; lane 0 of warps 0 / 1 also issue MMAs / loads
 constexpr int DRAIN_WARPS = 8;
-constexpr int TMEM_COLS = 512;          // ND x TN
+constexpr int TMEM_COLS = 512;          // >= ND x TN (allocations are powers of two)
 constexpr long long WAIT_CYCLES = 2000000000LL;  // ~1 s at 1.9 GHz per wait
 constexpr int SPLIT_ROWS = 64;          // rows per split CTA
 // offset that turns the six lower bytes of x + C6 into digits + 128:
@@ -65,7 +66,7 @@ constexpr int SPLIT_ROWS = 64;          // rows per split CTA
 constexpr long long C6 = 128LL * ((1LL << 48) - 1) / 255;
 }  // namespace oz
 
-// weight 2^(-12 - 8D) of digit diagonal D = 0..7 (a compile-time constant)
+// weight 2^(-12 - 8D) of digit diagonal D = 0..6 (a compile-time constant)
 __host__ __device__ constexpr double oz_diag_weight(int D) {
   double w = 0x1p-12;
   for (int d = 0; d < D; ++d) w *= 0x1p-8;
@@ -445,21 +446,19 @@ __device__ __forceinline__ void oz_mma(uint32_t tmem, uint64_t dA0, uint64_t dB0
       "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
 }
 
-// The 34 digit pairs (i + j <= 7) of a stage as 12 MMAs; the order makes every
-// accumulator's first write an INIT one.
+// The 28 digit pairs (i + j <= 6) of a stage as 10 MMAs; the first two write
+// every accumulator first (INIT on the first K chunk of a product).
 __device__ __forceinline__ void oz_stage_mmas(uint32_t tmem, uint64_t dA0, uint64_t dB0, bool first_chunk) {
   oz_mma<0, 0, 4, 1>(tmem, dA0, dB0, first_chunk);
   oz_mma<0, 4, 3, 1>(tmem, dA0, dB0, first_chunk);
   oz_mma<1, 0, 4, 0>(tmem, dA0, dB0, first_chunk);
   oz_mma<1, 4, 2, 0>(tmem, dA0, dB0, first_chunk);
-  oz_mma<1, 6, 1, 1>(tmem, dA0, dB0, first_chunk);
   oz_mma<2, 0, 4, 0>(tmem, dA0, dB0, first_chunk);
-  oz_mma<2, 4, 2, 0>(tmem, dA0, dB0, first_chunk);
+  oz_mma<2, 4, 1, 0>(tmem, dA0, dB0, first_chunk);
   oz_mma<3, 0, 4, 0>(tmem, dA0, dB0, first_chunk);
-  oz_mma<3, 4, 1, 0>(tmem, dA0, dB0, first_chunk);
-  oz_mma<4, 0, 4, 0>(tmem, dA0, dB0, first_chunk);
-  oz_mma<5, 0, 3, 0>(tmem, dA0, dB0, first_chunk);
-  oz_mma<6, 0, 2, 0>(tmem, dA0, dB0, first_chunk);
+  oz_mma<4, 0, 3, 0>(tmem, dA0, dB0, first_chunk);
+  oz_mma<5, 0, 2, 0>(tmem, dA0, dB0, first_chunk);
+  oz_mma<6, 0, 1, 0>(tmem, dA0, dB0, first_chunk);
 }
 
 // Persistent: CTA b computes tiles b, b + G, b + 2G, ... (G = gridDim.x); the
@@ -669,10 +668,12 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
 #pragma unroll
         for (int j = 0; j < 8; ++j) v[j] = 0.0;
 #pragma unroll
-        for (int g = 0; g < ND / 4; ++g) {  // four diagonals per TMEM round trip
-          uint32_t x[4][8];
+        for (int g = 0; g < (ND + 3) / 4; ++g) {  // up to four diagonals per TMEM round trip
+          constexpr int kMax = 4;
+          const int nd = ND - 4 * g < kMax ? ND - 4 * g : kMax;
+          uint32_t x[kMax][8];
 #pragma unroll
-          for (int dd = 0; dd < 4; ++dd) {
+          for (int dd = 0; dd < nd; ++dd) {
             const int d = 4 * g + dd;
             const uint32_t addr = tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(d * TN + hh * 32 + c8 * 8);
             asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
@@ -682,7 +683,7 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
           }
           asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-          for (int dd = 0; dd < 4; ++dd) {
+          for (int dd = 0; dd < nd; ++dd) {
             const double w = oz_diag_weight(4 * g + dd);
 #pragma unroll
             for (int j = 0; j < 8; ++j) v[j] = fma(oz_i2d(x[dd][j]), w, v[j]);

@@ -1,5 +1,6 @@
-// Batched complex FP64 LU with partial pivoting (LAPACK getrf semantics) and
-// triangular inverses of the factors.
+// Batched complex FP64 LU with partial pivoting (LAPACK getrf semantics) or
+// without row interchanges (lu(A, NoPivot())), and triangular inverses of the
+// factors.
 //
 // Used by the selected inverse (the reference's be_getrf! / be_trsm! /
 // be_getri!, src/backend_cpu.jl:229-265, called from
@@ -41,6 +42,13 @@ __global__ void __launch_bounds__(LU_THREADS)
   }
   __syncthreads();
   for (int c = 0; c < w; ++c) {
+    if (p.nopiv) {  // block-uniform branch: lu(A, NoPivot())
+      if (tid == 0) {
+        *sp = c;
+        if (cabs1(S[(size_t)c * h + c]) <= 0.0 && p.info) atomicCAS(p.info, 0, k0 + c + 1);
+      }
+      __syncthreads();
+    } else {
     double bv = -1.0;
     int br = -1;
     for (int r = c + tid; r < h; r += LU_THREADS) {
@@ -71,6 +79,7 @@ __global__ void __launch_bounds__(LU_THREADS)
       }
     }
     __syncthreads();
+    }
     const int pr = *sp;
     if (tid == 0) p.ipiv[k0 + c] = k0 + pr;
     if (pr != c)

@@ -41,6 +41,9 @@ class SolveOpts(ctypes.Structure):
 
 NEGF_PREC_FP64 = 0
 NEGF_PREC_MIXED = 1
+NEGF_METHOD_RGF = 0
+NEGF_METHOD_DDRGF = 1
+NEGF_METHOD_SELINV = 2
 
 
 class CCscMatrix(ctypes.Structure):
@@ -58,6 +61,8 @@ PROTOTYPES = {
                                                 ctypes.POINTER(ZGemmProblem), ctypes.c_void_p]),
     "negf_zcopy_batched": (ctypes.c_int, [ctypes.c_char, ctypes.c_int32, c_int32_p, c_int32_p, c_void_pp, c_int32_p,
                                           c_void_pp, c_int32_p, ctypes.c_void_p]),
+    "negf_zfill_batched": (ctypes.c_int, [ctypes.c_int32, c_int32_p, c_int32_p, c_void_pp, c_int32_p, c_double_p,
+                                          ctypes.c_void_p]),
     "negf_zinv_batched": (ctypes.c_int, [ctypes.c_int32, c_int32_p, c_void_pp, c_int32_p, c_void_pp, c_int32_p,
                                          c_int32_p, ctypes.c_void_p]),
     "negf_zinv_batched_noalloc": (ctypes.c_int, [ctypes.c_int32, c_int32_p, c_void_pp, c_int32_p, c_void_pp,
@@ -78,6 +83,16 @@ PROTOTYPES = {
                                              ctypes.c_int32, ctypes.c_void_p]),
     "negf_ddrgf": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, c_int32_p, c_void_pp, c_void_pp, c_void_pp,
                                   ctypes.c_int32, c_void_pp, c_void_pp, c_void_pp, ctypes.c_void_p]),
+    "negf_selected_inverse_batched": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, c_void_pp,
+                                                     ctypes.POINTER(ctypes.c_uint8), ctypes.c_int32, ctypes.c_int32,
+                                                     ctypes.c_int32, ctypes.c_void_p]),
+    "negf_ddrgf_levels_ex": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, c_int32_p, c_void_pp, c_void_pp,
+                                            c_void_pp, ctypes.c_int32, c_int32_p, c_void_pp, c_void_pp, c_void_pp,
+                                            ctypes.c_int32, ctypes.c_void_p]),
+    "negf_device_selected_inverse": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, c_double_p,
+                                                    ctypes.POINTER(SolveOpts), ctypes.c_int32, ctypes.c_int32,
+                                                    c_int32_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                    ctypes.c_int32, ctypes.c_void_p]),
     "negf_ddrgf_get_nr_tasks": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, c_int32_p, c_int32_p]),
     "negf_ddrgf_choose_d1": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, c_int32_p]),
     "negf_ddrgf_levels": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, c_int32_p, c_void_pp, c_void_pp, c_void_pp,

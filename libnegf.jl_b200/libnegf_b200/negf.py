@@ -105,6 +105,46 @@ class Device:
                                 t.ctypes.data_as(_lib.c_double_p) if t is not None else None, 0, None))
         return self._split(gr, nE), self._split(gl, nE), t
 
+    def selected_inverse(self, energies, method="ddrgf", precision="fp64", eta=1e-6, levels=None, max_chunk=0,
+                         want=("d", "u", "l")):
+        """Blocks (i,i), (i,i+1), (i+1,i) of G^R(E) = M(E)^{-1} for every energy
+        (negf_device_selected_inverse): method "rgf", "ddrgf" (levels: interior
+        sizes per level, None = the library's cost model) or "selinv" (block LU
+        selected inverse, no pivoting inside blocks).
+
+        Returns (d, u, l): per energy lists of blocks (None where not wanted)."""
+        E = np.ascontiguousarray(np.asarray(energies, dtype=np.float64))
+        nE = len(E)
+        sd = sum(b * b for b in self.sizes)
+        su = sum(self.sizes[i] * self.sizes[i + 1] for i in range(self.npl - 1))
+        gd = np.empty(nE * sd, dtype=np.complex128) if "d" in want else None
+        gu = np.empty(max(1, nE * su), dtype=np.complex128) if "u" in want and su else None
+        gl = np.empty(max(1, nE * su), dtype=np.complex128) if "l" in want and su else None
+        o = make_opts(eta, max_chunk=max_chunk, precision=precision)
+        m = {"rgf": _lib.NEGF_METHOD_RGF, "ddrgf": _lib.NEGF_METHOD_DDRGF, "selinv": _lib.NEGF_METHOD_SELINV}[method]
+        lv = list(levels) if levels else []
+        check(load().negf_device_selected_inverse(self._handle, nE, E.ctypes.data_as(_lib.c_double_p), ctypes.byref(o),
+                                                  m, len(lv), int_array(lv) if lv else None,
+                                                  gd.ctypes.data if gd is not None else None,
+                                                  gu.ctypes.data if gu is not None else None,
+                                                  gl.ctypes.data if gl is not None else None, 0, None))
+
+        def split(flat, shapes):
+            if flat is None:
+                return None
+            out = []
+            for e in range(nE):
+                o, row = e * sum(r * c for r, c in shapes), []
+                for r, c in shapes:
+                    row.append(flat[o:o + r * c].reshape(r, c, order="F"))
+                    o += r * c
+                out.append(row)
+            return out
+
+        b = self.sizes
+        return (split(gd, [(x, x) for x in b]), split(gu, [(b[i], b[i + 1]) for i in range(self.npl - 1)]),
+                split(gl, [(b[i + 1], b[i]) for i in range(self.npl - 1)]))
+
     def _split(self, flat, nE):
         if flat is None:
             return None

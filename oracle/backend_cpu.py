@@ -65,6 +65,25 @@ def be_getrf(A):
     return lu
 
 
+def lu_nopivot(A):
+    """lu(A, NoPivot()) -- the factorisation ``selected_inverse.jl:17`` names and
+    ``test_selected_inverse.jl`` checks against -- as packed L\\U factors
+    (unit lower L), by right-looking elimination in blocks of 32 columns."""
+    F = np.array(A, dtype=np.complex128)
+    n = F.shape[0]
+    nb = 32
+    for k0 in range(0, n, nb):
+        k1 = min(n, k0 + nb)
+        for k in range(k0, k1):
+            F[k + 1:, k] /= F[k, k]
+            F[k + 1:, k + 1:k1] -= np.outer(F[k + 1:, k], F[k, k + 1:k1])
+        if k1 < n:
+            L11 = np.tril(F[k0:k1, k0:k1], -1) + np.eye(k1 - k0)
+            F[k0:k1, k1:] = blas.ztrsm(1.0, L11, F[k0:k1, k1:], side=0, lower=1, diag=1)
+            F[k1:, k1:] -= F[k1:, k0:k1] @ F[k0:k1, k1:]
+    return F
+
+
 def be_trsm(side, ul, tA, dA, alpha, A, B):
     """``be_trsm!`` (backend_cpu.jl:241-253): ztrsm."""
     return blas.ztrsm(alpha, A, np.asarray(B, dtype=np.complex128),

@@ -14,13 +14,15 @@ unassigned entries absent); arithmetic is complex128.
 
 import numpy as np
 
-from .backend_cpu import be_getrf, be_trsm, be_gemm, be_getri
+from .backend_cpu import be_getrf, be_trsm, be_gemm, be_getri, lu_nopivot
 
 
-def block_factorization(A_in, npl):
+def block_factorization(A_in, npl, nopivot=False):
+    """``nopivot``: factor the diagonal blocks by lu(NoPivot()) (the
+    factorisation selected_inverse.jl:17 names) instead of be_getrf!."""
     A = {k: np.array(v, dtype=np.complex128) for k, v in A_in.items()}
     for i in range(npl):
-        A[(i, i)] = be_getrf(A[(i, i)])                                           # :18
+        A[(i, i)] = lu_nopivot(A[(i, i)]) if nopivot else be_getrf(A[(i, i)])     # :18
         for j in range(i + 1, npl):
             if (j, i) in A:
                 A[(j, i)] = be_trsm("R", "U", "N", "N", 1.0, A[(i, i)], A[(j, i)])  # :23
