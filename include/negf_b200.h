@@ -449,19 +449,25 @@ int negf_probe_int8_peak(double* tops);
  * Request server.  The reference has no request loop (one system and one
  * energy per call); this batches whole NEGF solves (RGF + RKD +
  * transmission: src/matinvertndiag_rgf.jl:114-200, src/keldyshndiag.jl:
- * 120-317) submitted from any thread of any host language.  A worker thread
- * takes the queued requests first in, first out, as many as fit an HBM budget
- * (negf_batch_bytes estimates; budget_gb <= 0: 80 % of free memory when a
- * group forms) and solves them as one batch plan.  A group that fails to
- * allocate is halved, one that fails otherwise is re-solved request by
- * request, and a single request above the budget goes through negf_solve,
- * which splits its energies.  opts gives eta, mu_l, mu_r, kT, precision and
- * the schedule knobs; the want_* flags follow each request's non-NULL
- * outputs; sigma_per_energy must be 0.  The server keeps a few bytes per
- * ticket (status, latency) until it is destroyed.
+ * 120-317) submitted from any thread of any host language, continuously:
+ * `lanes` worker threads, each with its own CUDA stream, admit queued
+ * requests first in, first out, whenever the HBM budget (negf_batch_bytes
+ * estimates; budget_gb <= 0: 80 % of the memory free at creation) has room
+ * for them beside the groups already in flight, and solve each admitted group
+ * as one batch plan.  A request that arrives while others are on the GPU
+ * therefore starts as soon as memory allows and runs beside them.  A group
+ * that fails to allocate is halved, one that fails otherwise is re-solved
+ * request by request, and a single request above the budget goes through
+ * negf_solve, which splits its energies.  opts gives eta, mu_l, mu_r, kT,
+ * precision and the schedule knobs; the want_* flags follow each request's
+ * non-NULL outputs; sigma_per_energy must be 0.  The server keeps a few bytes
+ * per ticket (status, latency) until it is destroyed.
  * ---------------------------------------------------------------------- */
 typedef struct negf_server_s* negf_server_t;
+/* Two lanes. */
 int negf_server_create(const negf_solve_opts* opts, double budget_gb, negf_server_t* out);
+/* lanes in [1, 16] (1: one group at a time). */
+int negf_server_create_ex(const negf_solve_opts* opts, double budget_gb, int32_t lanes, negf_server_t* out);
 /* Upload the device (host blocks as negf_device_create; the caller may free
  * them on return) and queue nE energies.  gr_out / gl_out (nE * sum b_i^2
  * complex128, energy-major then layer, each block column-major) and t_out
@@ -474,14 +480,19 @@ int negf_server_submit(negf_server_t srv, int32_t npl, const int32_t* block_size
  * the request's status (NEGF_SUCCESS while pending). */
 int negf_server_poll(negf_server_t srv, int64_t ticket, int32_t* done);
 /* Wait at most timeout_s seconds: the request's status, or NEGF_ERR_TIMEOUT;
- * latency_s (may be NULL) receives submission-to-completion seconds. */
+ * latency_s (may be NULL) receives the seconds from the entry into
+ * negf_server_submit to completion. */
 int negf_server_wait(negf_server_t srv, int64_t ticket, double timeout_s, double* latency_s);
 /* Completed requests, groups solved, and the p50 / p99 latency (seconds) of
  * the completed requests. */
 int negf_server_stats(negf_server_t srv, int64_t* completed, int64_t* groups, double* p50_s, double* p99_s);
-/* Finish the queued requests, stop the worker, free the server. */
+/* Requests waiting, groups on the GPU now, the most groups ever on the GPU at
+ * once, and the byte estimate (GB) of the groups on the GPU. */
+int negf_server_stats_ex(negf_server_t srv, int64_t* queued, int32_t* inflight_groups,
+                         int32_t* peak_inflight_groups, double* inflight_gb);
+/* Finish the queued requests, stop the lanes, free the server. */
 int negf_server_destroy(negf_server_t srv);
-/* The worker's grouping rule (host only): requests in order, each group as
+/* The grouping rule for an idle server (host only): requests in order, each group as
  * many as fit budget bytes (a request above it alone); sizes receives the
  * group sizes (room for nreq), ngroups their count. */
 int negf_server_group_sizes(int32_t nreq, const int64_t* bytes, double budget, int32_t* sizes, int32_t* ngroups);

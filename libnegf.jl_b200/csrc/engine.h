@@ -295,3 +295,11 @@ std::string& last_error();
 void set_error(const std::string& msg);
 
 }  // namespace negf
+
+struct negf_solver_s;
+namespace negf {
+// One pass of a solver launch by launch on `stream`, without graph capture
+// (negf_api.cu): for one-off plans such as a request-server group's.
+int solver_run_direct(negf_solver_s* s, cudaStream_t stream);
+
+}  // namespace negf

@@ -966,6 +966,19 @@ int negf_solver_run(negf_solver_t s, void* stream) {
   return NEGF_SUCCESS;
 }
 
+extern "C++" {
+namespace negf {
+// One pass launch by launch on `stream` (no graph capture: for one-off plans
+// such as a server group's).
+int solver_run_direct(negf_solver_s* s, cudaStream_t stream) {
+  if (!s) return fail(NEGF_ERR_INVALID, "NULL solver");
+  cudaError_t e = s->plan->run(stream, false);
+  if (e != cudaSuccess) return cuda_fail(e, "negf_solver_run");
+  return NEGF_SUCCESS;
+}
+}  // namespace negf
+}  // extern "C++"
+
 int negf_solver_run_profiled(negf_solver_t s, void* stream) {
   if (!s) return fail(NEGF_ERR_INVALID, "NULL solver");
   const size_t need = s->plan->steps.size() + 1;

@@ -4,16 +4,20 @@
 // The reference has no request loop: it solves one system and one energy per
 // call (src/matinvertndiag_rgf.jl:114-200, src/keldyshndiag.jl:120-317).  A
 // request here is one device (H blocks, Sigma_L, Sigma_R) with a list of
-// energies and host output buffers.  submit() uploads the device and queues
-// the request.  A worker thread takes the queued requests first in, first
-// out, as many as fit an HBM budget by the library's own estimate
-// (negf_batch_bytes), and solves them as one batch plan
-// (negf_solver_create_batch: one launch per recursion step over every
-// (device, energy) pair).  It copies each request's G^R / G^< diagonal blocks
-// and T(E) into the caller's buffers, and marks the request done with its
-// latency (submission to completion).  A group that fails to allocate is
-// halved; a single request larger than the budget runs through negf_solve,
-// which splits its energies.
+// energies and host output buffers.  submit() stamps the arrival, uploads the
+// device and queues the request.  Several lanes -- worker threads, each with
+// its own non-blocking CUDA stream -- admit work continuously: whenever the
+// HBM budget has room (the library's own estimate, negf_batch_bytes, of every
+// group in flight is counted against it), a free lane takes the queued
+// requests first in, first out, as many as fit the room left, and solves them
+// as one batch plan (negf_solver_create_batch: one launch per recursion step
+// over every (device, energy) pair) on its stream.  So a request that arrives
+// while other groups are on the GPU starts as soon as memory allows, and its
+// launches overlap theirs on the device.  Each lane copies its requests'
+// G^R / G^< diagonal blocks and T(E) into the callers' buffers on its own
+// stream and marks them done with their latency (arrival to completion).  A
+// group that fails to allocate is halved; a single request larger than the
+// budget runs alone through negf_solve, which splits its energies.
 #include "../../include/negf_b200.h"
 #include "engine.h"
 
@@ -34,6 +38,7 @@ using Clock = std::chrono::steady_clock;
 
 struct Request {
   int64_t ticket = 0;
+  int64_t bytes = 0;  // negf_batch_bytes estimate of the request alone
   negf_device_t dev = nullptr;
   std::vector<int32_t> sizes;
   std::vector<double> energies;
@@ -60,7 +65,9 @@ size_t per_energy(const std::vector<int32_t>& sizes) {
 struct negf_server_s {
   negf_solve_opts opts{};
   double budget_gb = 0.0;
+  double budget = 0.0;        // bytes every group in flight shares
   int device = 0;
+  int lanes = 2;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<std::unique_ptr<Request>> queue;
@@ -68,8 +75,11 @@ struct negf_server_s {
   std::vector<double> latencies;
   int64_t next_ticket = 1;
   int64_t groups = 0;
+  double inflight_bytes = 0.0;  // estimates of the groups being solved
+  int inflight_groups = 0;
+  int peak_inflight = 0;        // most groups ever solved at once
   bool stop = false;
-  std::thread worker;
+  std::vector<std::thread> workers;
 };
 
 namespace {
@@ -93,39 +103,40 @@ std::vector<int> group_sizes(const std::vector<int64_t>& bytes, double budget) {
   return out;
 }
 
-double budget_bytes(const negf_server_s& S) {
-  if (S.budget_gb > 0.0) return S.budget_gb * 1e9;
-  size_t fr = 0, tot = 0;
-  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return 0.0;
-  return 0.8 * (double)fr;
-}
-
-// Copy request outputs out of a finished batch solver (device-major layout).
-int deliver(negf_solver_t s, const std::vector<Request*>& group) {
+// Copy request outputs out of a finished batch solver (device-major layout)
+// on the lane's stream, then wait for them.
+int deliver(negf_solver_t s, const std::vector<Request*>& group, cudaStream_t st) {
   void *gr = nullptr, *gl = nullptr;
   double* t2 = nullptr;
   if (int r = negf_solver_outputs(s, &gr, &gl, &t2)) return r;
-  size_t off = 0, e0 = 0;
+  size_t off = 0, e0 = 0, nt = 0;
+  for (Request* q : group) nt += q->energies.size();
+  std::vector<double> tt(2 * nt);
+  if (t2 && cudaMemcpyAsync(tt.data(), t2, 2 * nt * sizeof(double), cudaMemcpyDeviceToHost, st))
+    return NEGF_ERR_CUDA;
   for (Request* q : group) {
     const size_t n = q->energies.size(), per = per_energy(q->sizes), bytes = n * per * sizeof(negf::cplx);
-    if (q->gr && gr && cudaMemcpy(q->gr, static_cast<negf::cplx*>(gr) + off, bytes, cudaMemcpyDeviceToHost))
+    if (q->gr && gr &&
+        cudaMemcpyAsync(q->gr, static_cast<negf::cplx*>(gr) + off, bytes, cudaMemcpyDeviceToHost, st))
       return NEGF_ERR_CUDA;
-    if (q->gl && gl && cudaMemcpy(q->gl, static_cast<negf::cplx*>(gl) + off, bytes, cudaMemcpyDeviceToHost))
+    if (q->gl && gl &&
+        cudaMemcpyAsync(q->gl, static_cast<negf::cplx*>(gl) + off, bytes, cudaMemcpyDeviceToHost, st))
       return NEGF_ERR_CUDA;
-    if (q->t && t2) {
-      std::vector<double> tt(2 * n);
-      if (cudaMemcpy(tt.data(), t2 + 2 * e0, 2 * n * sizeof(double), cudaMemcpyDeviceToHost)) return NEGF_ERR_CUDA;
-      for (size_t e = 0; e < n; ++e) q->t[e] = tt[2 * e];
-    }
     off += n * per;
+  }
+  if (cudaStreamSynchronize(st) != cudaSuccess) return NEGF_ERR_CUDA;
+  for (Request* q : group) {
+    const size_t n = q->energies.size();
+    if (q->t && t2)
+      for (size_t e = 0; e < n; ++e) q->t[e] = tt[2 * (e0 + e)];
     e0 += n;
   }
   return NEGF_SUCCESS;
 }
 
-// Solve a group as one batch plan; NEGF_ERR_NOMEM is returned to the caller
-// (which halves the group) only for groups of two or more requests.
-int solve_group(negf_server_s& S, const std::vector<Request*>& group) {
+// Solve a group as one batch plan on stream st; NEGF_ERR_NOMEM is returned to
+// the caller (which halves the group) only for groups of two or more requests.
+int solve_group(negf_server_s& S, const std::vector<Request*>& group, cudaStream_t st) {
   negf_solve_opts o = S.opts;
   o.want_gr = o.want_gl = o.want_t = 0;
   for (Request* q : group) {
@@ -136,8 +147,8 @@ int solve_group(negf_server_s& S, const std::vector<Request*>& group) {
   if (group.size() == 1) {
     // negf_solve splits the energies of a request that does not fit at once
     Request* q = group[0];
-    o.hbm_budget_gb = S.budget_gb;
-    return negf_solve(q->dev, (int32_t)q->energies.size(), q->energies.data(), &o, q->gr, q->gl, q->t, 0, nullptr);
+    o.hbm_budget_gb = S.budget / 1e9;
+    return negf_solve(q->dev, (int32_t)q->energies.size(), q->energies.data(), &o, q->gr, q->gl, q->t, 0, st);
   }
   std::vector<negf_device_t> devs;
   std::vector<int32_t> counts;
@@ -149,11 +160,12 @@ int solve_group(negf_server_s& S, const std::vector<Request*>& group) {
   }
   negf_solver_t s = nullptr;
   if (int r = negf_solver_create_batch((int32_t)devs.size(), devs.data(), counts.data(), &o, &s)) return r;
-  int r = negf_solver_set_energies(s, E.data(), nullptr);
-  // the legacy stream replays the launches directly (no graph for a one-off plan)
-  if (r == NEGF_SUCCESS) r = negf_solver_run(s, nullptr);
+  int r = negf_solver_set_energies(s, E.data(), st);
+  // launches replayed directly on the lane's stream (no graph for a one-off plan)
+  if (r == NEGF_SUCCESS) r = negf::solver_run_direct(s, st);
+  if (r == NEGF_SUCCESS && cudaStreamSynchronize(st) != cudaSuccess) r = NEGF_ERR_CUDA;
   if (r == NEGF_SUCCESS) r = negf_solver_check(s);
-  if (r == NEGF_SUCCESS) r = deliver(s, group);
+  if (r == NEGF_SUCCESS) r = deliver(s, group, st);
   negf_solver_destroy(s);
   return r;
 }
@@ -172,32 +184,37 @@ void finish(negf_server_s& S, std::vector<std::unique_ptr<Request>>& reqs, int s
   S.cv_done.notify_all();
 }
 
-void worker_loop(negf_server_s* S) {
+// One lane: admit the queue's head group whenever the budget has room for it
+// next to the groups already in flight (or nothing runs), solve it on this
+// lane's stream, release its share of the budget.
+void lane_loop(negf_server_s* S) {
   cudaSetDevice(S->device);
+  cudaStream_t st = nullptr;
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) st = nullptr;
   for (;;) {
     std::vector<std::unique_ptr<Request>> taken;
+    double taken_bytes = 0.0;
     {
       std::unique_lock<std::mutex> lk(S->mu);
-      S->cv_work.wait(lk, [&] { return S->stop || !S->queue.empty(); });
-      if (S->queue.empty()) return;  // stopping with nothing left
-      std::vector<int64_t> bytes;
-      for (auto& q : S->queue) {
-        int64_t b = 0;
-        const int32_t n = (int32_t)q->energies.size();
-        if (negf_batch_bytes(1, &q->dev, &n, &S->opts, &b) != NEGF_SUCCESS) b = 0;
-        bytes.push_back(b);
-      }
-      const int n = group_sizes(bytes, budget_bytes(*S))[0];
-      for (int k = 0; k < n; ++k) {
+      S->cv_work.wait(lk, [&] {
+        if (S->queue.empty()) return S->stop;
+        return S->inflight_groups == 0 || S->inflight_bytes + (double)S->queue.front()->bytes <= S->budget;
+      });
+      if (S->queue.empty()) break;  // stopping with nothing left
+      const double room = S->budget - S->inflight_bytes;
+      do {
+        taken_bytes += (double)S->queue.front()->bytes;
         taken.push_back(std::move(S->queue.front()));
         S->queue.pop_front();
-      }
+      } while (!S->queue.empty() && taken_bytes + (double)S->queue.front()->bytes <= room);
+      S->inflight_bytes += taken_bytes;
+      S->peak_inflight = std::max(S->peak_inflight, ++S->inflight_groups);
     }
     // halve a group whose allocation fails; the second half goes back to the queue front
     for (;;) {
       std::vector<Request*> g;
       for (auto& q : taken) g.push_back(q.get());
-      const int r = solve_group(*S, g);
+      const int r = solve_group(*S, g, st);
       if (r == NEGF_ERR_NOMEM && taken.size() > 1) {
         const size_t half = taken.size() / 2;
         std::lock_guard<std::mutex> lk(S->mu);
@@ -213,7 +230,7 @@ void worker_loop(negf_server_s* S) {
         // one request's failure (a singular block, an unsupported shape) does not fail the others
         for (auto& q : taken) {
           std::vector<Request*> one{q.get()};
-          const int ri = solve_group(*S, one);
+          const int ri = solve_group(*S, one, st);
           std::vector<std::unique_ptr<Request>> v;
           v.push_back(std::move(q));
           finish(*S, v, ri);
@@ -223,7 +240,15 @@ void worker_loop(negf_server_s* S) {
       finish(*S, taken, r);
       break;
     }
+    {
+      std::lock_guard<std::mutex> lk(S->mu);
+      S->inflight_bytes -= taken_bytes;
+      --S->inflight_groups;
+    }
+    S->cv_work.notify_all();
   }
+  if (st) cudaStreamDestroy(st);
+  S->cv_work.notify_all();
 }
 
 }  // namespace
@@ -242,7 +267,11 @@ int negf_server_group_sizes(int32_t nreq, const int64_t* bytes, double budget, i
 }
 
 int negf_server_create(const negf_solve_opts* opts, double budget_gb, negf_server_t* out) {
-  if (!opts || !out) {
+  return negf_server_create_ex(opts, budget_gb, 2, out);
+}
+
+int negf_server_create_ex(const negf_solve_opts* opts, double budget_gb, int32_t lanes, negf_server_t* out) {
+  if (!opts || !out || lanes < 1 || lanes > 16) {
     negf::set_error("negf_server_create: bad arguments");
     return NEGF_ERR_INVALID;
   }
@@ -260,8 +289,15 @@ int negf_server_create(const negf_solve_opts* opts, double budget_gb, negf_serve
   auto* S = new negf_server_s();
   S->opts = *opts;
   S->budget_gb = budget_gb;
+  S->lanes = lanes;
   cudaGetDevice(&S->device);
-  S->worker = std::thread(worker_loop, S);
+  if (budget_gb > 0.0) {
+    S->budget = budget_gb * 1e9;
+  } else {
+    size_t fr = 0, tot = 0;
+    S->budget = cudaMemGetInfo(&fr, &tot) == cudaSuccess ? 0.8 * (double)fr : 0.0;
+  }
+  for (int k = 0; k < lanes; ++k) S->workers.emplace_back(lane_loop, S);
   *out = S;
   return NEGF_SUCCESS;
 }
@@ -274,6 +310,7 @@ int negf_server_submit(negf_server_t S, int32_t npl, const int32_t* block_sizes,
     negf::set_error("negf_server_submit: bad arguments");
     return NEGF_ERR_INVALID;
   }
+  const auto arrival = Clock::now();  // latency includes the upload below
   int cur = -1;
   if (cudaGetDevice(&cur) != cudaSuccess || cur != S->device) {
     negf::set_error("negf_server_submit: call with the server's device current (the device is uploaded there)");
@@ -286,7 +323,14 @@ int negf_server_submit(negf_server_t S, int32_t npl, const int32_t* block_sizes,
   q->gr = gr_out;
   q->gl = gl_out;
   q->t = t_out;
-  q->arrival = Clock::now();
+  q->arrival = arrival;
+  {
+    negf_solve_opts o = S->opts;
+    o.want_gr = gr_out != nullptr;
+    o.want_gl = gl_out != nullptr;
+    o.want_t = t_out != nullptr;
+    if (negf_batch_bytes(1, &q->dev, &nE, &o, &q->bytes) != NEGF_SUCCESS) q->bytes = 0;
+  }
   std::lock_guard<std::mutex> lk(S->mu);
   if (S->stop) {
     negf_device_destroy(q->dev);
@@ -370,8 +414,23 @@ int negf_server_destroy(negf_server_t S) {
     S->stop = true;
   }
   S->cv_work.notify_all();
-  if (S->worker.joinable()) S->worker.join();  // the worker finishes the queued requests first
+  for (auto& w : S->workers)
+    if (w.joinable()) w.join();  // the lanes finish the queued requests first
   delete S;
+  return NEGF_SUCCESS;
+}
+
+int negf_server_stats_ex(negf_server_t S, int64_t* queued, int32_t* inflight_groups, int32_t* peak_inflight_groups,
+                         double* inflight_gb) {
+  if (!S) {
+    negf::set_error("negf_server_stats_ex: bad arguments");
+    return NEGF_ERR_INVALID;
+  }
+  std::lock_guard<std::mutex> lk(S->mu);
+  if (queued) *queued = (int64_t)S->queue.size();
+  if (inflight_groups) *inflight_groups = S->inflight_groups;
+  if (peak_inflight_groups) *peak_inflight_groups = S->peak_inflight;
+  if (inflight_gb) *inflight_gb = S->inflight_bytes / 1e9;
   return NEGF_SUCCESS;
 }
 

@@ -100,6 +100,10 @@ PROTOTYPES = {
     "negf_ddrgf_choose_levels": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                                 c_int32_p, c_int32_p]),
     "negf_server_create": (ctypes.c_int, [ctypes.POINTER(SolveOpts), ctypes.c_double, ctypes.POINTER(ctypes.c_void_p)]),
+    "negf_server_create_ex": (ctypes.c_int, [ctypes.POINTER(SolveOpts), ctypes.c_double, ctypes.c_int32,
+                                             ctypes.POINTER(ctypes.c_void_p)]),
+    "negf_server_stats_ex": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), c_int32_p, c_int32_p,
+                                            c_double_p]),
     "negf_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, c_int32_p, c_void_pp, c_void_pp,
                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, c_double_p,
                                           ctypes.c_void_p, ctypes.c_void_p, c_double_p,

@@ -2,12 +2,15 @@
 
 A request is (H blocks, Sigma_L, Sigma_R, energy list); its Hamiltonian is
 uploaded once at submission and stays resident until the request completes.
-A worker thread batches continuously: whenever the GPU is free it takes the
-queued work FIFO -- (request, chunk of its energies) items, split so that one
-group's workspace fits the HBM budget (the library's own estimate,
+A worker thread batches whenever the GPU is free: it takes the queued work
+FIFO -- (request, chunk of its energies) items, split so that one group's
+workspace fits the HBM budget (the library's own estimate,
 ``negf_batch_bytes``) -- and solves the group as one ``BatchSolver`` (one
-launch per recursion step over every item) with autotuned schedule knobs.
-Requests arriving meanwhile join the next group.  A request completes when its
+launch per recursion step over every item) with autotuned schedule knobs
+(tuned once per group signature and cached).  Requests arriving meanwhile
+join the next group; this server runs one group at a time.  ``NativeServer``
+(the library's negf_server_*) runs several groups at once on separate
+streams, admitting new requests while others are on the GPU.  A request completes when its
 last chunk is done; its latency (arrival to completion) feeds the p50 / p99
 statistics.
 
@@ -83,6 +86,7 @@ class NegfServer:
         self.energy_points = 0
         self.device_ms = 0.0
         self._stream = torch.cuda.Stream()
+        self._tuned = {}  # schedule knobs per group signature
         self._worker = threading.Thread(target=self._loop, daemon=True)
         self._worker.start()
 
@@ -145,8 +149,12 @@ class NegfServer:
             devs = [r.device for r, _, _ in group]
             knobs = {}
             if self.tune:
-                from .autotune import autotune
-                knobs, _ = autotune(devs, [c for _, _, c in group], precision=self.precision, eta=self.phys["eta"])
+                from .autotune import autotune, signature
+                sig = signature(devs, self.precision)
+                if sig not in self._tuned:
+                    self._tuned[sig], _ = autotune(devs, [c for _, _, c in group], precision=self.precision,
+                                                   eta=self.phys["eta"])
+                knobs = self._tuned[sig]
             try:
                 try:
                     solver = BatchSolver(devs, [c for _, _, c in group], precision=self.precision,
@@ -212,19 +220,23 @@ class NegfServer:
 
 
 class NativeServer:
-    """The library's own request server (negf_server_*): the same FIFO,
-    budget-packed batching as ``NegfServer`` but run by a native worker
-    thread, so C and Julia callers get it too.  ``submit`` returns a ticket
-    object whose ``wait()`` gives (gr, gl, t) as host arrays."""
+    """The library's own request server (negf_server_*), for any host
+    language: ``lanes`` native worker threads, each with its own CUDA stream,
+    admit queued requests first in, first out, whenever the HBM budget has
+    room beside the groups already on the GPU, so requests that arrive while
+    others run start at once and their launches overlap (continuous
+    batching).  ``submit`` returns a ticket object whose ``wait()`` gives
+    (gr, gl, t) as host arrays."""
 
-    def __init__(self, budget_gb=0.0, **opts):
+    def __init__(self, budget_gb=0.0, lanes=2, **opts):
         import ctypes
         from . import _lib
         from .negf import make_opts
         self._lib = _lib
         o = make_opts(**opts)
         self._h = ctypes.c_void_p()
-        _lib.check(_lib.load().negf_server_create(ctypes.byref(o), float(budget_gb), ctypes.byref(self._h)))
+        _lib.check(_lib.load().negf_server_create_ex(ctypes.byref(o), float(budget_gb), int(lanes),
+                                                     ctypes.byref(self._h)))
 
     class Ticket:
         def __init__(self, server, tid, sizes, nE, keep):
@@ -288,7 +300,11 @@ class NativeServer:
         p50, p99 = ctypes.c_double(), ctypes.c_double()
         self._lib.check(self._lib.load().negf_server_stats(self._h, ctypes.byref(c), ctypes.byref(g),
                                                            ctypes.byref(p50), ctypes.byref(p99)))
-        return {"requests": c.value, "groups": g.value, "p50_s": p50.value, "p99_s": p99.value}
+        q, inf, peak, gb = ctypes.c_int64(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_double()
+        self._lib.check(self._lib.load().negf_server_stats_ex(self._h, ctypes.byref(q), ctypes.byref(inf),
+                                                              ctypes.byref(peak), ctypes.byref(gb)))
+        return {"requests": c.value, "groups": g.value, "p50_s": p50.value, "p99_s": p99.value, "queued": q.value,
+                "inflight_groups": inf.value, "peak_inflight_groups": peak.value, "inflight_gb": gb.value}
 
     def close(self):
         if self._h:
