@@ -14,16 +14,20 @@ One step = one pass of RGF (shared upward pass) + downward G^R + RKD + the
 transmission chain over all 256 energies, on device-resident inputs, replayed
 as one CUDA graph.  The headline is the mixed-precision path (Schur products on
 the INT8 tensor cores with FP64-grade digit splitting; inversions in FP64),
-checked block by block against the FP64 path's outputs (bar 1e-10); the FP64
-path is timed beside it ("fp64_path").
+checked block by block against the FP64 path's outputs on every 8th energy
+(bar 1e-10) and, on four energies, both paths against the oracle
+("accuracy_vs_oracle"); the FP64 path is timed beside it ("fp64_path").  The
+p50 / p99 solve latency comes from a short Poisson request stream through the
+library's request server (continuous batching, mixed precision, "serving").
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--workload cfg2|cfg3|cfg4|cfg5]
 
-Multi-GPU: one process per GPU (torchrun); every rank solves its own 256
-energies (weak scaling, no data-path collective); the time is the max over
-ranks.  ``--impl reference`` times the CPU restatement of the reference's
-algorithm (the oracle: LibNEGF.jl itself is Julia and cannot run here) on the
-host cores.
+Multi-GPU: one process per GPU (torchrun; --gpus N without a launcher starts
+the N ranks itself); every rank solves its own 256 energies (weak scaling, no
+data-path collective); the time is the max over ranks.  ``--impl reference``
+times the CPU restatement of the reference's algorithm (the oracle: LibNEGF.jl
+itself is Julia and cannot run here) on the host cores.
 """
 
 import argparse
@@ -58,6 +62,9 @@ def parse():
     ap.add_argument("--cpu-budget-s", type=float, default=12.0, help="time budget of each CPU baseline mode")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="skip the request-stream latency sample")
+    ap.add_argument("--serve-requests", type=int, default=12, help="requests in the latency sample")
+    ap.add_argument("--serve-rate", type=float, default=4.0, help="arrival rate of the latency sample, requests/s")
     ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg3", "cfg4", "cfg5"],
                     help="cfg2 (default, the headline line); cfg4: a bounded sample of the uneven batch (systems "
                          "of N in U{8..96}, b in {32..384}, 16 energies each); cfg5: a bounded sample of the "
@@ -232,22 +239,28 @@ def run_reference(args):
     if rank != 0:
         return
     energies = np.linspace(-1.0, 1.0, args.ne)
-    vals = []
+    vals, walls = [], []
     cb = None
     for step in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
         r = cpu_baseline(args.npl, args.b, energies, budget_s=args.cpu_budget_s / 2)
         if step >= args.warmup:
             vals.append(r["value"])
+            walls.append(time.perf_counter() - t0)
             cb = r
     v = float(np.median(vals))
+    # a step is one bounded sample of the workload (both threading modes); its
+    # wall time is ms_per_step, its energies per second the value
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 * args.ne / v, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": 1000.0 * float(np.median(walls)), "higher_is_better": True,
+            "scaling": "weak",
             "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded numpy, the generator of the config)",
             "impl": "reference",
             "config": {"workload": WORKLOAD, "npl": args.npl, "b": args.b, "energies": args.ne, "precision": "fp64",
                        "note": "LibNEGF.jl is Julia and no Julia toolchain exists here: the reference arm times the "
                                "oracle, a numpy/scipy restatement of its LAPACK/BLAS call sequence; each step is a "
-                               "bounded sample of the workload's energies"},
+                               "bounded sample of the workload's energies (ms_per_step is that sample's wall time, "
+                               "value its energy points per second)"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cb["cores"], "kind": "port", "sample": cb["sample"]},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -256,17 +269,9 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # GPU arm
 
-# DRAM bytes (read + write) per launch of ozaki_mma_kernel, measured by ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum over one pass of the mixed
-# solver, N = 32, b = 256, 32 energies: 469 launches, 67.0 GB); recorded in
-# profiles/ozaki_mixed_cfg2_traffic.md.  A launch's tiles scale with the number
-# of energies, so a full launch of E energies moves E / 32 times as much.
-OZ_MMA_TRAFFIC_32 = {"npl": 32, "b": 256, "energies": 32, "bytes_per_launch": 142.7e6}
-
-
 def measured_hbm_gbs():
-    """HBM copy bandwidth of this pool's B200s (MEASURED_PEAKS.json at the
-    repository root), else the pool's earlier measurement."""
+    """Measured HBM copy bandwidth of the GPU (MEASURED_PEAKS.json at the
+    repository root), else an earlier measurement of 6.65 TB/s."""
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json)"
@@ -274,11 +279,44 @@ def measured_hbm_gbs():
         return 6650.0, "fallback (6.65 TB/s)"
 
 
-def oz_mma_traffic(npl, b, ne):
-    t = OZ_MMA_TRAFFIC_32
-    if npl != t["npl"] or b != t["b"]:
-        return None
-    return t["bytes_per_launch"] * ne / t["energies"]
+def _host_outputs(outs, ne, per, idx):
+    """Host copies of the G^R / G^< diagonal blocks (flat complex128) and T of
+    the energies idx from a solver's device outputs."""
+    import torch
+    res = []
+    for w in range(2):
+        v = _device_doubles(outs[w], 2 * ne * per).view(ne, 2 * per)[idx].cpu().numpy()
+        res.append(v.view(np.complex128))
+    res.append(_device_doubles(outs[2], 2 * ne)[0::2][torch.tensor(idx, device="cuda")].cpu().numpy())
+    return res
+
+
+def accuracy_vs_oracle(sysm, energies, idx, sizes, paths):
+    """Per-block relative Frobenius error of each path's G^R / G^< diagonal
+    blocks and |dT| / max(1, |T|) against the oracle (the reference's LAPACK
+    call sequence restated on the host) at the energies idx."""
+    from oracle import physics
+    out = {k: {"max_block_rel_err_GR": 0.0, "max_block_rel_err_GL": 0.0, "max_T_err": 0.0} for k in paths}
+    for j, e in enumerate(idx):
+        r = physics.solve_energy(sysm, energies[e])
+        o = 0
+        for i, b in enumerate(sizes):
+            gr_ref, gl_ref = r["GR"].M[(i, i)], 1j * r["Gn"].M[(i, i)]
+            for k, (gr, gl, t) in paths.items():
+                a = gr[j][o:o + b * b].reshape(b, b, order="F")
+                c = gl[j][o:o + b * b].reshape(b, b, order="F")
+                d = out[k]
+                d["max_block_rel_err_GR"] = max(d["max_block_rel_err_GR"],
+                                                float(np.linalg.norm(a - gr_ref) / np.linalg.norm(gr_ref)))
+                d["max_block_rel_err_GL"] = max(d["max_block_rel_err_GL"],
+                                                float(np.linalg.norm(c - gl_ref) / np.linalg.norm(gl_ref)))
+            o += b * b
+        for k, (gr, gl, t) in paths.items():
+            out[k]["max_T_err"] = max(out[k]["max_T_err"], float(abs(t[j] - r["T"]) / max(1.0, abs(r["T"]))))
+    for k in out:
+        out[k]["energies"] = [float(energies[e]) for e in idx]
+        out[k]["bar"] = 1e-10 if k == "mixed" else 1e-12
+    return out
 
 
 def run_ours(args):
@@ -397,6 +435,9 @@ def run_ours(args):
     outs = solver.outputs()
     refs = [_device_doubles(outs[w], 2 * args.ne * per).view(args.ne, 2 * per)[checked].clone() for w in range(2)]
     t_ref = _device_doubles(outs[2], 2 * args.ne)[0::2].clone()
+    # four energies checked against the oracle (host copies of both paths' blocks)
+    oidx = sorted({min(args.ne - 1, args.ne * k // 4 + args.ne // 8) for k in range(4)})
+    host_f64 = _host_outputs(outs, args.ne, per, oidx)
     solver.close()
 
     # ---- mixed path (the headline): INT8 tensor-core Schur products
@@ -420,6 +461,10 @@ def run_ours(args):
     t_mix = _device_doubles(outs[2], 2 * args.ne)[0::2]
     t_err = float(((t_mix - t_ref).abs() / t_ref.abs().clamp(min=1.0)).max())
     del refs, t_ref
+    host_mix = _host_outputs(outs, args.ne, per, oidx)
+    acc_oracle = None
+    if rank == 0:
+        acc_oracle = accuracy_vs_oracle(sysm, my_E, oidx, dev.sizes, {"mixed": host_mix, "fp64": host_f64})
 
     # dominant kernel: the INT8 product kernel; algorithmic work per launch =
     # 3 real products x 28 digit pairs x 2mnk int8 ops per complex product
@@ -438,10 +483,9 @@ def run_ours(args):
         achieved = (k_fl / k_n) / ((k_ms / k_n) / 1000.0) / 1e12 if k_n else 0.0
         roof = {"kernel": kind, "bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                 "frac": achieved / fp64_peak if fp64_peak else None}
-    roof["traffic"] = oz_mma_traffic(args.npl, args.b, args.ne) if kind == "oz_mma" else None
-    if roof["traffic"] is not None:
-        roof["traffic_note"] = ("ncu DRAM bytes per launch at 32 energies (profiles/ozaki_mixed_cfg2_traffic.md) "
-                                "scaled by energies / 32")
+    # DRAM bytes of the dominant kernel are an ncu measurement; this run is not
+    # under ncu, so the per-launch traffic is not reported here
+    roof["traffic"] = None
     roof["share"] = k_ms / sum(v[0] for v in prof.values())
     roof["launch_ms"] = k_ms / max(1, k_n)
     whole = {"algorithmic_tflops": step_flops / ((ms / args.steps) / 1000.0) / 1e12,
@@ -481,6 +525,15 @@ def run_ours(args):
         e2e = {"value": total_pts / el, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(2 * nbytes + 16 * args.ne), "ms_per_step": 1000 * el / args.steps}
 
+    # p50 / p99 solve latency of a short Poisson request stream through the
+    # library's request server (mixed precision, continuous batching)
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serving:
+        reqs, gaps = request_stream(args.serve_requests, args.serve_rate, 6, (16, 64), [64, 128, 192, 256], (16, 64))
+        serving = serve_stream(reqs, gaps, "mixed")
+        serving["workload"] = ("%d requests, N in {16..64}, b in {64..256}, 16..64 energies each, Poisson arrivals "
+                               "at %.1f/s" % (args.serve_requests, args.serve_rate))
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -493,6 +546,9 @@ def run_ours(args):
                                  (stats["workspace_bytes"] / 1e9)},
                 "accuracy_vs_fp64": {"max_block_rel_err_GR": errs[0], "max_block_rel_err_GL": errs[1],
                                      "max_T_err": t_err, "energies_checked": len(checked), "bar": 1e-10},
+                "accuracy_vs_oracle": acc_oracle,
+                "p50_s": serving["p50_s"] if serving else None, "p99_s": serving["p99_s"] if serving else None,
+                "serving": serving,
                 "roofline": roof, "kernels": breakdown_of(prof), "whole_step": whole, "clocks": clk.summary(),
                 "gpu_launches": int(stats["launches"]) * args.steps,
                 "e2e": e2e, "cpu_baseline": cpu, "fp64_path": fp64,
@@ -636,58 +692,86 @@ def run_cfg4(args):
         d.close()
 
 
-def run_cfg5(args):
-    """Request stream: seeded requests (N in {16..128}, b in {64..512}, energy
-    lists of 32..1024 scaled to a bounded sample) arriving as a Poisson process
-    at --rate, served by NegfServer; latency = arrival to completion."""
-    import torch
-    from libnegf_b200.server import NegfServer
+def request_stream(n_req, rate, seed, npl_range, b_choices, ne_range, ne_div=1):
+    """Seeded requests (N uniform in npl_range, b from b_choices, energy lists
+    of ne_range // ne_div points, the H / Sigma generator with a per-request
+    seed) and their Poisson inter-arrival gaps at `rate` requests/s."""
     from oracle import physics
-    rng = np.random.default_rng(5)
+    rng = np.random.default_rng(seed)
     reqs = []
-    for k in range(args.requests):
-        n = int(rng.integers(16, 129))
-        b = int(rng.choice([64, 128, 192, 256, 384, 512]))
-        ne = int(rng.integers(32, 1025)) // 8  # bounded sample: 1/8 of the energy-list length
-        s = physics.physics_system(n, b, seed=2000 + k)
+    for k in range(n_req):
+        n = int(rng.integers(npl_range[0], npl_range[1] + 1))
+        b = int(rng.choice(b_choices))
+        ne = max(1, int(rng.integers(ne_range[0], ne_range[1] + 1)) // ne_div)
+        s = physics.physics_system(n, b, seed=seed * 1000 + k)
         reqs.append((s, np.linspace(-0.9, 0.9, ne)))
-    gaps = rng.exponential(1.0 / args.rate, size=len(reqs))
-    srv = NegfServer(precision=args.precision, eta=1e-6)
-    # tune once per block-size class before the clock starts (a long-running
-    # server carries its tuning cache)
-    from libnegf_b200.autotune import autotune
-    from libnegf_b200.negf import Device
-    for b in sorted({len(s.Hd[0]) for s, _ in reqs}):
-        s0 = physics.physics_system(4, b, seed=1)
-        d0 = Device(s0.Hd, s0.Hu, s0.sigL, s0.sigR)
-        autotune([d0], [4], precision=args.precision)
-        d0.close()
-    handles = []
-    clk = ClockSampler(torch.cuda.current_device())
-    with clk:
+    return reqs, rng.exponential(1.0 / rate, size=n_req)
+
+
+def serve_stream(reqs, gaps, precision, lanes=2):
+    """Submit the requests at their arrival times to the library's request
+    server (negf_server_*, continuous batching over `lanes` streams) and wait
+    for all; latency = entry into submit to completion."""
+    from libnegf_b200.server import NativeServer
+    srv = NativeServer(lanes=lanes, precision=precision, eta=1e-6)
+    try:
+        tickets = []
         t0 = time.perf_counter()
         for (s, E), gap in zip(reqs, gaps):
             time.sleep(gap)
-            handles.append(srv.submit(s.Hd, s.Hu, s.sigL, s.sigR, E))
-        for h in handles:
-            h.wait(timeout=1800)
+            tickets.append(srv.submit(s.Hd, s.Hu, s.sigL, s.sigR, E, want_blocks=True))
+        for tk in tickets:
+            tk.wait(timeout=1800)
         wall = time.perf_counter() - t0
-    lat = srv.latency_stats()
+        st = srv.stats()
+    finally:
+        srv.close()
     pts = sum(len(E) for _, E in reqs)
-    print(json.dumps({"metric": "energy pts/s and p50/p99 solve latency (request stream)", "value": pts / wall,
-                      "unit": UNIT, "p50_s": lat["p50_s"], "p99_s": lat["p99_s"], "mean_latency_s": lat["mean_s"],
-                      "device_pts_per_s": pts / (srv.device_ms / 1000.0), "n_gpus": 1, "dtype": args.precision,
+    return {"pts_per_s": pts / wall, "p50_s": st["p50_s"], "p99_s": st["p99_s"], "requests": st["requests"],
+            "energy_points": pts, "wall_s": wall, "groups": st["groups"],
+            "peak_inflight_groups": st["peak_inflight_groups"], "lanes": lanes, "precision": precision}
+
+
+def run_cfg5(args):
+    """Request stream: seeded requests (N in {16..128}, b in {64..512}, energy
+    lists of 32..1024 scaled to a bounded sample) arriving as a Poisson process
+    at --rate, served by the library's request server (two lanes, continuous
+    batching) in FP64 and in the mixed precision mode; latency = entry into
+    submit to completion."""
+    import torch
+    reqs, gaps = request_stream(args.requests, args.rate, 5, (16, 128), [64, 128, 192, 256, 384, 512], (32, 1024),
+                                ne_div=8)
+    clk = ClockSampler(torch.cuda.current_device())
+    res = {}
+    with clk:
+        for precision in ("fp64", "mixed"):
+            res[precision] = serve_stream(reqs, gaps, precision)
+    print(json.dumps({"metric": "energy pts/s and p50/p99 solve latency (request stream)",
+                      "value": res["mixed"]["pts_per_s"], "unit": UNIT, "p50_s": res["mixed"]["p50_s"],
+                      "p99_s": res["mixed"]["p99_s"], "n_gpus": 1, "dtype": "int8 products / f64",
                       "data": "synthetic (seeded)",
                       "config": {"workload": "bounded sample of the request stream: %d requests, N in {16..128}, "
                                              "b in {64..512}, energy lists of 4..128 (1/8 of 32..1024), Poisson "
-                                             "arrivals at %.2f/s" % (len(reqs), args.rate),
-                                 "groups": srv.groups, "budget_gb": srv.budget / 1e9},
-                      "clocks": clk.summary()}), flush=True)
-    srv.close()
+                                             "arrivals at %.2f/s" % (len(reqs), args.rate)},
+                      "by_precision": res, "clocks": clk.summary()}), flush=True)
+
+
+def spawn_ranks(args):
+    """--gpus N without a launcher: start N ranks (one per GPU) through
+    torch.distributed.run on this node and return the launcher's exit code."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(args.gpus),
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.run(cmd).returncode
 
 
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(spawn_ranks(args))
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "cfg3":

@@ -38,7 +38,7 @@ extern "C" {
 #define NEGF_ERR_CUDA 2      /* CUDA runtime error / no device */
 #define NEGF_ERR_SINGULAR 3  /* zero pivot in a diagonal block */
 #define NEGF_ERR_NOMEM 4     /* device allocation failed */
-#define NEGF_ERR_TIMEOUT 5   /* a bounded wait ran out (negf_server_wait) */
+#define NEGF_ERR_TIMEOUT 5   /* a bounded wait ran out (negf_server_wait, tensor-core pipeline waits) */
 
 /* Message of the last failure on this thread ("" when none). */
 const char* negf_last_error(void);
@@ -70,6 +70,16 @@ int negf_zgemm_batched(char opA, char opB, int32_t nprob, const negf_zgemm_probl
  * digit splitting; see NEGF_PREC_MIXED).  Same problems; results agree with
  * the FP64 ones to ~1e-15 relative to |op(A)| |op(B)| (FP64-grade); k <= 1024. */
 int negf_zgemm_batched_mixed(char opA, char opB, int32_t nprob, const negf_zgemm_problem* probs, void* stream);
+
+/* Limit, in seconds, of each pipeline wait inside the mixed-precision product
+ * kernel (its mbarrier waits on copies, tensor-core completion and
+ * accumulator drains; seconds <= 0: the default, about 1 s).  A wait that
+ * runs out ends the kernel's work early: it waits for its own copies and
+ * tensor-core operations in flight, releases its tensor memory and returns,
+ * and the call reports NEGF_ERR_TIMEOUT; the CUDA context stays usable.
+ * Process-wide; applies to launches made after the call (a solver plan
+ * replayed from a CUDA graph keeps the limit of its capture). */
+int negf_set_tensor_wait_limit(double seconds);
 
 /* Batched be_copy_in_hw! / be_ctranspose! (src/backend_cpu.jl:42-68):
  * C[i] = op(A[i]) with op 'N' (copy) or 'C' (conjugate transpose); C[i] is

@@ -67,6 +67,8 @@ cudaError_t launch_csc_direct_out(int pass, int n, int npl, int wout, const int*
 // tile_map: per output tile an int4 (problem, m tile | n tile << 16,
 // K chunks | m tiles << 16, n tiles)
 cudaError_t launch_ozaki_mma(const void* probs, const void* tile_map, int total_tiles, int* err, cudaStream_t st);
+// pipeline wait limit (clock cycles) of product launches made from now on; <= 0: the default (~1 s)
+void ozaki_set_wait_cycles(long long cycles);
 
 // LU request (LAPACK getrf semantics, in place).  ipiv receives 0-based
 // global pivot rows; ipiv_lapack (optional, device int32) 1-based ones.

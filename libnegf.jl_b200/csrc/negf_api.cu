@@ -518,6 +518,13 @@ int negf_zgemm_batched(char opA, char opB, int32_t nprob, const negf_zgemm_probl
   }
 }
 
+int negf_set_tensor_wait_limit(double seconds) {
+  if (!(seconds == seconds)) return fail(NEGF_ERR_INVALID, "negf_set_tensor_wait_limit: NaN");
+  // clock64() runs at the SM clock (<= ~2 GHz on B200)
+  ozaki_set_wait_cycles(seconds > 0.0 ? std::max(64LL, (long long)std::min(seconds * 2e9, 4e18)) : 0LL);
+  return NEGF_SUCCESS;
+}
+
 int negf_zgemm_batched_mixed(char opA, char opB, int32_t nprob, const negf_zgemm_problem* probs, void* stream) {
   if (int r = check_device()) return r;
   if (nprob < 0 || (nprob > 0 && !probs)) return fail(NEGF_ERR_INVALID, "bad problem list");
@@ -547,7 +554,7 @@ int negf_zgemm_batched_mixed(char opA, char opB, int32_t nprob, const negf_zgemm
     if (plan.error_flag()) {
       int h = 0;
       NEGF_TRY_CUDA(cudaMemcpy(&h, plan.error_flag(), sizeof(int), cudaMemcpyDeviceToHost), "mixed gemm");
-      if (h) return fail(NEGF_ERR_CUDA, "negf_zgemm_batched_mixed: tensor-core completion wait timed out");
+      if (h) return fail(NEGF_ERR_TIMEOUT, "negf_zgemm_batched_mixed: tensor-core completion wait timed out");
     }
     return NEGF_SUCCESS;
   } catch (const std::bad_alloc&) {
@@ -1114,7 +1121,7 @@ int negf_solver_check(negf_solver_t s) {
   if (s->plan->error_flag()) {
     int fl = 0;
     NEGF_TRY_CUDA(cudaMemcpy(&fl, s->plan->error_flag(), sizeof(int), cudaMemcpyDeviceToHost), "solver check");
-    if (fl) return fail(NEGF_ERR_CUDA, "tensor-core completion wait timed out in the mixed-precision products");
+    if (fl) return fail(NEGF_ERR_TIMEOUT, "tensor-core completion wait timed out in the mixed-precision products");
   }
   for (int e = 0; e < s->nE; ++e)
     if (h[e]) {

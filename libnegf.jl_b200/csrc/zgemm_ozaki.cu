@@ -36,11 +36,14 @@
 //     registers, and at the end of a tile they write
 //     C = alpha A B + beta Cin + diag I while the next tile's first product is
 //     already on the tensor cores.
-// Every mbarrier wait is bounded: a role that times out records an error code
-// and raises an abort flag that ends the other roles' waits; the CTA then
-// waits (bounded) for its copies and MMAs in flight, releases TMEM and returns.
+// Every mbarrier wait is bounded: a role whose pipeline wait runs past the
+// limit (a kernel argument, default ~1 s) records an error code and raises an
+// abort flag that ends the other roles' waits; the CTA then waits (bounded by
+// the default limit) for its copies and MMAs in flight, releases TMEM and
+// returns, and the host reports the error.
 #include "negf_common.cuh"
 
+#include <atomic>
 #include <cstdint>
 
 namespace negf {
@@ -363,14 +366,14 @@ __device__ __forceinline__ bool oz_try(uint32_t mbar, uint32_t parity) {
 
 // Bounded wait for the completion of the mbarrier phase of the given parity.
 // Returns false when another role raised the abort flag (watch) or after
-// WAIT_CYCLES, in which case it raises the flag and records the error.
+// `limit` cycles, in which case it raises the flag and records the error.
 __device__ __forceinline__ bool oz_wait(uint32_t mbar, uint32_t parity, volatile int* abort_flag, int* err,
-                                        bool watch) {
+                                        bool watch, long long limit = oz::WAIT_CYCLES) {
   if (oz_try(mbar, parity)) return true;
   const long long t0 = clock64();
   while (!oz_try(mbar, parity)) {
     if (watch && *abort_flag) return false;
-    if (clock64() - t0 > oz::WAIT_CYCLES) {
+    if (clock64() - t0 > limit) {
       *abort_flag = 1;
       atomicExch(err, 1);
       return false;
@@ -382,7 +385,8 @@ __device__ __forceinline__ bool oz_wait(uint32_t mbar, uint32_t parity, volatile
 // The same wait for a whole warp that has nothing else to do: lane 0 polls
 // with a back-off, so that idle warps leave the issue slots to the thread that
 // feeds the tensor cores; the result is uniform across the warp.
-__device__ __forceinline__ bool oz_wait_warp(uint32_t mbar, uint32_t parity, volatile int* abort_flag, int* err) {
+__device__ __forceinline__ bool oz_wait_warp(uint32_t mbar, uint32_t parity, volatile int* abort_flag, int* err,
+                                             long long limit) {
   int ok = 0;
   if ((threadIdx.x & 31) == 0) {
     const long long t0 = clock64();
@@ -392,7 +396,7 @@ __device__ __forceinline__ bool oz_wait_warp(uint32_t mbar, uint32_t parity, vol
         break;
       }
       if (*abort_flag) break;
-      if (clock64() - t0 > oz::WAIT_CYCLES) {
+      if (clock64() - t0 > limit) {
         *abort_flag = 1;
         atomicExch(err, 1);
         break;
@@ -466,7 +470,7 @@ __device__ __forceinline__ void oz_stage_mmas(uint32_t tmem, uint64_t dA0, uint6
 // tile is issued before the epilogue of the current one.
 __global__ void __launch_bounds__(oz::THREADS, 1)
     ozaki_mma_kernel(const OzMmaProblem* __restrict__ probs, const int4* __restrict__ tile_map, int total_tiles,
-                     int* __restrict__ err) {
+                     int* __restrict__ err, long long wait_cycles) {
   using namespace oz;
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES], accf_bar, acce_bar, done_bar;
@@ -566,7 +570,7 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
   auto refill_product = [&](long long P) {
     if (P % NP == 0) rkch = oz_tile(tile_map, (int)blockIdx.x + (int)(P / NP) * G).kch;
     for (int c = 0; c < rkch; ++c) {
-      if (!oz_wait(empty0 + rs * 8, rph, abort_flag, err, true)) {
+      if (!oz_wait(empty0 + rs * 8, rph, abort_flag, err, true, wait_cycles)) {
         load_ok = false;
         return;
       }
@@ -587,7 +591,7 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
   uint32_t mph = 0;
   auto issue_upto = [&](long long P, int cend) {
     if (cur_P != P) {
-      if (P > 0 && !oz_wait(oz_smem(&acce_bar), (uint32_t)((P - 1) & 1), abort_flag, err, true)) {
+      if (P > 0 && !oz_wait(oz_smem(&acce_bar), (uint32_t)((P - 1) & 1), abort_flag, err, true, wait_cycles)) {
         mma_ok = false;
         return;
       }
@@ -599,7 +603,7 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
     const int c1 = cend < mkch ? cend : mkch;
     for (; cur_c < c1; ++cur_c) {
       const int c = cur_c;
-      if (!oz_wait(full0 + ms * 8, mph, abort_flag, err, true)) {
+      if (!oz_wait(full0 + ms * 8, mph, abort_flag, err, true, wait_cycles)) {
         mma_ok = false;
         return;
       }
@@ -651,7 +655,7 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
         my_scA = oz_pow2(my_eA);
         __syncwarp();
       }
-      if (!oz_wait_warp(oz_smem(&accf_bar), (uint32_t)(P & 1), abort_flag, err)) {
+      if (!oz_wait_warp(oz_smem(&accf_bar), (uint32_t)(P & 1), abort_flag, err, wait_cycles)) {
         ok = false;
         break;
       }
@@ -765,7 +769,8 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
     }
   }
   // all MMAs of this CTA complete, and every issued copy has landed, before
-  // TMEM is released and the CTA exits
+  // TMEM is released and the CTA exits; these waits keep the default limit
+  // (work already issued always completes), also after an abort
   if (mma_thread) {
     oz_commit(oz_smem(&done_bar));
     oz_wait(oz_smem(&done_bar), 0, abort_flag, err, false);
@@ -910,6 +915,12 @@ cudaError_t launch_ozaki_split(const void* probs, int nprob, int max_rows_pad, i
   return cudaGetLastError();
 }
 
+// Pipeline wait limit of the product kernel in clock cycles (process-wide;
+// negf_set_tensor_wait_limit).
+static std::atomic<long long> g_oz_wait_cycles{oz::WAIT_CYCLES};
+
+void ozaki_set_wait_cycles(long long cycles) { g_oz_wait_cycles.store(cycles > 0 ? cycles : oz::WAIT_CYCLES); }
+
 cudaError_t launch_ozaki_mma(const void* probs, const void* tile_map, int total_tiles, int* err, cudaStream_t st) {
   if (total_tiles <= 0) return cudaSuccess;
   static int sms = 0;
@@ -921,7 +932,8 @@ cudaError_t launch_ozaki_mma(const void* probs, const void* tile_map, int total_
   }
   const int grid = total_tiles < sms ? total_tiles : sms;
   ozaki_mma_kernel<<<grid, oz::THREADS, ozaki_mma_smem_bytes(), st>>>(
-      static_cast<const OzMmaProblem*>(probs), static_cast<const int4*>(tile_map), total_tiles, err);
+      static_cast<const OzMmaProblem*>(probs), static_cast<const int4*>(tile_map), total_tiles, err,
+      g_oz_wait_cycles.load());
   return cudaGetLastError();
 }
 

@@ -61,6 +61,7 @@ PROTOTYPES = {
                                                 ctypes.POINTER(ZGemmProblem), ctypes.c_void_p]),
     "negf_zcopy_batched": (ctypes.c_int, [ctypes.c_char, ctypes.c_int32, c_int32_p, c_int32_p, c_void_pp, c_int32_p,
                                           c_void_pp, c_int32_p, ctypes.c_void_p]),
+    "negf_set_tensor_wait_limit": (ctypes.c_int, [ctypes.c_double]),
     "negf_zfill_batched": (ctypes.c_int, [ctypes.c_int32, c_int32_p, c_int32_p, c_void_pp, c_int32_p, c_double_p,
                                           ctypes.c_void_p]),
     "negf_zinv_batched": (ctypes.c_int, [ctypes.c_int32, c_int32_p, c_void_pp, c_int32_p, c_void_pp, c_int32_p,

@@ -49,3 +49,20 @@ def test_two_gloo_ranks_shard_and_reduce(tmp_path):
     e0, e1 = res[0]["E"], res[1]["E"]
     assert len(set(e0) & set(e1)) == 0
     assert np.allclose(np.array(e0 + e1), np.linspace(-1.0, 1.0, 16))
+
+
+def test_gpus_flag_spawns_ranks_itself():
+    """bench.py --gpus 2 without a launcher starts two ranks through
+    torch.distributed.run (the reference arm runs on CPU: rank 0 prints the one
+    JSON line, rank 1 exits without work)."""
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK")}
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--gpus", "2",
+                        "--steps", "1", "--warmup", "0", "--cpu-budget-s", "0.5", "--npl", "3", "--b", "8",
+                        "--ne", "4"], capture_output=True, text=True, timeout=300, env=env, cwd=root)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    assert lines[0]["impl"] == "reference" and lines[0]["n_gpus"] == 2
