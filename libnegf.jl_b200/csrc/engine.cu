@@ -541,7 +541,7 @@ cudaError_t Plan::launch_step(const Step& s, const unsigned char* base, cudaStre
         break;
       case Step::GJ_PANEL:
         e = launch_zgj_panel(reinterpret_cast<const ZInvProblem*>(base + s.off), s.count, s.k0, s.nb, s.blocked,
-                             s.smem, stream);
+                             s.smem, stream, s.max_n);
         break;
       case Step::GJ_UNPERMUTE:
         e = launch_zgj_unpermute(reinterpret_cast<const ZInvProblem*>(base + s.off), s.count, s.max_n, stream);

@@ -29,8 +29,10 @@ int zgemm_tiles(int m, int n);
 size_t zgemm_smem_bytes();
 cudaError_t zgemm_prepare(char opA, char opB);
 size_t zgj_panel_smem_bytes(int n, int nb);
+// max_n (the largest block of the batch) selects the register-resident panel
+// kernel where it applies; 0 keeps the shared-memory one
 cudaError_t launch_zgj_panel(const ZInvProblem* probs_dev, int nprob, int k0, int nb, int blocked, size_t smem,
-                             cudaStream_t stream);
+                             cudaStream_t stream, int max_n = 0);
 cudaError_t launch_zgj_unpermute(const ZInvProblem* probs_dev, int nprob, int max_n, cudaStream_t stream);
 cudaError_t launch_zblockops(const ZBlockOp* ops_dev, int nops, int max_m, int max_n, cudaStream_t stream);
 cudaError_t launch_ztrace_prod(const void* probs_dev, int nprob, cudaStream_t stream);

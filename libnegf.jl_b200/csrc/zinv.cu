@@ -148,6 +148,193 @@ __global__ void __launch_bounds__(GJ_THREADS)
   }
 }
 
+// The same panel step with the slab in registers, for blocked panels of
+// n <= 256 RT rows and nb <= 2 CT columns (RT * CT = 16 values per thread):
+// thread t owns rows r = (t >> 1) + 256 k (k < RT) and panel columns
+// (t & 1) CT .. (t & 1) CT + CT - 1.  The threads of the half that holds the
+// pivot column rotate their register columns by one after every step, so the
+// pivot column is always register column 0 (every register index is a
+// compile-time one); register column j of half h holds panel column
+// h CT + (j + rot) mod CT.  Per column: each warp reduces the arg-max of its
+// rows, every thread merges the 16 warp results (one barrier), the two threads
+// of the pivot row publish the scaled pivot row (a second barrier), and every
+// thread updates its 16 values, taking its row's pivot column value from its
+// partner lane.  Shared memory holds only the 16 partials and the pivot row;
+// the arithmetic and the pivot rule are those of zgj_panel_kernel, so the
+// results are identical.
+template <int RT, int CT>
+__global__ void __launch_bounds__(GJ_THREADS, 1)
+    zgj_panel_reg_kernel(const ZInvProblem* __restrict__ probs, GjPanelArgs args) {
+  static_assert(GJ_THREADS == 512 && RT * CT == 16, "register panel layout");
+  // fields are read where needed (not held in registers across the column loop)
+  const ZInvProblem* __restrict__ pp = probs + blockIdx.x;
+  const int n = pp->n;
+  const int k0 = args.k0;
+  if (n <= 0 || k0 >= n) return;
+  const int w = min(args.nb, n - k0);
+  constexpr int NW = GJ_THREADS / 32;
+  __shared__ double part_v[NW];
+  __shared__ int part_r[NW];
+  __shared__ cplx rowbuf[2 * CT];
+  __shared__ cplx sh_pv;
+  __shared__ int sh_piv[2 * CT];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, h = tid & 1, rr = tid >> 1;
+  if (tid < 2 * CT) sh_piv[tid] = 0;  // valid row indices even if the column loop stops early
+
+  cplx a[RT][CT];
+  bool used[RT];
+  {
+    const cplx* W = pp->W;
+    const int ld = pp->ld;
+#pragma unroll
+    for (int k = 0; k < RT; ++k) {
+      const int r = rr + 256 * k;
+      used[k] = r >= n || (k0 > 0 && pp->used[r]);
+#pragma unroll
+      for (int j = 0; j < CT; ++j) {
+        const int col = h * CT + j;
+        a[k][j] = (r < n && col < w) ? W[r + (size_t)(k0 + col) * ld] : make_double2(0.0, 0.0);
+      }
+    }
+  }
+
+  int rot = 0;  // rotations of this thread's register columns
+  for (int c = 0; c < w; ++c) {
+    const bool mine = h == (c >= CT ? 1 : 0);
+    // 1. arg-max of |re| + |im| over this thread's unused rows of column c
+    double bv = -1.0;
+    int br = -1;
+    if (mine)
+#pragma unroll
+      for (int k = 0; k < RT; ++k)
+        if (!used[k]) argmax_merge(bv, br, cabs1(a[k][0]), rr + 256 * k);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const double v2 = __shfl_xor_sync(0xffffffffu, bv, off);
+      const int r2 = __shfl_xor_sync(0xffffffffu, br, off);
+      argmax_merge(bv, br, v2, r2);
+    }
+    if (lane == 0) {
+      part_v[warp] = bv;
+      part_r[warp] = br;
+    }
+    __syncthreads();
+    // 2. every thread merges the warp results (one order for all): one pivot
+    bv = part_v[0];
+    br = part_r[0];
+#pragma unroll
+    for (int q = 1; q < NW; ++q) argmax_merge(bv, br, part_v[q], part_r[q]);
+    const int pr = br;
+    if (pr < 0 || bv == 0.0) {
+      if (tid == 0 && pp->info) atomicCAS(pp->info, 0, k0 + c + 1);
+      if (pr < 0) break;  // uniform: the host reports the info code
+    }
+    // 3. the pivot column value of each of this thread's rows (register column
+    //    0 of the partner that holds column c), then the two threads of row pr
+    //    publish the pivot inverse and the scaled pivot row
+    const int kp = pr >> 8;
+    cplx cv[RT];
+#pragma unroll
+    for (int k = 0; k < RT; ++k) {
+      cplx o;
+      o.x = __shfl_xor_sync(0xffffffffu, a[k][0].x, 1);
+      o.y = __shfl_xor_sync(0xffffffffu, a[k][0].y, 1);
+      cv[k] = mine ? a[k][0] : o;
+    }
+    if (rr == (pr & 255)) {
+      cplx pivv = cv[0];
+#pragma unroll
+      for (int k = 1; k < RT; ++k)
+        if (k == kp) pivv = cv[k];
+      const cplx pv = (pivv.x == 0.0 && pivv.y == 0.0) ? make_double2(0.0, 0.0) : cinv(pivv);
+#pragma unroll
+      for (int j = 0; j < CT; ++j) {
+        cplx sj = a[0][j];
+#pragma unroll
+        for (int k = 1; k < RT; ++k)
+          if (k == kp) sj = a[k][j];
+        const int jj = j + rot < CT ? j + rot : j + rot - CT;
+        rowbuf[h * CT + jj] = (mine && j == 0) ? pv : cmul(sj, pv);
+      }
+      if (mine) {
+        sh_pv = pv;
+        sh_piv[c] = pr;
+      }
+#pragma unroll
+      for (int k = 0; k < RT; ++k)
+        if (k == kp) used[k] = true;
+    }
+    __syncthreads();
+    // 4. the Gauss-Jordan step on this thread's values (the pivot row is read
+    //    element by element, so its values are not all held in registers)
+    const cplx pv = sh_pv;
+    const volatile double* rb = reinterpret_cast<const volatile double*>(rowbuf + h * CT);
+#pragma unroll
+    for (int k = 0; k < RT; ++k) {
+      const bool prow = rr + 256 * k == pr;
+#pragma unroll
+      for (int j = 0; j < CT; ++j) {
+        const int jj = j + rot < CT ? j + rot : j + rot - CT;
+        const cplx rj = make_double2(rb[2 * jj], rb[2 * jj + 1]);
+        if (prow) a[k][j] = rj;
+        else if (mine && j == 0) a[k][j] = cneg(cmul(cv[k], pv));
+        else a[k][j] = cfms(a[k][j], cv[k], rj);
+      }
+    }
+    // 5. the pivot half brings its next column to register column 0
+    if (mine) {
+#pragma unroll
+      for (int k = 0; k < RT; ++k) {
+        const cplx t = a[k][0];
+#pragma unroll
+        for (int j = 0; j + 1 < CT; ++j) a[k][j] = a[k][j + 1];
+        a[k][CT - 1] = t;
+      }
+      rot = rot + 1 == CT ? 0 : rot + 1;
+    }
+    // the next column's partials overwrite part_v only after every thread
+    // passed the barrier above, and rowbuf only after the next one
+  }
+  __syncthreads();
+  // write back slab, pivots, used flags and F = slab - E_P (n x w, ld n)
+  {
+    cplx* W = pp->W;
+    cplx* F = pp->F;
+    const int ld = pp->ld;
+#pragma unroll
+    for (int k = 0; k < RT; ++k) {
+      const int r = rr + 256 * k;
+      if (r >= n) continue;
+#pragma unroll
+      for (int j = 0; j < CT; ++j) {
+        const int jj = j + rot < CT ? j + rot : j + rot - CT;
+        const int col = h * CT + jj;
+        if (col >= w) continue;
+        cplx v = a[k][j];
+        W[r + (size_t)(k0 + col) * ld] = v;
+        if (r == sh_piv[col]) v.x -= 1.0;
+        F[r + (size_t)col * n] = v;
+      }
+      if (h == 0) pp->used[r] = used[k] ? 1 : 0;
+    }
+  }
+  for (int c = tid; c < w; c += GJ_THREADS) pp->piv[k0 + c] = sh_piv[c];
+  // Bbuf = W[P, :] with panel columns zeroed  (w x n, ld w)
+  {
+    const cplx* W = pp->W;
+    cplx* Bbuf = pp->Bbuf;
+    const int ld = pp->ld;
+    for (int j = warp; j < n; j += NW) {
+      const bool inK = (j >= k0 && j < k0 + w);
+      for (int c = lane; c < w; c += 32) {
+        cplx v = make_double2(0.0, 0.0);
+        if (!inK) v = W[sh_piv[c] + (size_t)j * ld];
+        Bbuf[c + (size_t)j * w] = v;
+      }
+    }
+  }
+}
+
 // out[r, j] = W[piv[r], q[j]] with q the inverse permutation of piv:
 // out[r, piv[c]] = W[piv[r], c].
 __global__ void zgj_unpermute_kernel(const ZInvProblem* __restrict__ probs) {
@@ -170,10 +357,17 @@ size_t zgj_panel_smem_bytes(int n, int nb) {
 }
 
 cudaError_t launch_zgj_panel(const ZInvProblem* probs_dev, int nprob, int k0, int nb, int blocked, size_t smem,
-                             cudaStream_t stream) {
+                             cudaStream_t stream, int max_n) {
   if (nprob <= 0) return cudaSuccess;
   GjPanelArgs a{k0, nb, blocked};
-  zgj_panel_kernel<<<nprob, GJ_THREADS, smem, stream>>>(probs_dev, a);
+  // blocked panels of up to 256 rows x 32 columns or 512 rows x 16 columns:
+  // the slab in registers
+  if (blocked && max_n > 0 && max_n <= 256 && nb <= 32)
+    zgj_panel_reg_kernel<1, 16><<<nprob, GJ_THREADS, 0, stream>>>(probs_dev, a);
+  else if (blocked && max_n > 0 && max_n <= 512 && nb <= 16)
+    zgj_panel_reg_kernel<2, 8><<<nprob, GJ_THREADS, 0, stream>>>(probs_dev, a);
+  else
+    zgj_panel_kernel<<<nprob, GJ_THREADS, smem, stream>>>(probs_dev, a);
   return cudaGetLastError();
 }
 
