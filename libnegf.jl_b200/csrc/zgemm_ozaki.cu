@@ -29,14 +29,14 @@
 //     right operand's seven slices form one 448-row matrix, so that one MMA
 //     multiplies a left digit slice by several right digit slices at once;
 //   * the product kernel (persistent, one CTA per SM, 128 x 64 output tiles,
-//     256 threads): one thread streams stages with cp.async.bulk into a 5-deep
-//     mbarrier ring, refilling each slot as its MMAs retire; another issues the
+//     288 threads, warp-specialised): one producer lane streams stages with
+//     cp.async.bulk into a 5-deep mbarrier ring, refilling each slot as its
+//     MMAs retire; another producer lane issues the
 //     12 (or 10) MMAs (N = 64..256) of each stage into eight (seven) TMEM
-//     accumulators, one per digit diagonal of 64 columns; after
-//     each real product the eight warps drain the accumulators into FP64
-//     registers, and at the end of a tile they write
-//     C = alpha A B + beta Cin + diag I while the next tile's first product is
-//     already on the tensor cores.
+//     accumulators, one per digit diagonal of 64 columns; after each real
+//     product eight warps drain the accumulators into FP64 registers, and at
+//     the end of a tile they write C = alpha A B + beta Cin + diag I while the
+//     next tile's first product runs on the tensor cores.
 // Every mbarrier wait is bounded: a role whose pipeline wait runs past the
 // limit (a kernel argument, default ~1 s) records an error code and raises an
 // abort flag that ends the other roles' waits; the CTA then waits (bounded by
@@ -60,8 +60,14 @@ constexpr int A_BLOCK = S * A_SLICE;    // 28 KiB: one stage of the left operand
 constexpr int B_BLOCK = S * B_SLICE;    // 14 KiB
 constexpr int STAGE = A_BLOCK + B_BLOCK;
 constexpr int STAGES = 5;
-constexpr int THREADS = 256;            // 8 warps drain; lane 0 of warps 0 / 1 also issue MMAs / loads
-constexpr int DRAIN_WARPS = 8;
+constexpr int DRAIN_WARPS = 8;          // warps 0..7 drain and write the epilogue
+// warps 8..11 (one warpgroup) are the producers: lane 0 of warp 8 issues the
+// MMAs, lane 0 of warp 9 streams the stages.  Registers are moved from the producer
+// warpgroup to the two drain warpgroups after launch (setmaxnreg): launch
+// 384 x 168 = 64512 = 256 x 232 (drain) + 128 x 40 (producer).
+constexpr int THREADS = 32 * DRAIN_WARPS + 128;
+constexpr int REGS_LAUNCH = 168, REGS_DRAIN = 232, REGS_PRODUCER = 40;
+static_assert(THREADS * REGS_LAUNCH == 32 * DRAIN_WARPS * REGS_DRAIN + 128 * REGS_PRODUCER, "register split");
 constexpr int TMEM_COLS = 512;          // ND_MAX x TN
 constexpr long long WAIT_CYCLES = 2000000000LL;  // ~1 s at 1.9 GHz per wait
 constexpr int SPLIT_ROWS = 64;          // rows per split CTA
@@ -482,9 +488,14 @@ __device__ __forceinline__ void oz_stage_mmas(uint32_t tmem, uint64_t dA0, uint6
   }
 }
 
-// Persistent: CTA b computes tiles b, b + G, b + 2G, ... (G = gridDim.x); the
-// stage ring streams across tile boundaries, and the first product of the next
-// tile is issued before the epilogue of the current one.
+// Persistent: CTA b computes tiles b, b + G, b + 2G, ... (G = gridDim.x).
+// Warp-specialised: warps 0..7 drain the accumulators after every real product
+// and write each tile's epilogue; warp 8 is the producer -- lane 0 issues the
+// MMAs, lane 1 streams the stages into the ring.  Because neither producer
+// takes part in the drains or the epilogue, the stage ring keeps streaming and
+// the next product's MMAs are issued as soon as the previous product is
+// drained, so the first product of a tile runs under the previous tile's
+// epilogue.
 template <int ND>
 __global__ void __launch_bounds__(oz::THREADS, 1)
     ozaki_mma_kernel(const OzMmaProblem* __restrict__ probs, const int4* __restrict__ tile_map, int total_tiles,
@@ -505,7 +516,7 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int G = gridDim.x;
   const int my_tiles = (int)blockIdx.x < total_tiles ? (total_tiles - (int)blockIdx.x + G - 1) / G : 0;
-  const long long my_products = (long long)my_tiles * NP;
+  const int my_products = my_tiles * NP;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(oz_smem(&tmem_sh)),
@@ -528,274 +539,227 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
   asm volatile("tcgen05.fence::after_thread_sync;" ::);
   const uint32_t tmem = tmem_sh;
   const uint32_t sbase = oz_smem(smem);
-  // Lane 0 of warp 0 issues the MMAs; lane 0 of warp 1 streams the stages.
-  const bool mma_thread = tid == 0, load_thread = tid == 32;
-
-  // ---- load thread. Load cursor: tile lq, product lp, chunk lc, ring slot
-  // ls; refill cursor: the slot rs (phase rph) whose MMAs retire next. All
-  // counters are small ints (no division on the issue paths).
   const uint32_t full0 = oz_smem(&full_bar[0]), empty0 = oz_smem(&empty_bar[0]);
-  int lq = 0, lp = 0, lc = 0, ls = 0, rs = 0;
-  uint32_t rph = 0;
-  uint32_t used = 0, last_ph = 0;  // per slot: ever loaded, phase parity of its last load
-  bool lvalid = my_tiles > 0;
-  OzTile lt = oz_tile(tile_map, lvalid ? (int)blockIdx.x : 0);
-  const int8_t* la = nullptr;  // next A / B stage source of the load cursor
-  const int8_t* lb = nullptr;
-  auto load_product_base = [&]() {
-    const OzMmaProblem& q = probs[lt.prob];
-    la = q.SA + (size_t)(lp * lt.tiles_m + lt.mt) * lt.kch * A_BLOCK;
-    lb = q.SB + (size_t)(lp * lt.tiles_n + lt.nt) * lt.kch * B_BLOCK;
-  };
-  if (load_thread && lvalid) load_product_base();
-  bool load_ok = true, mma_ok = true;
-  long long next_refill = 0;  // first product not refilled yet
 
-  auto issue_load = [&]() {
-    const uint32_t fb = full0 + ls * 8;
-    const uint32_t dA = sbase + ls * STAGE, dB = dA + A_BLOCK;
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb), "r"(STAGE) : "memory");
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dA),
-                 "l"(la), "r"(A_BLOCK), "r"(fb)
-                 : "memory");
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dB),
-                 "l"(lb), "r"(B_BLOCK), "r"(fb)
-                 : "memory");
-    // phase parity of this load of slot ls: flips on every reuse of the slot
-    const uint32_t bit = 1u << ls;
-    last_ph = (used & bit) ? (last_ph ^ bit) : (last_ph & ~bit);
-    used |= bit;
-    ls = ls + 1 == STAGES ? 0 : ls + 1;
-    la += A_BLOCK;
-    lb += B_BLOCK;
-    if (++lc == lt.kch) {
-      lc = 0;
-      if (++lp == NP) {
-        lp = 0;
-        if (++lq == my_tiles) {
-          lvalid = false;
-          return;
+  if (warp >= DRAIN_WARPS) {
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(REGS_PRODUCER));
+  } else {
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(REGS_DRAIN));
+  }
+  if (warp >= DRAIN_WARPS) {
+    if (lane != 0 || warp > DRAIN_WARPS + 1) {
+      // the rest of the producer warpgroup has no work
+    } else if (warp == DRAIN_WARPS + 1) {
+      // ---- loader: every stage of every product of every tile, in order;
+      // a slot is refilled once the MMAs of its previous stage retired (its
+      // empty barrier); per slot, the parity of its last load is kept for the
+      // final wait
+      uint32_t loaded = 0, last_ph = 0;
+      int ls = 0, use = 0;  // ring slot and how many times the ring wrapped
+      bool ok = true;
+      for (int q = 0; q < my_tiles && ok; ++q) {
+        const OzTile t = oz_tile(tile_map, (int)blockIdx.x + q * G);
+        const OzMmaProblem& pq = probs[t.prob];
+        for (int p = 0; p < NP && ok; ++p) {
+          const int8_t* la = pq.SA + (size_t)(p * t.tiles_m + t.mt) * t.kch * A_BLOCK;
+          const int8_t* lb = pq.SB + (size_t)(p * t.tiles_n + t.nt) * t.kch * B_BLOCK;
+          for (int c = 0; c < t.kch; ++c) {
+            if (use > 0 && !oz_wait(empty0 + ls * 8, (uint32_t)((use - 1) & 1), abort_flag, err, true, wait_cycles)) {
+              ok = false;
+              break;
+            }
+            const uint32_t fb = full0 + ls * 8;
+            const uint32_t dA = sbase + ls * STAGE, dB = dA + A_BLOCK;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb), "r"(STAGE) : "memory");
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dA),
+                "l"(la + (size_t)c * A_BLOCK), "r"(A_BLOCK), "r"(fb)
+                : "memory");
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dB),
+                "l"(lb + (size_t)c * B_BLOCK), "r"(B_BLOCK), "r"(fb)
+                : "memory");
+            loaded |= 1u << ls;
+            last_ph = (last_ph & ~(1u << ls)) | ((uint32_t)(use & 1) << ls);
+            if (++ls == STAGES) {
+              ls = 0;
+              ++use;
+            }
+          }
         }
-        lt = oz_tile(tile_map, (int)blockIdx.x + lq * G);
       }
-      load_product_base();
+      // every issued copy lands before the CTA exits (default limit, also
+      // after an abort: issued copies always complete)
+      for (int s = 0; s < STAGES; ++s)
+        if (loaded & (1u << s)) oz_wait(full0 + s * 8, (last_ph >> s) & 1u, abort_flag, err, false);
+    } else {
+      // ---- MMA issuer: product P waits for the drain of P - 1 (the
+      // accumulators are reused), then issues its stages as they land
+      const uint64_t descA0 = oz_desc(sbase, TM * 16, 128), descB0 = oz_desc(sbase + A_BLOCK, S * TN * 16, 128);
+      int ms = 0;
+      uint32_t mph = 0;
+      bool ok = true;
+      for (int P = 0; P < my_products && ok; ++P) {
+        if (P > 0 && !oz_wait(oz_smem(&acce_bar), (uint32_t)((P - 1) & 1), abort_flag, err, true, wait_cycles))
+          break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::);
+        const int kch = oz_tile(tile_map, (int)blockIdx.x + (P / NP) * G).kch;
+        for (int c = 0; c < kch; ++c) {
+          if (!oz_wait(full0 + ms * 8, mph, abort_flag, err, true, wait_cycles)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::);
+          const uint64_t soff = (uint64_t)(ms * (STAGE >> 4));
+          oz_stage_mmas<ND>(tmem, descA0 + soff, descB0 + soff, c == 0);
+          oz_commit(empty0 + ms * 8);
+          if (c == kch - 1) oz_commit(oz_smem(&accf_bar));
+          if (++ms == STAGES) {
+            ms = 0;
+            mph ^= 1u;
+          }
+        }
+      }
+      // all MMAs of this CTA complete before TMEM is released (default limit)
+      oz_commit(oz_smem(&done_bar));
+      oz_wait(oz_smem(&done_bar), 0, abort_flag, err, false);
     }
-  };
-
-  // refill, stage by stage as the MMAs of global product P retire, the slots
-  // with the next stages of the load cursor
-  int rkch = 0;
-  auto refill_product = [&](long long P) {
-    if (P % NP == 0) rkch = oz_tile(tile_map, (int)blockIdx.x + (int)(P / NP) * G).kch;
-    for (int c = 0; c < rkch; ++c) {
-      if (!oz_wait(empty0 + rs * 8, rph, abort_flag, err, true, wait_cycles)) {
-        load_ok = false;
-        return;
-      }
-      if (++rs == STAGES) {
-        rs = 0;
-        rph ^= 1u;
-      }
-      if (lvalid) issue_load();
-    }
-  };
-
-  // ---- MMA thread: the stages of global product P (tile P / NP, real product
-  // P % NP) up to chunk cend; product cur_P has its chunks [0, cur_c) issued.
-  // Ring slot ms with its full-barrier phase mph.
-  const uint64_t descA0 = oz_desc(sbase, TM * 16, 128), descB0 = oz_desc(sbase + A_BLOCK, S * TN * 16, 128);
-  int ms = 0, mkch = 0, cur_c = 0;
-  long long cur_P = -1;
-  uint32_t mph = 0;
-  auto issue_upto = [&](long long P, int cend) {
-    if (cur_P != P) {
-      if (P > 0 && !oz_wait(oz_smem(&acce_bar), (uint32_t)((P - 1) & 1), abort_flag, err, true, wait_cycles)) {
-        mma_ok = false;
-        return;
-      }
-      asm volatile("tcgen05.fence::after_thread_sync;" ::);
-      if (P % NP == 0) mkch = oz_tile(tile_map, (int)blockIdx.x + (int)(P / NP) * G).kch;
-      cur_P = P;
-      cur_c = 0;
-    }
-    const int c1 = cend < mkch ? cend : mkch;
-    for (; cur_c < c1; ++cur_c) {
-      const int c = cur_c;
-      if (!oz_wait(full0 + ms * 8, mph, abort_flag, err, true, wait_cycles)) {
-        mma_ok = false;
-        return;
-      }
-      asm volatile("tcgen05.fence::after_thread_sync;" ::);
-      const uint64_t soff = (uint64_t)(ms * (STAGE >> 4));
-      oz_stage_mmas<ND>(tmem, descA0 + soff, descB0 + soff, c == 0);
-      oz_commit(empty0 + ms * 8);
-      if (c == mkch - 1) oz_commit(oz_smem(&accf_bar));
-      if (++ms == STAGES) {
-        ms = 0;
-        mph ^= 1u;
-      }
-    }
-  };
-
-  if (load_thread)
-    for (int i = 0; i < STAGES && lvalid; ++i) issue_load();
-
-  // ---- all eight warps: drain each product, then the tile epilogue; warp w
-  // reads TMEM lanes 32 (w % 4).. and columns 32 (w / 4)..
-  const int qd = warp & 3, hh = warp >> 2;
-  bool ok = true;
-  constexpr int mkch_all = 1 << 30;
-  int my_eA = 0;
-  double my_scA = 1.0;
-  for (int q = 0; q < my_tiles && ok; ++q) {
-    const OzTile tq = oz_tile(tile_map, (int)blockIdx.x + q * G);
-    double cr[32], ci[32];
+  } else {
+    // ---- warps 0..7: drain each product, then the tile epilogue; warp w
+    // reads TMEM lanes 32 (w % 4).. and columns 32 (w / 4)..
+    const int qd = warp & 3, hh = warp >> 2;
+    bool ok = true;
+    int my_eA = 0;
+    double my_scA = 1.0;
+    for (int q = 0; q < my_tiles && ok; ++q) {
+      const OzTile tq = oz_tile(tile_map, (int)blockIdx.x + q * G);
+      double cr[32], ci[32];
 #pragma unroll
-    for (int j = 0; j < 32; ++j) { cr[j] = 0.0; ci[j] = 0.0; }
-    for (int p = 0; p < NP; ++p) {
-      const long long P = (long long)q * NP + p;
-      if (mma_thread && mma_ok) issue_upto(P, mkch_all);
-      if (load_thread && load_ok && next_refill == P) {
-        refill_product(P);
-        ++next_refill;
-      }
-      __syncwarp();
-      if (p == 0) {
-        // stage this tile's epilogue inputs while its first product runs
-        const int* src = reinterpret_cast<const int*>(probs + tq.prob);
-        int* eps = ep_sh[q & 1][warp];
-        for (int w = lane; w < PROB_WORDS; w += 32) eps[w] = src[w];
-        const OzMmaProblem* pp = probs + tq.prob;
-        const int eb = pp->eB[tq.nt * TN + hh * 32 + lane];
-        eps[40 + lane] = eb;
-        reinterpret_cast<double*>(eps + 72)[lane] = oz_pow2(eb);
-        my_eA = pp->eA[tq.mt * TM + qd * 32 + lane];
-        my_scA = oz_pow2(my_eA);
+      for (int j = 0; j < 32; ++j) { cr[j] = 0.0; ci[j] = 0.0; }
+      for (int p = 0; p < NP; ++p) {
+        const int P = q * NP + p;
+        if (p == 0) {
+          // stage this tile's epilogue inputs while its first product runs
+          const int* src = reinterpret_cast<const int*>(probs + tq.prob);
+          int* eps = ep_sh[q & 1][warp];
+          for (int w = lane; w < PROB_WORDS; w += 32) eps[w] = src[w];
+          const OzMmaProblem* pp = probs + tq.prob;
+          const int eb = pp->eB[tq.nt * TN + hh * 32 + lane];
+          eps[40 + lane] = eb;
+          reinterpret_cast<double*>(eps + 72)[lane] = oz_pow2(eb);
+          my_eA = pp->eA[tq.mt * TM + qd * 32 + lane];
+          my_scA = oz_pow2(my_eA);
+          __syncwarp();
+        }
+        if (!oz_wait_warp(oz_smem(&accf_bar), (uint32_t)(P & 1), abort_flag, err, wait_cycles)) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::);
+        // product p adds v to Re with sign sr and to Im with sign si (P1: +Re,
+        // -Im; P2: -Re, -Im; P3: +Im); alpha is folded in: (kr, ki) = alpha (sr, si)
+        const double sr = (p == 2) ? 0.0 : (p == 0 ? 1.0 : -1.0);
+        const double si = (p == 2) ? 1.0 : -1.0;
+        const cplx al = reinterpret_cast<const OzMmaProblem*>(ep_sh[q & 1][warp])->alpha;
+        const double kr = al.x * sr - al.y * si, ki = al.x * si + al.y * sr;
+#pragma unroll
+        for (int c8 = 0; c8 < 4; ++c8) {
+          double v[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) v[j] = 0.0;
+#pragma unroll
+          for (int g = 0; g < (ND + 3) / 4; ++g) {  // up to four diagonals per TMEM round trip
+            constexpr int kMax = 4;
+            const int nd = ND - 4 * g < kMax ? ND - 4 * g : kMax;
+            uint32_t x[kMax][8];
+#pragma unroll
+            for (int dd = 0; dd < nd; ++dd) {
+              const int d = 4 * g + dd;
+              const uint32_t addr = tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(d * TN + hh * 32 + c8 * 8);
+              asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                           : "=r"(x[dd][0]), "=r"(x[dd][1]), "=r"(x[dd][2]), "=r"(x[dd][3]), "=r"(x[dd][4]),
+                             "=r"(x[dd][5]), "=r"(x[dd][6]), "=r"(x[dd][7])
+                           : "r"(addr));
+            }
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int dd = 0; dd < nd; ++dd) {
+              const double w = oz_diag_weight(4 * g + dd);
+#pragma unroll
+              for (int j = 0; j < 8; ++j) v[j] = fma(oz_i2d(x[dd][j]), w, v[j]);
+            }
+          }
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            cr[c8 * 8 + j] = fma(kr, v[j], cr[c8 * 8 + j]);
+            ci[c8 * 8 + j] = fma(ki, v[j], ci[c8 * 8 + j]);
+          }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::);
         __syncwarp();
+        if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(oz_smem(&acce_bar)) : "memory");
       }
-      if (!oz_wait_warp(oz_smem(&accf_bar), (uint32_t)(P & 1), abort_flag, err, wait_cycles)) {
-        ok = false;
-        break;
-      }
-      asm volatile("tcgen05.fence::after_thread_sync;" ::);
-      // product p adds v to Re with sign sr and to Im with sign si (P1: +Re,
-      // -Im; P2: -Re, -Im; P3: +Im); alpha is folded in: (kr, ki) = alpha (sr, si)
-      const double sr = (p == 2) ? 0.0 : (p == 0 ? 1.0 : -1.0);
-      const double si = (p == 2) ? 1.0 : -1.0;
-      const cplx al = reinterpret_cast<const OzMmaProblem*>(ep_sh[q & 1][warp])->alpha;
-      const double kr = al.x * sr - al.y * si, ki = al.x * si + al.y * sr;
+      if (!ok) break;
+      // C = alpha 2^(eA + eB) (Re, Im) + beta Cin + diag I (alpha already in
+      // cr, ci), from the staged descriptor and scales; Cin is read one group
+      // of columns ahead of the stores.  The producer keeps the tensor cores
+      // busy with the next tile meanwhile.
+      const int* eps = ep_sh[q & 1][warp];
+      const OzMmaProblem& ps = *reinterpret_cast<const OzMmaProblem*>(eps);
+      const int r = tq.mt * TM + qd * 32 + lane;
+      if (r < ps.m) {
+        const int pn = ps.n, ldc = ps.ldc, ldcin = ps.ldcin;
+        const cplx beta = ps.beta;
+        cplx* const Cout = ps.C;
+        const cplx* const Cin = ps.Cin;
+        const cplx dg = ps.diag_ptr ? *ps.diag_ptr : ps.diag;
+        const bool has_cin = Cin && (beta.x != 0.0 || beta.y != 0.0);
+        const int c0 = tq.nt * TN + hh * 32;
+        constexpr int GW = 4;  // columns per group
+        cplx cb[GW], cn[GW];
 #pragma unroll
-      for (int c8 = 0; c8 < 4; ++c8) {
-        double v[8];
+        for (int jj = 0; jj < GW; ++jj)
+          cn[jj] = (has_cin && c0 + jj < pn) ? Cin[r + (size_t)(c0 + jj) * ldcin] : make_double2(0.0, 0.0);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) v[j] = 0.0;
+        for (int g8 = 0; g8 < 32 / GW; ++g8) {
 #pragma unroll
-        for (int g = 0; g < (ND + 3) / 4; ++g) {  // up to four diagonals per TMEM round trip
-          constexpr int kMax = 4;
-          const int nd = ND - 4 * g < kMax ? ND - 4 * g : kMax;
-          uint32_t x[kMax][8];
+          for (int jj = 0; jj < GW; ++jj) cb[jj] = cn[jj];
+          if (g8 < 32 / GW - 1) {
 #pragma unroll
-          for (int dd = 0; dd < nd; ++dd) {
-            const int d = 4 * g + dd;
-            const uint32_t addr = tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(d * TN + hh * 32 + c8 * 8);
-            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                         : "=r"(x[dd][0]), "=r"(x[dd][1]), "=r"(x[dd][2]), "=r"(x[dd][3]), "=r"(x[dd][4]),
-                           "=r"(x[dd][5]), "=r"(x[dd][6]), "=r"(x[dd][7])
-                         : "r"(addr));
+            for (int jj = 0; jj < GW; ++jj) {
+              const int c = c0 + (g8 + 1) * GW + jj;
+              cn[jj] = (has_cin && c < pn) ? Cin[r + (size_t)c * ldcin] : make_double2(0.0, 0.0);
+            }
           }
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-          for (int dd = 0; dd < nd; ++dd) {
-            const double w = oz_diag_weight(4 * g + dd);
-#pragma unroll
-            for (int j = 0; j < 8; ++j) v[j] = fma(oz_i2d(x[dd][j]), w, v[j]);
-          }
-        }
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          cr[c8 * 8 + j] = fma(kr, v[j], cr[c8 * 8 + j]);
-          ci[c8 * 8 + j] = fma(ki, v[j], ci[c8 * 8 + j]);
-        }
-      }
-      asm volatile("tcgen05.fence::before_thread_sync;" ::);
-      __syncwarp();
-      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(oz_smem(&acce_bar)) : "memory");
-    }
-    if (!ok) break;
-    // the next tile's first product goes to the tensor cores before this
-    // epilogue, as far as its stages are loaded already (STAGES of them); the
-    // rest follows after the epilogue, as does the load thread's refill
-    if (mma_thread && mma_ok && (long long)(q + 1) * NP < my_products) issue_upto((long long)(q + 1) * NP, STAGES);
-    __syncwarp();
-    // C = alpha 2^(eA + eB) (Re, Im) + beta Cin + diag I (alpha already in
-    // cr, ci), from the
-    // staged descriptor and scales; Cin is read one group of columns ahead of
-    // the stores
-    const int* eps = ep_sh[q & 1][warp];
-    const OzMmaProblem& ps = *reinterpret_cast<const OzMmaProblem*>(eps);
-    const int r = tq.mt * TM + qd * 32 + lane;
-    if (r < ps.m) {
-      const int pn = ps.n, ldc = ps.ldc, ldcin = ps.ldcin;
-      const cplx beta = ps.beta;
-      cplx* const Cout = ps.C;
-      const cplx* const Cin = ps.Cin;
-      const cplx dg = ps.diag_ptr ? *ps.diag_ptr : ps.diag;
-      const bool has_cin = Cin && (beta.x != 0.0 || beta.y != 0.0);
-      const int c0 = tq.nt * TN + hh * 32;
-      constexpr int GW = 4;  // columns per group
-      cplx cb[GW], cn[GW];
-#pragma unroll
-      for (int jj = 0; jj < GW; ++jj)
-        cn[jj] = (has_cin && c0 + jj < pn) ? Cin[r + (size_t)(c0 + jj) * ldcin] : make_double2(0.0, 0.0);
-#pragma unroll
-      for (int g8 = 0; g8 < 32 / GW; ++g8) {
-#pragma unroll
-        for (int jj = 0; jj < GW; ++jj) cb[jj] = cn[jj];
-        if (g8 < 32 / GW - 1) {
 #pragma unroll
           for (int jj = 0; jj < GW; ++jj) {
-            const int c = c0 + (g8 + 1) * GW + jj;
-            cn[jj] = (has_cin && c < pn) ? Cin[r + (size_t)c * ldcin] : make_double2(0.0, 0.0);
+            const int j = g8 * GW + jj;
+            const int c = c0 + j;
+            if (c >= pn) continue;
+            // alpha 2^(eA + eB) (Re, Im): two exact power-of-two factors when
+            // both exponents are moderate, else one ldexp
+            const double scB = reinterpret_cast<const double*>(eps + 72)[j];
+            double xr, xi;
+            if (my_scA != 0.0 && scB != 0.0) {
+              xr = cr[j] * my_scA * scB;
+              xi = ci[j] * my_scA * scB;
+            } else {
+              xr = ldexp(cr[j], my_eA + eps[40 + j]);
+              xi = ldexp(ci[j], my_eA + eps[40 + j]);
+            }
+            cplx v;
+            v.x = xr + (beta.x * cb[jj].x - beta.y * cb[jj].y);
+            v.y = xi + (beta.x * cb[jj].y + beta.y * cb[jj].x);
+            if (r == c) {
+              v.x += dg.x;
+              v.y += dg.y;
+            }
+            Cout[r + (size_t)c * ldc] = v;
           }
-        }
-#pragma unroll
-        for (int jj = 0; jj < GW; ++jj) {
-          const int j = g8 * GW + jj;
-          const int c = c0 + j;
-          if (c >= pn) continue;
-          // alpha 2^(eA + eB) (Re, Im): two exact power-of-two factors when
-          // both exponents are moderate, else one ldexp
-          const double scB = reinterpret_cast<const double*>(eps + 72)[j];
-          double xr, xi;
-          if (my_scA != 0.0 && scB != 0.0) {
-            xr = cr[j] * my_scA * scB;
-            xi = ci[j] * my_scA * scB;
-          } else {
-            xr = ldexp(cr[j], my_eA + eps[40 + j]);
-            xi = ldexp(ci[j], my_eA + eps[40 + j]);
-          }
-          cplx v;
-          v.x = xr + (beta.x * cb[jj].x - beta.y * cb[jj].y);
-          v.y = xi + (beta.x * cb[jj].y + beta.y * cb[jj].x);
-          if (r == c) {
-            v.x += dg.x;
-            v.y += dg.y;
-          }
-          Cout[r + (size_t)c * ldc] = v;
         }
       }
     }
   }
-  // all MMAs of this CTA complete, and every issued copy has landed, before
-  // TMEM is released and the CTA exits; these waits keep the default limit
-  // (work already issued always completes), also after an abort
-  if (mma_thread) {
-    oz_commit(oz_smem(&done_bar));
-    oz_wait(oz_smem(&done_bar), 0, abort_flag, err, false);
-  }
-  if (load_thread)
-    for (int s = 0; s < STAGES; ++s)
-      if (used & (1u << s)) oz_wait(full0 + s * 8, (last_ph >> s) & 1u, abort_flag, err, false);
   __syncwarp();
   asm volatile("tcgen05.fence::before_thread_sync;" ::);
   __syncthreads();
@@ -898,6 +862,15 @@ static_assert(split1_smem(128) <= kSplit1SmemMax && split1_smem(256) <= kSplit1S
               "single-read split staging");
 
 cudaError_t ozaki_prepare() {
+  // the register split of the product kernel assumes the launch allocates
+  // exactly REGS_LAUNCH registers per thread; with fewer, setmaxnreg.inc of
+  // the drain warps could never be satisfied, so such a build is refused
+  for (const void* f : {(const void*)ozaki_mma_kernel<7>, (const void*)ozaki_mma_kernel<8>}) {
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, f);
+    if (e != cudaSuccess) return e;
+    if (a.numRegs != oz::REGS_LAUNCH) return cudaErrorInvalidKernelImage;
+  }
   cudaError_t e = cudaFuncSetAttribute(ozaki_mma_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)ozaki_mma_smem_bytes());
   if (e == cudaSuccess)

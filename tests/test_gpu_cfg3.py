@@ -9,18 +9,25 @@ launch over all energies, with the block products in FP64 or on the INT8
 tensor cores (mixed).
 
 Bars: DDRGF (both precisions) against the oracle's DDRGF restatement with the
-same levels, within 2.5e-10 (the reference's DDRGF tolerance,
-test_matinvertndiag_ddrgf.jl:245-293) plus 10x that restatement's own distance
-from sequential RGF: on the NEGF generator the interior domains are closed
-systems (eta = 1e-6) whose inverses are ill-conditioned, so DDRGF itself -- the
-reference's algorithm, restated on the CPU -- departs from RGF by up to ~1e-8
-here, and two FP64 executions of it differ by that order; the selected inverse on the
+same levels. With eta = 1e-2 every interior domain is well conditioned and the
+bar is the reference's DDRGF tolerance, 2.5e-10
+(test_matinvertndiag_ddrgf.jl:245-293). With eta = 1e-6 the interior domains
+are closed systems (no lead self-energy) whose inverses are ill-conditioned:
+DDRGF itself -- the reference's algorithm, restated on the CPU -- departs from
+sequential RGF by up to ~3e-8 at b = 512, and a relative perturbation of the
+input at the unit roundoff moves it by as much. There the bar is 2.5e-10 plus
+30x the larger of those two figures at the same energy (two backward-stable
+executions of DDRGF -- LAPACK LU solves on the CPU, Gauss-Jordan inverses on
+the GPU -- differ by up to ~10x that sensitivity). Sequential RGF on the same
+device stays within 1e-11 of the oracle's. The selected inverse on the
 NEGF generator (lu(NoPivot()) diagonal factorisations) against the oracle's
 restatement with the same factorisation and the dense inverse at 1e-12 (FP64)
 / 1e-10 (mixed); the batched reference-API entry point against the oracle's
 restatement of the reference (be_getrf! with discarded pivots) on the
 reference test's diagonally dominant generator at 1e-13 absolute.
 """
+
+import copy
 
 import numpy as np
 import pytest
@@ -45,11 +52,25 @@ def _oracle_tri(sysm, E):
             [G.M[(i + 1, i)] for i in range(n - 1)])
 
 
-@pytest.mark.parametrize("npl,b,nE,levels", [(16, 512, 4, [3]), (19, 64, 5, [4]), (40, 32, 3, [3, 3])])
-def test_device_ddrgf_fp64_and_mixed(negf, npl, b, nE, levels):
+def _perturbed(M, rng):
+    """M with every stored block scaled entrywise by (1 + 2^-53 z), z complex normal."""
+    P = copy.deepcopy(M)
+    for k, v in P.M.items():
+        P.M[k] = v * (1.0 + 2.0 ** -53 * (rng.standard_normal(v.shape) + 1j * rng.standard_normal(v.shape)))
+    return P
+
+
+def _tri_of(D, n):
+    return ([D.M[(i, i)] for i in range(n)], [D.M[(i, i + 1)] for i in range(n - 1)],
+            [D.M[(i + 1, i)] for i in range(n - 1)])
+
+
+@pytest.mark.parametrize("npl,b,nE,levels,eta", [(16, 512, 4, [3], 1e-2), (16, 512, 4, [3], 1e-6),
+                                                 (19, 64, 5, [4], 1e-6), (40, 32, 3, [3, 3], 1e-6)])
+def test_device_ddrgf_fp64_and_mixed(negf, npl, b, nE, levels, eta):
     """DDRGF of the NEGF generator over energies; (16, 512, [3]) is the
     benchmark's b = 512 with four partitions (separators at layers 0, 4, 8, 12)."""
-    sysm = o_phys.physics_system(npl, b, seed=31)
+    sysm = o_phys.physics_system(npl, b, seed=31, eta=eta)
     Es = np.linspace(-0.7, 0.8, nE)
     dev = negf.Device(sysm.Hd, sysm.Hu, sysm.sigL, sysm.sigR)
     f64 = dev.selected_inverse(Es, method="ddrgf", precision="fp64", eta=sysm.eta, levels=levels)
@@ -57,15 +78,19 @@ def test_device_ddrgf_fp64_and_mixed(negf, npl, b, nE, levels):
     rgf = dev.selected_inverse(Es, method="rgf", precision="fp64", eta=sysm.eta)
     dev.close()
     n = npl
+    rng = np.random.default_rng(7)
     for e, E in enumerate(Es):
+        M = sysm.M_of_E(E)
         ref = _oracle_tri(sysm, E)
-        D = o_ddrgf.bndiag_of_inv_ddrgf(sysm.M_of_E(E), levels)[0]
-        dd = ([D.M[(i, i)] for i in range(n)], [D.M[(i, i + 1)] for i in range(n - 1)],
-              [D.M[(i + 1, i)] for i in range(n - 1)])
+        dd = _tri_of(o_ddrgf.bndiag_of_inv_ddrgf(M, levels)[0], n)
+        if eta >= 1e-2:
+            bars = [2.5e-10] * 3
+        else:
+            pert = _tri_of(o_ddrgf.bndiag_of_inv_ddrgf(_perturbed(M, rng), levels)[0], n)
+            bars = [2.5e-10 + 30.0 * max(_max_err(dd[p], ref[p]), _max_err(pert[p], dd[p])) for p in range(3)]
         for part in range(3):
-            bar = 2.5e-10 + 10.0 * _max_err(dd[part], ref[part])
-            assert _max_err(f64[part][e], dd[part]) < bar
-            assert _max_err(mix[part][e], dd[part]) < bar
+            assert _max_err(f64[part][e], dd[part]) < bars[part]
+            assert _max_err(mix[part][e], dd[part]) < bars[part]
             assert _max_err(rgf[part][e], ref[part]) < 1e-11
 
 
