@@ -69,6 +69,7 @@ constexpr int THREADS = 32 * DRAIN_WARPS + 128;
 constexpr int REGS_LAUNCH = 168, REGS_DRAIN = 232, REGS_PRODUCER = 40;
 static_assert(THREADS * REGS_LAUNCH == 32 * DRAIN_WARPS * REGS_DRAIN + 128 * REGS_PRODUCER, "register split");
 constexpr int TMEM_COLS = 512;          // ND_MAX x TN
+static_assert(TMEM_COLS == ND_MAX * TN, "one accumulator per digit diagonal");
 constexpr long long WAIT_CYCLES = 2000000000LL;  // ~1 s at 1.9 GHz per wait
 constexpr int SPLIT_ROWS = 64;          // rows per split CTA
 // offset that turns the six lower bytes of x + C6 into digits + 128:
@@ -81,12 +82,6 @@ __host__ __device__ constexpr double oz_diag_weight(int D) {
   double w = 0x1p-12;
   for (int d = 0; d < D; ++d) w *= 0x1p-8;
   return w;
-}
-
-// 2^e as a double for |e| <= 500, else 0 (callers then take an ldexp path);
-// the limit keeps products of two such factors and an accumulator in range
-__device__ __forceinline__ double oz_pow2(int e) {
-  return (e >= -500 && e <= 500) ? __longlong_as_double((long long)(e + 1023) << 52) : 0.0;
 }
 
 // exact int32 -> double on the FP64 pipe: the bits 0x43300000:(x ^ 2^31) are
@@ -505,12 +500,14 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
   __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES], accf_bar, acce_bar, done_bar;
   __shared__ uint32_t tmem_sh;
   __shared__ int abort_sh;
-  // per (tile parity, warp): a copy of the tile's problem descriptor and the
-  // warp's 32 column exponents and scales 2^eB, staged at the start of a tile
+  // per (tile parity, warp): a copy of the tile's problem descriptor, staged
+  // at the start of a tile.  The column exponents and scales stay in
+  // registers (lane j holds column j's) and reach the other lanes by shuffle:
+  // while the tensor cores stream their operands, shared-memory loads wait
+  // hundreds of cycles each
   constexpr int PROB_WORDS = (int)(sizeof(OzMmaProblem) / 4);
   static_assert(sizeof(OzMmaProblem) % 16 == 0 && PROB_WORDS <= 40, "epilogue staging layout");
-  // words 0..39 descriptor, 40..71 column exponents, 72..135 column scales
-  __shared__ __align__(16) int ep_sh[2][DRAIN_WARPS][136];
+  __shared__ __align__(16) int ep_sh[2][DRAIN_WARPS][40];
   volatile int* abort_flag = &abort_sh;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -600,10 +597,10 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
       uint32_t mph = 0;
       bool ok = true;
       for (int P = 0; P < my_products && ok; ++P) {
+        const int kch = oz_tile(tile_map, (int)blockIdx.x + (P / NP) * G).kch;  // read before the wait
         if (P > 0 && !oz_wait(oz_smem(&acce_bar), (uint32_t)((P - 1) & 1), abort_flag, err, true, wait_cycles))
           break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::);
-        const int kch = oz_tile(tile_map, (int)blockIdx.x + (P / NP) * G).kch;
         for (int c = 0; c < kch; ++c) {
           if (!oz_wait(full0 + ms * 8, mph, abort_flag, err, true, wait_cycles)) {
             ok = false;
@@ -627,30 +624,40 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
   } else {
     // ---- warps 0..7: drain each product, then the tile epilogue; warp w
     // reads TMEM lanes 32 (w % 4).. and columns 32 (w / 4)..
+    //
+    // On this hardware FP64 arithmetic makes no progress while the tensor
+    // cores run INT8 MMAs (the two share a datapath), so the drains run
+    // between products and the epilogue keeps its FP64 work to two
+    // multiplications per output (four more with a Cin term): the column and
+    // row scales are combined as exponents in integer arithmetic.
     const int qd = warp & 3, hh = warp >> 2;
     bool ok = true;
-    int my_eA = 0;
-    double my_scA = 1.0;
+    // this tile's inputs: row exponent (per lane), column exponent (lane j
+    // holds column j's), alpha; the next tile's are fetched before this
+    // tile's epilogue so that their latency is hidden
+    int my_eA = 0, my_eB = 0;
+    cplx al = make_double2(0.0, 0.0);
+    auto fetch = [&](int q, const OzTile& t, int& eA, int& eB, cplx& a) {
+      const int* src = reinterpret_cast<const int*>(probs + t.prob);
+      int* eps = ep_sh[q & 1][warp];
+      for (int w = lane; w < PROB_WORDS; w += 32) eps[w] = src[w];
+      const OzMmaProblem* pp = probs + t.prob;
+      eB = pp->eB[t.nt * TN + hh * 32 + lane];
+      eA = pp->eA[t.mt * TM + qd * 32 + lane];
+      a = pp->alpha;
+    };
+    OzTile tq{};
+    if (my_tiles > 0) {
+      tq = oz_tile(tile_map, (int)blockIdx.x);
+      fetch(0, tq, my_eA, my_eB, al);
+      __syncwarp();
+    }
     for (int q = 0; q < my_tiles && ok; ++q) {
-      const OzTile tq = oz_tile(tile_map, (int)blockIdx.x + q * G);
       double cr[32], ci[32];
 #pragma unroll
       for (int j = 0; j < 32; ++j) { cr[j] = 0.0; ci[j] = 0.0; }
       for (int p = 0; p < NP; ++p) {
         const int P = q * NP + p;
-        if (p == 0) {
-          // stage this tile's epilogue inputs while its first product runs
-          const int* src = reinterpret_cast<const int*>(probs + tq.prob);
-          int* eps = ep_sh[q & 1][warp];
-          for (int w = lane; w < PROB_WORDS; w += 32) eps[w] = src[w];
-          const OzMmaProblem* pp = probs + tq.prob;
-          const int eb = pp->eB[tq.nt * TN + hh * 32 + lane];
-          eps[40 + lane] = eb;
-          reinterpret_cast<double*>(eps + 72)[lane] = oz_pow2(eb);
-          my_eA = pp->eA[tq.mt * TM + qd * 32 + lane];
-          my_scA = oz_pow2(my_eA);
-          __syncwarp();
-        }
         if (!oz_wait_warp(oz_smem(&accf_bar), (uint32_t)(P & 1), abort_flag, err, wait_cycles)) {
           ok = false;
           break;
@@ -660,34 +667,28 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
         // -Im; P2: -Re, -Im; P3: +Im); alpha is folded in: (kr, ki) = alpha (sr, si)
         const double sr = (p == 2) ? 0.0 : (p == 0 ? 1.0 : -1.0);
         const double si = (p == 2) ? 1.0 : -1.0;
-        const cplx al = reinterpret_cast<const OzMmaProblem*>(ep_sh[q & 1][warp])->alpha;
         const double kr = al.x * sr - al.y * si, ki = al.x * si + al.y * sr;
 #pragma unroll
         for (int c8 = 0; c8 < 4; ++c8) {
           double v[8];
 #pragma unroll
           for (int j = 0; j < 8; ++j) v[j] = 0.0;
+          // all ND diagonals of the column group in one TMEM round trip
+          uint32_t x[ND][8];
 #pragma unroll
-          for (int g = 0; g < (ND + 3) / 4; ++g) {  // up to four diagonals per TMEM round trip
-            constexpr int kMax = 4;
-            const int nd = ND - 4 * g < kMax ? ND - 4 * g : kMax;
-            uint32_t x[kMax][8];
+          for (int d = 0; d < ND; ++d) {
+            const uint32_t addr = tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(d * TN + hh * 32 + c8 * 8);
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                         : "=r"(x[d][0]), "=r"(x[d][1]), "=r"(x[d][2]), "=r"(x[d][3]), "=r"(x[d][4]), "=r"(x[d][5]),
+                           "=r"(x[d][6]), "=r"(x[d][7])
+                         : "r"(addr));
+          }
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-            for (int dd = 0; dd < nd; ++dd) {
-              const int d = 4 * g + dd;
-              const uint32_t addr = tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(d * TN + hh * 32 + c8 * 8);
-              asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                           : "=r"(x[dd][0]), "=r"(x[dd][1]), "=r"(x[dd][2]), "=r"(x[dd][3]), "=r"(x[dd][4]),
-                             "=r"(x[dd][5]), "=r"(x[dd][6]), "=r"(x[dd][7])
-                           : "r"(addr));
-            }
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          for (int d = 0; d < ND; ++d) {
+            const double w = oz_diag_weight(d);
 #pragma unroll
-            for (int dd = 0; dd < nd; ++dd) {
-              const double w = oz_diag_weight(4 * g + dd);
-#pragma unroll
-              for (int j = 0; j < 8; ++j) v[j] = fma(oz_i2d(x[dd][j]), w, v[j]);
-            }
+            for (int j = 0; j < 8; ++j) v[j] = fma(oz_i2d(x[d][j]), w, v[j]);
           }
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
@@ -700,64 +701,86 @@ __global__ void __launch_bounds__(oz::THREADS, 1)
         if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(oz_smem(&acce_bar)) : "memory");
       }
       if (!ok) break;
+      // the next tile's inputs (into the other staging slot)
+      OzTile tn{};
+      int nx_eA = 0, nx_eB = 0;
+      cplx nx_al = make_double2(0.0, 0.0);
+      if (q + 1 < my_tiles) {
+        tn = oz_tile(tile_map, (int)blockIdx.x + (q + 1) * G);
+        fetch(q + 1, tn, nx_eA, nx_eB, nx_al);
+      }
       // C = alpha 2^(eA + eB) (Re, Im) + beta Cin + diag I (alpha already in
-      // cr, ci), from the staged descriptor and scales; Cin is read one group
-      // of columns ahead of the stores.  The producer keeps the tensor cores
-      // busy with the next tile meanwhile.
-      const int* eps = ep_sh[q & 1][warp];
-      const OzMmaProblem& ps = *reinterpret_cast<const OzMmaProblem*>(eps);
+      // cr, ci), from the staged descriptor and the shuffled column exponents
+      // (all lanes take part in the shuffles; rows past m skip the memory
+      // accesses); Cin is read one group of columns ahead of the stores.  The
+      // producer keeps the tensor cores busy with the next tile meanwhile.
+      const OzMmaProblem& ps = *reinterpret_cast<const OzMmaProblem*>(ep_sh[q & 1][warp]);
       const int r = tq.mt * TM + qd * 32 + lane;
-      if (r < ps.m) {
-        const int pn = ps.n, ldc = ps.ldc, ldcin = ps.ldcin;
-        const cplx beta = ps.beta;
-        cplx* const Cout = ps.C;
-        const cplx* const Cin = ps.Cin;
-        const cplx dg = ps.diag_ptr ? *ps.diag_ptr : ps.diag;
-        const bool has_cin = Cin && (beta.x != 0.0 || beta.y != 0.0);
-        const int c0 = tq.nt * TN + hh * 32;
-        constexpr int GW = 4;  // columns per group
-        cplx cb[GW], cn[GW];
+      const bool row_ok = r < ps.m;
+      const int pn = ps.n, ldc = ps.ldc, ldcin = ps.ldcin;
+      const cplx beta = ps.beta;
+      cplx* const Cout = ps.C;
+      const cplx* const Cin = ps.Cin;
+      const cplx dg = ps.diag_ptr ? *ps.diag_ptr : ps.diag;
+      const bool has_cin = row_ok && Cin && (beta.x != 0.0 || beta.y != 0.0);
+      // every exponent of the warp's rows and columns within +-500: the scale
+      // 2^(eA + eB) is a normal double built from its exponent bits
+      const bool pow2_ok = __all_sync(0xffffffffu, my_eA >= -500 && my_eA <= 500 && my_eB >= -500 && my_eB <= 500);
+      const int c0 = tq.nt * TN + hh * 32;
+      constexpr int GW = 4;  // columns per group
+      cplx cb[GW], cn[GW];
 #pragma unroll
-        for (int jj = 0; jj < GW; ++jj)
-          cn[jj] = (has_cin && c0 + jj < pn) ? Cin[r + (size_t)(c0 + jj) * ldcin] : make_double2(0.0, 0.0);
+      for (int jj = 0; jj < GW; ++jj)
+        cn[jj] = (has_cin && c0 + jj < pn) ? Cin[r + (size_t)(c0 + jj) * ldcin] : make_double2(0.0, 0.0);
 #pragma unroll
-        for (int g8 = 0; g8 < 32 / GW; ++g8) {
+      for (int g8 = 0; g8 < 32 / GW; ++g8) {
 #pragma unroll
-          for (int jj = 0; jj < GW; ++jj) cb[jj] = cn[jj];
-          if (g8 < 32 / GW - 1) {
-#pragma unroll
-            for (int jj = 0; jj < GW; ++jj) {
-              const int c = c0 + (g8 + 1) * GW + jj;
-              cn[jj] = (has_cin && c < pn) ? Cin[r + (size_t)c * ldcin] : make_double2(0.0, 0.0);
-            }
-          }
+        for (int jj = 0; jj < GW; ++jj) cb[jj] = cn[jj];
+        if (g8 < 32 / GW - 1) {
 #pragma unroll
           for (int jj = 0; jj < GW; ++jj) {
-            const int j = g8 * GW + jj;
-            const int c = c0 + j;
-            if (c >= pn) continue;
-            // alpha 2^(eA + eB) (Re, Im): two exact power-of-two factors when
-            // both exponents are moderate, else one ldexp
-            const double scB = reinterpret_cast<const double*>(eps + 72)[j];
-            double xr, xi;
-            if (my_scA != 0.0 && scB != 0.0) {
-              xr = cr[j] * my_scA * scB;
-              xi = ci[j] * my_scA * scB;
-            } else {
-              xr = ldexp(cr[j], my_eA + eps[40 + j]);
-              xi = ldexp(ci[j], my_eA + eps[40 + j]);
-            }
-            cplx v;
-            v.x = xr + (beta.x * cb[jj].x - beta.y * cb[jj].y);
-            v.y = xi + (beta.x * cb[jj].y + beta.y * cb[jj].x);
-            if (r == c) {
-              v.x += dg.x;
-              v.y += dg.y;
-            }
-            Cout[r + (size_t)c * ldc] = v;
+            const int c = c0 + (g8 + 1) * GW + jj;
+            cn[jj] = (has_cin && c < pn) ? Cin[r + (size_t)c * ldcin] : make_double2(0.0, 0.0);
           }
         }
+        int eB[GW];
+#pragma unroll
+        for (int jj = 0; jj < GW; ++jj) eB[jj] = __shfl_sync(0xffffffffu, my_eB, g8 * GW + jj);
+#pragma unroll
+        for (int jj = 0; jj < GW; ++jj) {
+          const int j = g8 * GW + jj;
+          const int c = c0 + j;
+          if (!row_ok || c >= pn) continue;
+          const int e = my_eA + eB[jj];
+          double xr, xi;
+          if (pow2_ok) {
+            const double sc = __longlong_as_double((long long)(e + 1023) << 52);
+            xr = cr[j] * sc;
+            xi = ci[j] * sc;
+          } else {
+            xr = ldexp(cr[j], e);
+            xi = ldexp(ci[j], e);
+          }
+          cplx v;
+          if (has_cin) {
+            v.x = fma(beta.x, cb[jj].x, fma(-beta.y, cb[jj].y, xr));
+            v.y = fma(beta.x, cb[jj].y, fma(beta.y, cb[jj].x, xi));
+          } else {
+            v.x = xr;
+            v.y = xi;
+          }
+          if (r == c) {
+            v.x += dg.x;
+            v.y += dg.y;
+          }
+          Cout[r + (size_t)c * ldc] = v;
+        }
       }
+      tq = tn;
+      my_eA = nx_eA;
+      my_eB = nx_eB;
+      al = nx_al;
+      __syncwarp();
     }
   }
   __syncwarp();
