@@ -362,6 +362,11 @@ def run_ours(args):
     fp64_peak = max(d1.value, d2.value)
     negf._lib.check(negf.load().negf_probe_int8_peak(ctypes.byref(d3)))
     int8_peak = d3.value
+    # FP64 arithmetic beside INT8 MMAs on one SM (cycles): the product kernel's
+    # FP64 drains cannot hide under its MMAs when beside ~ alone + mma
+    o1, o2, o3 = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    negf._lib.check(negf.load().negf_probe_fp64_int8_overlap(ctypes.byref(o1), ctypes.byref(o2), ctypes.byref(o3)))
+    overlap = {"fp64_alone_cycles": o1.value, "fp64_beside_int8_mma_cycles": o2.value, "int8_mma_cycles": o3.value}
     step_flops = canonical_flops(args.npl, args.b) * args.ne
     total_pts = args.ne * args.steps * world
     ev0 = torch.cuda.Event(enable_timing=True)
@@ -486,6 +491,7 @@ def run_ours(args):
     # DRAM bytes of the dominant kernel are an ncu measurement; this run is not
     # under ncu, so the per-launch traffic is not reported here
     roof["traffic"] = None
+    roof["fp64_beside_int8"] = overlap
     roof["share"] = k_ms / sum(v[0] for v in prof.values())
     roof["launch_ms"] = k_ms / max(1, k_n)
     whole = {"algorithmic_tflops": step_flops / ((ms / args.steps) / 1000.0) / 1e12,

@@ -454,6 +454,12 @@ int negf_bndiag_of_inv_direct(int32_t n, int32_t nnz, const int32_t* colptr, con
  * ---------------------------------------------------------------------- */
 int negf_probe_fp64_peak(double* dmma_tflops, double* dfma_tflops);
 int negf_probe_int8_peak(double* tops);
+/* Whether FP64 arithmetic progresses beside INT8 tensor-core MMAs on one SM:
+ * mean cycles of seven warps of DFMA chains alone, the same beside one thread
+ * issuing back-to-back 128 x 256 x 32 kind::i8 MMAs, and the MMA stream
+ * alone.  fp64_beside ~ fp64_alone + mma means the two do not overlap, so
+ * the product kernel's FP64 drains cost their full time. */
+int negf_probe_fp64_int8_overlap(double* fp64_alone_cycles, double* fp64_beside_mma_cycles, double* mma_cycles);
 
 /* ------------------------------------------------------------------------
  * Request server.  The reference has no request loop (one system and one

@@ -51,6 +51,7 @@ size_t ozaki_mma_smem_bytes();
 cudaError_t ozaki_prepare();
 // dense INT8 tensor-core throughput of this device, TOP/s
 cudaError_t ozaki_probe_int8(double* tops);
+cudaError_t ozaki_probe_overlap(double* fp64_alone, double* fp64_beside_mma, double* mma_alone);
 cudaError_t launch_ozaki_split(const void* probs, int nprob, int max_rows_pad, int max_k_pad, cudaStream_t st);
 // CSC <-> band blocks on the device (csc.cu); block table slot 3 i + (j - i + 1)
 cudaError_t launch_csc_scatter(int n, const int* colptr, const int* rowval, const cplx* nz, int nnz, const int* blk_of,

@@ -1482,4 +1482,11 @@ int negf_probe_int8_peak(double* tops) {
   return NEGF_SUCCESS;
 }
 
+int negf_probe_fp64_int8_overlap(double* fp64_alone_cycles, double* fp64_beside_mma_cycles, double* mma_cycles) {
+  if (int r = check_device()) return r;
+  cudaError_t e = ozaki_probe_overlap(fp64_alone_cycles, fp64_beside_mma_cycles, mma_cycles);
+  if (e != cudaSuccess) return cuda_fail(e, "overlap probe");
+  return NEGF_SUCCESS;
+}
+
 }  // extern "C"

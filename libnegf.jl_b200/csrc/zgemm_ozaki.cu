@@ -46,6 +46,7 @@
 
 #include <atomic>
 #include <cstdint>
+#include <vector>
 
 namespace negf {
 
@@ -869,6 +870,126 @@ cudaError_t ozaki_probe_int8(double* tops) {
   if (e != cudaSuccess) return e;
   if (h) return cudaErrorLaunchTimeout;
   if (tops) *tops = 2.0 * 128 * 256 * 32 * 32.0 * rounds * sms / (ms * 1e9);
+  return cudaSuccess;
+}
+
+// measurement: does FP64 arithmetic progress while the same SM's tensor cores
+// run INT8 MMAs?  Thread 0 issues back-to-back 128 x 256 x 32 kind::i8 MMAs
+// (when `mma`); warps 1..7 run eight independent DFMA chains per thread (when
+// `fp64`).  Per CTA, out[0] = cycles of the MMA thread, out[1] = mean cycles
+// of the FP64 warps.  The drain of the product kernel is placed by this
+// figure: FP64 work beside the MMAs only waits for them.
+__global__ void __launch_bounds__(256, 1) ozaki_overlap_probe_kernel(int mma, int fp64, int rounds, int iters,
+                                                                      long long* out, double* sink, int* err) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tm;
+  __shared__ long long fp_cycles;
+  for (int i = threadIdx.x; i < (4096 + 8192) / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(sm)[i] = 0x01010101u;
+  if (threadIdx.x < 32) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(oz_smem(&tm)), "r"(512));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (threadIdx.x == 0) {
+    fp_cycles = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(oz_smem(&bar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::);
+  const uint32_t t = tm;
+  if (threadIdx.x < 32) {
+    if (threadIdx.x == 0) {
+      const long long t0 = clock64();
+      if (mma) {
+        const uint64_t da = oz_desc(oz_smem(sm), 128 * 16, 128), db = oz_desc(oz_smem(sm) + 4096, 256 * 16, 128);
+        constexpr uint32_t idesc =
+            (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(256 >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+        for (int it = 0; it < rounds; ++it) {
+#pragma unroll
+          for (int u = 0; u < 32; ++u) {
+            const uint32_t acc = (it > 0 || u >= 2) ? 1u : 0u;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+                    t + (uint32_t)((u & 1) * 256)),
+                "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+          }
+        }
+      }
+      oz_commit(oz_smem(&bar));
+      int dummy = 0;
+      if (!oz_wait(oz_smem(&bar), 0, &dummy, err, false)) atomicExch(err, 1);
+      out[2 * blockIdx.x] = clock64() - t0;
+    }
+  } else {
+    const long long t0 = clock64();
+    double d[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) d[k] = 1.0 + threadIdx.x * 1e-3 + k;
+    if (fp64) {
+      for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) d[k] = fma(d[k], 0.999999, 1e-7);
+      }
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += d[k];
+    sink[blockIdx.x * blockDim.x + threadIdx.x] = s;
+    if ((threadIdx.x & 31) == 0) atomicAdd(reinterpret_cast<unsigned long long*>(&fp_cycles),
+                                           (unsigned long long)(clock64() - t0));
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::);
+  __syncthreads();
+  if (threadIdx.x == 0) out[2 * blockIdx.x + 1] = fp_cycles / 7;
+  if (threadIdx.x < 32) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::);
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(t), "r"(512));
+  }
+}
+
+cudaError_t ozaki_probe_overlap(double* fp64_alone, double* fp64_beside_mma, double* mma_alone) {
+  int dev = 0, sms = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  constexpr int smem = 160 * 1024;  // one CTA per SM
+  constexpr int rounds = 20, iters = 3000;
+  e = cudaFuncSetAttribute(ozaki_overlap_probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  long long* out = nullptr;
+  double* sink = nullptr;
+  int* err = nullptr;
+  if ((e = cudaMalloc(&out, sizeof(long long) * 2 * sms)) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&sink, sizeof(double) * 256 * sms)) != cudaSuccess) { cudaFree(out); return e; }
+  if ((e = cudaMalloc(&err, sizeof(int))) != cudaSuccess) { cudaFree(out); cudaFree(sink); return e; }
+  cudaMemset(err, 0, sizeof(int));
+  std::vector<long long> h(2 * (size_t)sms);
+  double res[3][2] = {};
+  const int modes[3][2] = {{0, 1}, {1, 1}, {1, 0}};  // (mma, fp64)
+  for (int m = 0; m < 3 && e == cudaSuccess; ++m) {
+    for (int rep = 0; rep < 2; ++rep)  // the first launch warms up
+      ozaki_overlap_probe_kernel<<<sms, 256, smem>>>(modes[m][0], modes[m][1], rounds, iters, out, sink, err);
+    e = cudaMemcpy(h.data(), out, sizeof(long long) * h.size(), cudaMemcpyDeviceToHost);
+    for (int b = 0; b < sms; ++b) {
+      res[m][0] += (double)h[2 * b] / sms;
+      res[m][1] += (double)h[2 * b + 1] / sms;
+    }
+  }
+  int herr = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&herr, err, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  cudaFree(out);
+  cudaFree(sink);
+  cudaFree(err);
+  if (e != cudaSuccess) return e;
+  if (herr) return cudaErrorLaunchTimeout;
+  if (fp64_alone) *fp64_alone = res[0][1];
+  if (fp64_beside_mma) *fp64_beside_mma = res[1][1];
+  if (mma_alone) *mma_alone = res[2][0];
   return cudaSuccess;
 }
 
