@@ -74,9 +74,10 @@ def parse():
     ap.add_argument("--systems", type=int, default=96, help="cfg4: number of systems in the sample")
     ap.add_argument("--requests", type=int, default=16, help="cfg5: number of requests in the sample")
     ap.add_argument("--rate", type=float, default=2.0, help="cfg5: mean arrival rate, requests/s")
-    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"], help="cfg4 / cfg5 precision")
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
+                    help="cfg4 / cfg5 / --launch-list precision")
     ap.add_argument("--launch-list", action="store_true",
-                    help="only two launch-by-launch passes of the mixed solver (for an ncu launch list: skip the "
+                    help="only two launch-by-launch passes of the solver (--precision; for an ncu launch list: skip the "
                          "first pass's launches, capture the second's); prints no bench line")
     a = ap.parse_args()
     dflt = {"cfg3": (64, 512, 128)}.get(a.workload, (32, 256, 256))
@@ -345,7 +346,7 @@ def run_ours(args):
     sh = stream.cuda_stream
     per = sum(b * b for b in dev.sizes)
     if args.launch_list:
-        solver = negf.Solver(dev, args.ne, eta=sysm.eta, precision="mixed")
+        solver = negf.Solver(dev, args.ne, eta=sysm.eta, precision=args.precision)
         solver.set_energies(my_E, sh)
         for _ in range(2):
             solver.run_profiled(sh)
