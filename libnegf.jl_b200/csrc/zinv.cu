@@ -319,17 +319,30 @@ __global__ void __launch_bounds__(GJ_THREADS, 1)
     }
   }
   for (int c = tid; c < w; c += GJ_THREADS) pp->piv[k0 + c] = sh_piv[c];
-  // Bbuf = W[P, :] with panel columns zeroed  (w x n, ld w)
+  // Bbuf = W[P, :] with panel columns zeroed  (w x n, ld w): element e = c +
+  // j w is W[piv_c, j]; the pivot rows are scattered, so every thread keeps
+  // GU gathers in flight before it stores them
   {
     const cplx* W = pp->W;
     cplx* Bbuf = pp->Bbuf;
     const int ld = pp->ld;
-    for (int j = warp; j < n; j += NW) {
-      const bool inK = (j >= k0 && j < k0 + w);
-      for (int c = lane; c < w; c += 32) {
-        cplx v = make_double2(0.0, 0.0);
-        if (!inK) v = W[sh_piv[c] + (size_t)j * ld];
-        Bbuf[c + (size_t)j * w] = v;
+    const int total = w * n;
+    constexpr int GU = 8;
+    for (int e0 = tid; e0 < total; e0 += GU * GJ_THREADS) {
+      cplx v[GU];
+#pragma unroll
+      for (int u = 0; u < GU; ++u) {
+        const int e = e0 + u * GJ_THREADS;
+        v[u] = make_double2(0.0, 0.0);
+        if (e < total) {
+          const int c = e % w, j = e / w;
+          if (j < k0 || j >= k0 + w) v[u] = W[sh_piv[c] + (size_t)j * ld];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < GU; ++u) {
+        const int e = e0 + u * GJ_THREADS;
+        if (e < total) Bbuf[e] = v[u];
       }
     }
   }
