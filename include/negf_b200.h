@@ -448,6 +448,17 @@ int negf_bndiag_of_inv_direct(int32_t n, int32_t nnz, const int32_t* colptr, con
                               CCscMatrix* result);
 
 /* ------------------------------------------------------------------------
+ * Device memory of finished plans.  The reference allocates per call through
+ * Julia's GC; here the workspace of a destroyed plan (solver, sweep, server
+ * group) stays with the library, per device, and is reused by the next plans
+ * (at most half of the device's memory is kept; the library's own HBM budget
+ * queries count it as free, and a failed allocation releases it and retries).
+ * This call hands all of it back to the driver, for callers that allocate
+ * device memory outside the library after a solve.
+ * ---------------------------------------------------------------------- */
+int negf_release_cached_memory(void);
+
+/* ------------------------------------------------------------------------
  * Measurement helpers (roofline denominators measured on the device):
  * FP64 throughput of the tensor (mma.sync f64) and DFMA paths, TFLOP/s, for
  * the FP64 path; dense INT8 tcgen05 throughput, TOP/s, for the mixed path.

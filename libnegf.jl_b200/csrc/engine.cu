@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <set>
 #include <tuple>
 
@@ -56,11 +57,95 @@ int TriSystem::maxb() const {
 // ---------------------------------------------------------------------------
 // Plan
 
+namespace {
+// Per-device cache of freed plan chunks, keyed by size.  It holds at most half
+// of the device's memory; a chunk that does not fit is freed.
+struct ChunkCache {
+  std::mutex mu;
+  std::map<int, std::multimap<size_t, void*>> free_by_dev;
+  std::map<int, size_t> bytes;
+  std::map<int, size_t> total;  // device memory, read once per device
+};
+ChunkCache& chunk_cache() {
+  static ChunkCache* c = new ChunkCache();  // kept until exit: chunks may be returned during teardown
+  return *c;
+}
+int current_device() {
+  int d = 0;
+  cudaGetDevice(&d);
+  return d;
+}
+// a cached chunk of at least `bytes` and at most 5/4 of it, or null
+void* cache_take(size_t bytes, size_t* got) {
+  ChunkCache& c = chunk_cache();
+  std::lock_guard<std::mutex> lk(c.mu);
+  const int d = current_device();
+  auto& m = c.free_by_dev[d];
+  auto it = m.lower_bound(bytes);
+  if (it == m.end() || it->first > bytes + bytes / 4) return nullptr;
+  void* p = it->second;
+  *got = it->first;
+  c.bytes[d] -= it->first;
+  m.erase(it);
+  return p;
+}
+void cache_put(void* p, size_t bytes) {
+  ChunkCache& c = chunk_cache();
+  const int d = current_device();
+  {
+    std::lock_guard<std::mutex> lk(c.mu);
+    size_t& tot = c.total[d];
+    if (tot == 0) {
+      size_t fr = 0;
+      if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) tot = 0;
+    }
+    if (c.bytes[d] + bytes <= tot / 2) {
+      c.free_by_dev[d].emplace(bytes, p);
+      c.bytes[d] += bytes;
+      return;
+    }
+  }
+  cudaFree(p);
+}
+void cache_flush(int d) {
+  ChunkCache& c = chunk_cache();
+  std::lock_guard<std::mutex> lk(c.mu);
+  for (auto& kv : c.free_by_dev[d]) cudaFree(kv.second);
+  c.free_by_dev[d].clear();
+  c.bytes[d] = 0;
+}
+}  // namespace
+
+size_t cached_bytes(int device) {
+  ChunkCache& c = chunk_cache();
+  std::lock_guard<std::mutex> lk(c.mu);
+  auto it = c.bytes.find(device);
+  return it == c.bytes.end() ? 0 : it->second;
+}
+
+void release_cached_memory() {
+  int n = 0, cur = 0;
+  cudaGetDevice(&cur);
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return;
+  for (int d = 0; d < n; ++d) {
+    if (cached_bytes(d) == 0) continue;
+    cudaSetDevice(d);
+    cache_flush(d);
+  }
+  cudaSetDevice(cur);
+}
+
 Plan::~Plan() {
   if (gexec_) cudaGraphExecDestroy(gexec_);
   if (graph_) cudaGraphDestroy(graph_);
+  // the chunks go back to the cache once no work that uses them is left on
+  // the device (cudaFree would wait for that as well)
+  const bool idle = cudaDeviceSynchronize() == cudaSuccess;
   if (dblob_) cudaFree(dblob_);
-  for (void* p : owned_) cudaFree(p);
+  for (auto& c : owned_) {
+    if (idle) cache_put(c.first, c.second);
+    else cudaFree(c.first);
+  }
 }
 
 // Workspace comes from a bump arena of zeroed chunks: the first is 1 MiB and
@@ -68,14 +153,25 @@ Plan::~Plan() {
 // costs a handful of cudaMalloc calls instead of one per block; a request of
 // 32 MiB or more gets a chunk of its own.  Every piece is 256-byte aligned.
 void* Plan::raw_alloc(size_t bytes) {
-  void* p = nullptr;
-  if (cudaMalloc(&p, bytes) != cudaSuccess) throw std::bad_alloc();
+  size_t got = bytes;
+  void* p = cache_take(bytes, &got);
+  if (!p) {
+    got = bytes;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+      cudaGetLastError();  // clear the allocation error, then retry without the cache
+      cache_flush(current_device());
+      if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        throw std::bad_alloc();
+      }
+    }
+  }
   if (cudaMemset(p, 0, bytes) != cudaSuccess) {
     cudaFree(p);
     throw std::bad_alloc();
   }
-  owned_.push_back(p);
-  owned_bytes_ += bytes;
+  owned_.push_back({p, got});
+  owned_bytes_ += got;
   return p;
 }
 

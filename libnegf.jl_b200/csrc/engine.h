@@ -201,7 +201,7 @@ class Plan {
   void* raw_alloc(size_t bytes);
   std::vector<unsigned char> blob_;
   void* dblob_ = nullptr;
-  std::vector<void*> owned_;
+  std::vector<std::pair<void*, size_t>> owned_;  // chunks and their sizes
   size_t owned_bytes_ = 0;
   std::vector<std::pair<size_t, int>> marks_;
   unsigned char* chunk_ = nullptr;  // bump pointer into the current chunk
@@ -301,6 +301,13 @@ int build_ddrgf_level(Plan& plan, const std::vector<TriSystem>& sys, std::vector
                       const std::vector<int>& d1s, size_t level);
 // Levels of the library's GPU cost model for nsys systems of npl layers of b.
 std::vector<int> choose_levels(int npl, int b, int nsys, int max_levels);
+
+// Device chunks of destroyed plans are kept per device for the next plans
+// (cudaFree of hundreds of chunks costs ~1 ms each and synchronises the
+// device): cached_bytes() is memory the library holds but can hand out again,
+// release_cached_memory() returns it to the driver.
+size_t cached_bytes(int device);
+void release_cached_memory();
 
 std::string& last_error();
 void set_error(const std::string& msg);

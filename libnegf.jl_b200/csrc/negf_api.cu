@@ -1149,6 +1149,7 @@ int negf_solve(negf_device_t dev, int32_t nE, const double* energies, const negf
   if (o.max_chunk <= 0) {
     size_t fr = 0, tot = 0;
     NEGF_TRY_CUDA(cudaMemGetInfo(&fr, &tot), "negf_solve");
+    { int d = 0; cudaGetDevice(&d); fr += cached_bytes(d); }  // the library's cached chunks are free to it
     double budget = o.hbm_budget_gb > 0 ? o.hbm_budget_gb * 1e9 : 0.8 * (double)fr;
     size_t per = solver_bytes_per_energy(*dev, o);
     int fit = (int)std::max(1.0, std::floor(budget / (double)per));
@@ -1280,6 +1281,7 @@ int negf_device_selected_inverse(negf_device_t dev, int32_t nE, const double* en
   if (opts->max_chunk <= 0) {
     size_t fr = 0, tot = 0;
     NEGF_TRY_CUDA(cudaMemGetInfo(&fr, &tot), "negf_device_selected_inverse");
+    { int d = 0; cudaGetDevice(&d); fr += cached_bytes(d); }
     const double budget = opts->hbm_budget_gb > 0 ? opts->hbm_budget_gb * 1e9 : 0.8 * (double)fr;
     const int d1 = nlevels > 0 ? fixed_d1s[0] : 16;
     const size_t per = selinv_bytes_per_energy(d, method, d1, mixed, !out_on_device);
@@ -1472,6 +1474,11 @@ int negf_probe_fp64_peak(double* dmma_tflops, double* dfma_tflops) {
   cudaError_t e = cudaGetLastError();
   cudaFree(out);
   if (e != cudaSuccess) return cuda_fail(e, "probe");
+  return NEGF_SUCCESS;
+}
+
+int negf_release_cached_memory(void) {
+  negf::release_cached_memory();
   return NEGF_SUCCESS;
 }
 

@@ -295,7 +295,13 @@ int negf_server_create_ex(const negf_solve_opts* opts, double budget_gb, int32_t
     S->budget = budget_gb * 1e9;
   } else {
     size_t fr = 0, tot = 0;
-    S->budget = cudaMemGetInfo(&fr, &tot) == cudaSuccess ? 0.8 * (double)fr : 0.0;
+    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
+      int d = 0;
+      cudaGetDevice(&d);
+      S->budget = 0.8 * (double)(fr + negf::cached_bytes(d));  // cached plan chunks are free to the library
+    } else {
+      S->budget = 0.0;
+    }
   }
   for (int k = 0; k < lanes; ++k) S->workers.emplace_back(lane_loop, S);
   *out = S;

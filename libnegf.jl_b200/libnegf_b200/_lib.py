@@ -161,6 +161,7 @@ PROTOTYPES = {
                                         ctypes.POINTER(ctypes.c_char_p), c_int32_p, ctypes.c_int32]),
     "negf_probe_fp64_peak": (ctypes.c_int, [c_double_p, c_double_p]),
     "negf_probe_int8_peak": (ctypes.c_int, [c_double_p]),
+    "negf_release_cached_memory": (ctypes.c_int, []),
     "negf_probe_fp64_int8_overlap": (ctypes.c_int, [c_double_p, c_double_p, c_double_p]),
 }
 

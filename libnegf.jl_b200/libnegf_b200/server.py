@@ -271,15 +271,30 @@ class NativeServer:
                 return out
             return split(gr), split(gl), t
 
-    def submit(self, Hd, Hu, sigL, sigR, energies, want_blocks=True):
+    def submit(self, Hd, Hu, sigL, sigR, energies, want_blocks=True, out=None):
+        """Queue one request.  ``out`` = (gr, gl, t): caller-owned flat output
+        arrays (complex128 of len(energies) * sum b_i^2, float64 of
+        len(energies)) that the results are written into -- e.g. views of
+        pinned host memory reused across requests, which receive at DMA speed;
+        by default fresh arrays are allocated (their pages are first touched by
+        the copy, which costs several times the transfer itself)."""
         import ctypes
         from .negf import _host_blocks
         E = np.ascontiguousarray(np.asarray(energies, dtype=np.float64))
         sizes = [int(h.shape[0]) for h in Hd]
         per = sum(b * b for b in sizes)
-        gr = np.empty(len(E) * per, dtype=np.complex128) if want_blocks else None
-        gl = np.empty(len(E) * per, dtype=np.complex128) if want_blocks else None
-        t = np.empty(len(E), dtype=np.float64)
+        if out is not None:
+            gr, gl, t = out
+            for a, n, dt in ((gr, len(E) * per, np.complex128), (gl, len(E) * per, np.complex128),
+                             (t, len(E), np.float64)):
+                if a is not None and (a.dtype != dt or a.size < n or not a.flags.c_contiguous):
+                    raise ValueError("out arrays: contiguous %s of at least %d elements" % (np.dtype(dt).name, n))
+            if t is None:
+                raise ValueError("out: t is required")
+        else:
+            gr = np.empty(len(E) * per, dtype=np.complex128) if want_blocks else None
+            gl = np.empty(len(E) * per, dtype=np.complex128) if want_blocks else None
+            t = np.empty(len(E), dtype=np.float64)
         kd, pd = _host_blocks(Hd)
         ku, pu = _host_blocks(Hu)
         sl = np.asfortranarray(np.asarray(sigL, dtype=np.complex128))
