@@ -75,6 +75,19 @@ int current_device() {
   cudaGetDevice(&d);
   return d;
 }
+// a non-blocking stream per device for zeroing new chunks (no legacy-stream work)
+cudaStream_t zero_stream() {
+  static std::mutex mu;
+  static std::map<int, cudaStream_t> streams;
+  std::lock_guard<std::mutex> lk(mu);
+  const int d = current_device();
+  auto it = streams.find(d);
+  if (it != streams.end()) return it->second;
+  cudaStream_t s = nullptr;
+  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) s = nullptr;
+  streams[d] = s;
+  return s;
+}
 // a cached chunk of at least `bytes` and at most 5/4 of it, or null
 void* cache_take(size_t bytes, size_t* got) {
   ChunkCache& c = chunk_cache();
@@ -138,14 +151,33 @@ void release_cached_memory() {
 Plan::~Plan() {
   if (gexec_) cudaGraphExecDestroy(gexec_);
   if (graph_) cudaGraphDestroy(graph_);
-  // the chunks go back to the cache once no work that uses them is left on
-  // the device (cudaFree would wait for that as well)
-  const bool idle = cudaDeviceSynchronize() == cudaSuccess;
+  // The chunks go back to the cache once the last recorded use on every
+  // stream is complete.  Only those uses are waited for: a device-wide
+  // synchronisation would invalidate CUDA-graph captures that other threads
+  // have in progress.  A plan without recorded uses, or whose wait fails,
+  // frees its chunks (cudaFree waits for the device itself).
+  bool idle = !fences_.empty();
+  for (auto& f : fences_) {
+    if (cudaEventSynchronize(f.second) != cudaSuccess) idle = false;
+    cudaEventDestroy(f.second);
+  }
+  if (!idle) cudaGetLastError();
   if (dblob_) cudaFree(dblob_);
   for (auto& c : owned_) {
     if (idle) cache_put(c.first, c.second);
     else cudaFree(c.first);
   }
+}
+
+void Plan::fence(cudaStream_t s) {
+  cudaEvent_t ev = nullptr;
+  for (auto& f : fences_)
+    if (f.first == s) ev = f.second;
+  if (!ev) {
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return;
+    fences_.push_back({s, ev});
+  }
+  cudaEventRecord(ev, s);
 }
 
 // Workspace comes from a bump arena of zeroed chunks: the first is 1 MiB and
@@ -166,7 +198,10 @@ void* Plan::raw_alloc(size_t bytes) {
       }
     }
   }
-  if (cudaMemset(p, 0, bytes) != cudaSuccess) {
+  // zeroed before the chunk is handed out: callers write plan memory from
+  // their own streams before the plan is finalised
+  cudaStream_t zs = zero_stream();
+  if (!zs || cudaMemsetAsync(p, 0, bytes, zs) != cudaSuccess || cudaStreamSynchronize(zs) != cudaSuccess) {
     cudaFree(p);
     throw std::bad_alloc();
   }
@@ -575,11 +610,11 @@ cudaError_t Plan::run_events(cudaStream_t stream, const std::vector<cudaEvent_t>
   const unsigned char* base = static_cast<const unsigned char*>(dblob_);
   for (size_t i = 0; i < steps.size(); ++i) {
     e = launch_step(steps[i], base, stream);
-    if (e != cudaSuccess) return e;
-    e = cudaEventRecord(events[i + 1], stream);
-    if (e != cudaSuccess) return e;
+    if (e == cudaSuccess) e = cudaEventRecord(events[i + 1], stream);
+    if (e != cudaSuccess) break;
   }
-  return cudaSuccess;
+  fence(stream);
+  return e;
 }
 
 cudaError_t Plan::run_marked(cudaStream_t stream, const std::function<cudaError_t(int)>& at_mark) {
@@ -587,19 +622,23 @@ cudaError_t Plan::run_marked(cudaStream_t stream, const std::function<cudaError_
   if (e != cudaSuccess) return e;
   const unsigned char* base = static_cast<const unsigned char*>(dblob_);
   size_t m = 0;
-  for (size_t i = 0; i <= steps.size(); ++i) {
-    for (; m < marks_.size() && marks_[m].first == i; ++m)
-      if ((e = at_mark(marks_[m].second)) != cudaSuccess) return e;
-    if (i == steps.size()) break;
-    if ((e = launch_step(steps[i], base, stream)) != cudaSuccess) return e;
+  for (size_t i = 0; i <= steps.size() && e == cudaSuccess; ++i) {
+    for (; m < marks_.size() && marks_[m].first == i && e == cudaSuccess; ++m) e = at_mark(marks_[m].second);
+    if (i == steps.size() || e != cudaSuccess) break;
+    e = launch_step(steps[i], base, stream);
   }
-  return cudaSuccess;
+  fence(stream);
+  return e;
 }
 
 cudaError_t Plan::run(cudaStream_t stream, bool use_graph) {
   cudaError_t e = finalize();
   if (e != cudaSuccess) return e;
-  if (use_graph && gexec_ && graph_stream_ == stream) return cudaGraphLaunch(gexec_, stream);
+  if (use_graph && gexec_ && graph_stream_ == stream) {
+    e = cudaGraphLaunch(gexec_, stream);
+    fence(stream);
+    return e;
+  }
   if (use_graph) {
     e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return e;
@@ -623,8 +662,11 @@ cudaError_t Plan::run(cudaStream_t stream, bool use_graph) {
     e = cudaGraphInstantiate(&gexec_, graph_, 0);
     if (e != cudaSuccess) return e;
     graph_stream_ = stream;
-    return cudaGraphLaunch(gexec_, stream);
+    e = cudaGraphLaunch(gexec_, stream);
+    fence(stream);
+    return e;
   }
+  fence(stream);
   return e;
 }
 

@@ -177,6 +177,12 @@ class Plan {
   void trtri(const std::vector<TriSpec>& specs, bool upper);
 
   cudaError_t finalize();
+  // Records a plan-owned event on s after work that uses the plan's memory
+  // (every run does it; callers add it after their own uploads outside a
+  // run).  The destructor waits for these events before the chunks are
+  // reused: events stay valid after their streams are destroyed, and waiting
+  // for them leaves other threads' graph captures alone.
+  void fence(cudaStream_t s);
   cudaError_t run(cudaStream_t stream, bool use_graph);
   // Launch-by-launch replay with a CUDA event recorded after every launch
   // (events[0] before the first); events must hold steps.size() + 1 events.
@@ -202,6 +208,7 @@ class Plan {
   std::vector<unsigned char> blob_;
   void* dblob_ = nullptr;
   std::vector<std::pair<void*, size_t>> owned_;  // chunks and their sizes
+  std::vector<std::pair<cudaStream_t, cudaEvent_t>> fences_;  // last use of the memory per stream (fence)
   size_t owned_bytes_ = 0;
   std::vector<std::pair<size_t, int>> marks_;
   unsigned char* chunk_ = nullptr;  // bump pointer into the current chunk

@@ -163,6 +163,8 @@ struct negf_solver_s {
   cudaStream_t copy_stream = nullptr;  // overlapped downloads (negf_solver_run_download)
   cudaEvent_t mark_ev = nullptr, join_ev = nullptr;
   ~negf_solver_s() {
+    // downloads on the copy stream read plan memory: done before the plan goes
+    if (copy_stream) cudaStreamSynchronize(copy_stream);
     for (auto& v : ev_sets)
       for (cudaEvent_t e : v) cudaEventDestroy(e);
     if (mark_ev) cudaEventDestroy(mark_ev);
@@ -964,6 +966,7 @@ int negf_solver_set_energies(negf_solver_t s, const double* energies, void* stre
   NEGF_TRY_CUDA(cudaMemcpyAsync(s->params, p.data(), p.size() * sizeof(cplx), cudaMemcpyHostToDevice, st),
                 "set energies");
   NEGF_TRY_CUDA(cudaMemsetAsync(s->info, 0, sizeof(int) * nE, st), "set energies");
+  s->plan->fence(st);
   return NEGF_SUCCESS;
 }
 

@@ -29,6 +29,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -52,6 +53,7 @@ struct Outcome {
   bool done = false;
   int status = NEGF_SUCCESS;
   double latency_s = 0.0;
+  std::string message;  // the lane's error text of a failed request
 };
 
 size_t per_energy(const std::vector<int32_t>& sizes) {
@@ -172,12 +174,14 @@ int solve_group(negf_server_s& S, const std::vector<Request*>& group, cudaStream
 
 void finish(negf_server_s& S, std::vector<std::unique_ptr<Request>>& reqs, int status) {
   const auto now = Clock::now();
+  const std::string msg = status == NEGF_SUCCESS ? std::string() : negf::last_error();
   for (auto& q : reqs) negf_device_destroy(q->dev);
   std::lock_guard<std::mutex> lk(S.mu);
   for (auto& q : reqs) {
     Outcome& oc = S.outcomes[q->ticket];
     oc.done = true;
     oc.status = status;
+    oc.message = msg;
     oc.latency_s = std::chrono::duration<double>(now - q->arrival).count();
     if (status == NEGF_SUCCESS) S.latencies.push_back(oc.latency_s);
   }
@@ -364,7 +368,7 @@ int negf_server_poll(negf_server_t S, int64_t ticket, int32_t* done) {
   }
   *done = it->second.done ? 1 : 0;
   if (it->second.done && it->second.status != NEGF_SUCCESS)
-    negf::set_error("negf_server_poll: the request failed (its status is returned)");
+    negf::set_error("negf_server_poll: the request failed: " + it->second.message);
   return it->second.done ? it->second.status : NEGF_SUCCESS;
 }
 
@@ -387,7 +391,7 @@ int negf_server_wait(negf_server_t S, int64_t ticket, double timeout_s, double* 
   }
   const Outcome oc = S->outcomes[ticket];
   if (latency_s) *latency_s = oc.latency_s;
-  if (oc.status != NEGF_SUCCESS) negf::set_error("negf_server_wait: the request failed (its status is returned)");
+  if (oc.status != NEGF_SUCCESS) negf::set_error("negf_server_wait: the request failed: " + oc.message);
   return oc.status;
 }
 
