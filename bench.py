@@ -715,7 +715,7 @@ def request_stream(n_req, rate, seed, npl_range, b_choices, ne_range, ne_div=1):
     return reqs, rng.exponential(1.0 / rate, size=n_req)
 
 
-def serve_stream(reqs, gaps, precision, lanes=2, receive="pinned"):
+def serve_stream(reqs, gaps, precision, lanes=4, receive="pinned"):
     """Submit the requests at their arrival times to the library's request
     server (negf_server_*, continuous batching over `lanes` streams) and wait
     for all; latency = entry into submit to completion.  receive="pinned": the
@@ -757,7 +757,7 @@ def serve_stream(reqs, gaps, precision, lanes=2, receive="pinned"):
 def run_cfg5(args):
     """Request stream: seeded requests (N in {16..128}, b in {64..512}, energy
     lists of 32..1024 scaled to a bounded sample) arriving as a Poisson process
-    at --rate, served by the library's request server (two lanes, continuous
+    at --rate, served by the library's request server (four lanes, continuous
     batching) in FP64 and in the mixed precision mode; latency = entry into
     submit to completion."""
     import torch
