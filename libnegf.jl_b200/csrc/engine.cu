@@ -285,46 +285,99 @@ void Plan::gemm_mixed(char opA, char opB, const std::vector<ZGemmProblem>& probs
     return id;
   };
   for (size_t i = 0; i < probs.size(); ++i) which[i] = {get(key_of(probs[i], true)), get(key_of(probs[i], false))};
-  // scratch layout of this step's digit slices (shared pool, grown as needed)
-  std::vector<size_t> off_s(keys.size()), off_e(keys.size());
-  std::vector<int> rpad(keys.size()), kpad(keys.size());
-  size_t need = 0;
-  for (size_t i = 0; i < keys.size(); ++i) {
+  // Digits the previous mixed step made are used again when no other step
+  // came in between, the operand view is the same (pointer, strides, shape,
+  // conjugation, side) and none of that step's products wrote into it.
+  if (steps.size() != oz_prev_steps_) {
+    oz_prev_.clear();
+    oz_prev_out_.clear();
+    oz_prev_end_ = 0;
+  }
+  auto view_key = [](const OzKey& k) {
+    return std::vector<long long>{(long long)(uintptr_t)k.X, k.sr, k.sk, k.rows, k.cols, k.conj, k.side};
+  };
+  auto written_before = [&](const OzKey& k) {
+    const char* lo = reinterpret_cast<const char*>(k.X);
+    const char* hi = lo + sizeof(cplx) * ((size_t)(k.rows - 1) * k.sr + (size_t)(k.cols - 1) * k.sk + 1);
+    for (const auto& r : oz_prev_out_)
+      if (lo < r.second && r.first < hi) return true;
+    return false;
+  };
+  const size_t nk = keys.size();
+  std::vector<int> rpad(nk), kpad(nk);
+  std::vector<int8_t*> slc(nk, nullptr);
+  std::vector<int*> exs(nk, nullptr);
+  bool any_reuse = false;
+  for (size_t i = 0; i < nk; ++i) {
     rpad[i] = round_up(std::max(keys[i].rows, 1), keys[i].side == 0 ? 128 : 64);
     kpad[i] = round_up(std::max(keys[i].cols, 1), 32);
-    off_s[i] = need;
-    need += (size_t)21 * rpad[i] * kpad[i];  // 3 real operands x 7 digit slices
-    need = (need + 255) & ~size_t(255);
-    off_e[i] = need;
-    need += sizeof(int) * (size_t)rpad[i];
-    need = (need + 255) & ~size_t(255);
+    auto it = oz_prev_.find(view_key(keys[i]));
+    if (it != oz_prev_.end() && it->second.rpad == rpad[i] && it->second.kpad == kpad[i] && !written_before(keys[i])) {
+      slc[i] = it->second.slices;
+      exs[i] = it->second.exps;
+      any_reuse = true;
+    }
   }
+  // new digits: 3 real operands x 7 digit slices, then a scale per row; they go
+  // after the reused ones when those are in the pool and there is room, else
+  // the pool is laid out afresh (and grown as needed) without reuse
+  std::vector<size_t> off_s(nk, 0), off_e(nk, 0);
+  auto layout = [&](size_t base) {
+    size_t need = base;
+    for (size_t i = 0; i < nk; ++i) {
+      if (slc[i]) continue;
+      off_s[i] = need;
+      need += (size_t)21 * rpad[i] * kpad[i];
+      need = (need + 255) & ~size_t(255);
+      off_e[i] = need;
+      need += sizeof(int) * (size_t)rpad[i];
+      need = (need + 255) & ~size_t(255);
+    }
+    return need;
+  };
+  size_t base = 0, need = 0;
+  if (any_reuse && oz_prev_pool_ == oz_pool_ && layout(oz_prev_end_) <= oz_pool_bytes_) {
+    base = oz_prev_end_;
+  } else if (any_reuse) {
+    any_reuse = false;
+    for (size_t i = 0; i < nk; ++i) {
+      slc[i] = nullptr;
+      exs[i] = nullptr;
+    }
+  }
+  need = layout(base);
   if (need > oz_pool_bytes_) {
     oz_pool_ = static_cast<unsigned char*>(alloc(need));
     oz_pool_bytes_ = need;
   }
-  std::vector<OzSplitProblem> sp(keys.size());
+  std::vector<OzSplitProblem> sp;
   int max_rows = 0, max_kpad = 0;
   double split_bytes = 0.0;
-  for (size_t i = 0; i < keys.size(); ++i) {
-    OzSplitProblem& s = sp[i];
-    s.X = keys[i].X; s.sr = keys[i].sr; s.sk = keys[i].sk;
-    s.rows = keys[i].rows; s.cols = keys[i].cols; s.rows_pad = rpad[i]; s.k_pad = kpad[i];
-    s.conj = keys[i].conj; s.tile_rows = keys[i].side == 0 ? 128 : 64;
-    s.slices = reinterpret_cast<int8_t*>(oz_pool_ + off_s[i]);
-    s.exps = reinterpret_cast<int*>(oz_pool_ + off_e[i]);
+  for (size_t i = 0; i < nk; ++i) {
+    if (slc[i]) continue;
+    slc[i] = reinterpret_cast<int8_t*>(oz_pool_ + off_s[i]);
+    exs[i] = reinterpret_cast<int*>(oz_pool_ + off_e[i]);
+    OzSplitProblem q;
+    q.X = keys[i].X; q.sr = keys[i].sr; q.sk = keys[i].sk;
+    q.rows = keys[i].rows; q.cols = keys[i].cols; q.rows_pad = rpad[i]; q.k_pad = kpad[i];
+    q.conj = keys[i].conj; q.tile_rows = keys[i].side == 0 ? 128 : 64;
+    q.slices = slc[i];
+    q.exps = exs[i];
+    sp.push_back(q);
     max_rows = std::max(max_rows, rpad[i]);
     max_kpad = std::max(max_kpad, kpad[i]);
     split_bytes += 16.0 * keys[i].rows * keys[i].cols + 21.0 * rpad[i] * kpad[i] + 4.0 * rpad[i];
   }
-  Step s1;
-  s1.kind = Step::OZ_SPLIT;
-  s1.off = push_bytes(sp.data(), sp.size() * sizeof(OzSplitProblem));
-  s1.count = (int)sp.size();
-  s1.max_m = max_rows;
-  s1.max_n = max_kpad;
-  s1.bytes = split_bytes;
-  steps.push_back(s1);
+  if (!sp.empty()) {
+    Step s1;
+    s1.kind = Step::OZ_SPLIT;
+    s1.off = push_bytes(sp.data(), sp.size() * sizeof(OzSplitProblem));
+    s1.count = (int)sp.size();
+    s1.max_m = max_rows;
+    s1.max_n = max_kpad;
+    s1.bytes = split_bytes;
+    steps.push_back(s1);
+  }
   std::vector<OzMmaProblem> mp;
   std::vector<int> tmap;  // 4 ints per output tile, see launch_ozaki_mma
   int total = 0;
@@ -333,7 +386,7 @@ void Plan::gemm_mixed(char opA, char opB, const std::vector<ZGemmProblem>& probs
     const ZGemmProblem& p = probs[i];
     const int a = which[i].first, b = which[i].second;
     OzMmaProblem q;
-    q.SA = sp[a].slices; q.eA = sp[a].exps; q.SB = sp[b].slices; q.eB = sp[b].exps;
+    q.SA = slc[a]; q.eA = exs[a]; q.SB = slc[b]; q.eB = exs[b];
     q.C = p.C; q.Cin = p.Cin; q.diag_ptr = p.diag_ptr;
     q.m = p.m; q.n = p.n; q.m_pad = rpad[a]; q.n_pad = rpad[b]; q.k_pad = kpad[a];
     q.ldc = p.ldc; q.ldcin = p.ldcin; q.pad_ = 0;
@@ -358,6 +411,18 @@ void Plan::gemm_mixed(char opA, char opB, const std::vector<ZGemmProblem>& probs
   s2.flops = fl;
   s2.form = oz_pairs_;
   steps.push_back(s2);
+  // what the next mixed step may use again
+  oz_prev_.clear();
+  for (size_t i = 0; i < nk; ++i) oz_prev_[view_key(keys[i])] = OzSplitDone{slc[i], exs[i], rpad[i], kpad[i]};
+  oz_prev_out_.clear();
+  for (const auto& p : probs) {
+    if (p.m <= 0 || p.n <= 0) continue;
+    const char* lo = reinterpret_cast<const char*>(p.C);
+    oz_prev_out_.push_back({lo, lo + sizeof(cplx) * ((size_t)(p.n - 1) * p.ldc + p.m)});
+  }
+  oz_prev_end_ = need;
+  oz_prev_pool_ = oz_pool_;
+  oz_prev_steps_ = steps.size();
 }
 
 void Plan::gemm_fp64(char opA, char opB, const std::vector<ZGemmProblem>& probs) {

@@ -11,6 +11,7 @@
 
 #include <string>
 #include <functional>
+#include <map>
 #include <vector>
 #include <cstddef>
 
@@ -223,6 +224,20 @@ class Plan {
   int* err_ = nullptr;            // tensor-core wait time-out flag (device int)
   unsigned char* oz_pool_ = nullptr;  // digit-slice scratch shared by all mixed steps
   size_t oz_pool_bytes_ = 0;
+  // Digits of the previous mixed step, reusable by the next one when no other
+  // step comes in between and its products did not write the operand: per
+  // operand view (pointer, row and K strides, rows, cols, conj, side) its
+  // slices, scales and padded sizes
+  struct OzSplitDone {
+    int8_t* slices;
+    int* exps;
+    int rpad, kpad;
+  };
+  std::map<std::vector<long long>, OzSplitDone> oz_prev_;
+  std::vector<std::pair<const char*, const char*>> oz_prev_out_;  // byte ranges the previous step wrote
+  size_t oz_prev_end_ = 0;        // pool bytes its digits occupy
+  size_t oz_prev_steps_ = 0;      // steps.size() right after it
+  unsigned char* oz_prev_pool_ = nullptr;
 };
 
 // ---------------------------------------------------------------------------
