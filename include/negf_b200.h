@@ -299,6 +299,11 @@ typedef struct {
    * energy from negf_solver_set_self_energies (replacing the device's
    * constant ones) and form Gamma(E) on the device. */
   int32_t sigma_per_energy;
+  /* NEGF_PREC_MIXED only: the Gauss-Jordan rank-nb updates of the diagonal
+   * inversions as INT8 digit products with 34 digit pairs (2; as accurate as
+   * FP64 products) or as FP64 DMMA products (1); 0: the library default (1).
+   * The inversion panels always run in FP64. */
+  int32_t gj_update;
 } negf_solve_opts;
 
 /* Precision modes.  FP64: every product in FP64 on the DMMA tensor path.
@@ -306,7 +311,8 @@ typedef struct {
  * (tcgen05) with FP64-accurate digit splitting (per row a 54-bit fixed-point
  * value as 7 base-256 digits, the 28 digit pairs of weight >= 2^-60 formed
  * with exact int32 accumulation: ~1e-15 relative to |op(A)| |op(B)| per
- * product); the diagonal-block inversions stay in FP64. */
+ * product); the inversion panels stay in FP64 and their rank-nb updates
+ * follow negf_solve_opts.gj_update. */
 #define NEGF_PREC_FP64 0
 #define NEGF_PREC_MIXED 1
 
@@ -329,8 +335,9 @@ int negf_solve(negf_device_t dev, int32_t nE, const double* energies, const negf
  *             9-206) with lu(NoPivot()) diagonal factorisations (one block
  *             size).
  * opts: eta, precision (NEGF_PREC_MIXED: block products on the INT8 tensor
- * cores with FP64-grade digit splitting, inversions / LU in FP64), max_chunk /
- * hbm_budget_gb (energies per chunk), gemm_form, gj_nb; sigma_per_energy must
+ * cores with FP64-grade digit splitting, inversion panels and LU in FP64),
+ * max_chunk / hbm_budget_gb (energies per chunk), gemm_form, gj_nb,
+ * gj_update; sigma_per_energy must
  * be 0.  Outputs (NULL: skipped), energy-major: gd_out nE * sum b_i^2; gu_out
  * (blocks (i,i+1), b_i x b_{i+1}) and gl_out (blocks (i+1,i), b_{i+1} x b_i)
  * nE * sum b_i b_{i+1}; column-major blocks.  HOST pointers unless
@@ -398,7 +405,9 @@ int negf_solver_run_profiled(negf_solver_t s, void* stream);
  * arrays hold NEGF_PROFILE_KINDS entries. Synchronises and writes, per
  * kind, the summed milliseconds, real flops (for kind 8, the digit split,
  * its algorithmic bytes instead: operands read once, 21 digit bytes per
- * complex element and a scale per row written) and launch counts of the
+ * complex element and a scale per row written; for kind 9 the INT8
+ * operations: 3 real products x digit pairs x 2mnk per complex product) and
+ * launch counts of the
  * profiled passes since the last reset (reset != 0 starts a new
  * accumulation). */
 #define NEGF_PROFILE_KINDS 10

@@ -257,7 +257,7 @@ struct OzKey {
 inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
 }  // namespace
 
-void Plan::gemm_mixed(char opA, char opB, const std::vector<ZGemmProblem>& probs) {
+void Plan::gemm_mixed(char opA, char opB, const std::vector<ZGemmProblem>& probs, int pairs) {
   if (probs.empty()) return;
   if (!err_) err_ = static_cast<int*>(alloc(sizeof(int)));
   std::map<OzKey, int> index;
@@ -409,7 +409,7 @@ void Plan::gemm_mixed(char opA, char opB, const std::vector<ZGemmProblem>& probs
   s2.count = (int)mp.size();
   s2.total_tiles = total;
   s2.flops = fl;
-  s2.form = oz_pairs_;
+  s2.form = pairs == 28 || pairs == 34 ? pairs : oz_pairs_;
   steps.push_back(s2);
   // what the next mixed step may use again
   oz_prev_.clear();
@@ -431,8 +431,12 @@ void Plan::gemm_fp64(char opA, char opB, const std::vector<ZGemmProblem>& probs)
   int total = 0;
   double fl = 0.0;
   bool pre = true;
+  int max_k = 0;
+  for (const auto& p : probs)
+    if (zgemm_tiles(p.m, p.n) > 0) max_k = std::max(max_k, p.k);
+  const bool small = zgemm_smallk_ok(gemm_form_, max_k);
   for (const auto& p : probs) {
-    int t = zgemm_tiles(p.m, p.n);
+    int t = small ? zgemm_tiles_smallk(p.m, p.n) : zgemm_tiles(p.m, p.n);
     if (t == 0) continue;
     v.push_back(p);
     starts.push_back(total);
@@ -446,7 +450,7 @@ void Plan::gemm_fp64(char opA, char opB, const std::vector<ZGemmProblem>& probs)
   s.opA = opA;
   s.opB = opB;
   s.preload = pre;
-  s.form = gemm_form_;
+  s.form = small ? 3 : gemm_form_;
   s.off = push_bytes(v.data(), v.size() * sizeof(ZGemmProblem));
   s.tiles_off = push_bytes(starts.data(), starts.size() * sizeof(int));
   s.count = static_cast<int>(v.size());
@@ -495,7 +499,12 @@ void Plan::inv(const std::vector<InvSpec>& specs) {
       int w = std::min(nb, p.n - k0);
       g.push_back(gp(p.F, p.n, p.Bbuf, w, p.W, p.ld, p.n, p.n, w, ONE, p.W, p.ld, ONE));
     }
-    gemm_fp64('N', 'N', g);  // the diagonal-block inversion stays in FP64
+    // W += F Bbuf: INT8 digit products at FP64 accuracy in a mixed plan (the
+    // panels stay in FP64), else DMMA
+    if (gj_update_int8())
+      gemm_mixed('N', 'N', g, 34);
+    else
+      gemm_fp64('N', 'N', g);
   }
   // the GEMM updates carry their own flop count; the panel work is the rest
   Step u;

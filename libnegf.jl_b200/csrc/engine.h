@@ -27,6 +27,11 @@ cudaError_t launch_zgemm_batched_ex(char opA, char opB, bool preload, const ZGem
                                     int form = 0);
 bool zgemm_preload_ok(const ZGemmProblem& p);
 int zgemm_tiles(int m, int n);
+// small-K 3M kernel (32 x 64 tiles, two CTAs per SM) for steps with every
+// k <= 32 in the 3M form; a step using it carries form 3 and counts its tiles
+// with zgemm_tiles_smallk
+bool zgemm_smallk_ok(int form, int max_k);
+int zgemm_tiles_smallk(int m, int n);
 size_t zgemm_smem_bytes();
 cudaError_t zgemm_prepare(char opA, char opB);
 size_t zgj_panel_smem_bytes(int n, int nb);
@@ -137,7 +142,7 @@ struct Step {
   int count = 0, total_tiles = 0, max_m = 0, max_n = 0;
   int k0 = 0, nb = 0, blocked = 0;
   bool preload = false;  // GEMM: accumulators start from Cin (all problems alpha, beta = +-1)
-  int form = 0;          // GEMM: 0 default, 1 four real products, 2 3M; OZ_MMA: digit pairs (34 or 28)
+  int form = 0;          // GEMM: 0 default, 1 four real products, 2 3M, 3 small-K 3M; OZ_MMA: digit pairs (34 or 28)
   size_t smem = 0;
   double flops = 0.0;    // real flops of the step (8mnk per complex GEMM)
   double bytes = 0.0;    // OZ_SPLIT: algorithmic bytes (operands read once, digit slices and scales written)
@@ -156,11 +161,12 @@ class Plan {
   cplx* alloc_c(size_t n) { return static_cast<cplx*>(alloc(n * sizeof(cplx))); }
 
   // Complex GEMM step; with set_mixed(true) the products (k > 0) run on the
-  // INT8 tensor cores with FP64-accurate Ozaki splitting.  Products issued by
-  // inv() (the Gauss-Jordan updates) always stay in FP64.
+  // INT8 tensor cores with FP64-accurate Ozaki splitting.  The Gauss-Jordan
+  // rank-nb updates issued by inv() follow set_gj_update.
   void gemm(char opA, char opB, const std::vector<ZGemmProblem>& probs);
   void gemm_fp64(char opA, char opB, const std::vector<ZGemmProblem>& probs);
-  void gemm_mixed(char opA, char opB, const std::vector<ZGemmProblem>& probs);
+  // pairs: 28 or 34 digit pairs for this step (0: the plan's count)
+  void gemm_mixed(char opA, char opB, const std::vector<ZGemmProblem>& probs, int pairs = 0);
   // pairs: digit pairs of the INT8 products, 34 (as accurate as FP64
   // products) or 28 (within ~3x of the FP64 rounding bound, ~18 % fewer MMAs)
   void set_mixed(bool on, int pairs = 34) { mixed_ = on; oz_pairs_ = pairs == 28 ? 28 : 34; }
@@ -168,6 +174,13 @@ class Plan {
   // schedule knobs: FP64 GEMM form (0 default, 1 four products, 2 3M) and the
   // Gauss-Jordan panel width for blocks > 112 (0 default)
   void set_schedule(int gemm_form, int gj_nb) { gemm_form_ = gemm_form; gj_nb_ = gj_nb; }
+  // Gauss-Jordan rank-nb updates of a mixed plan: 1 FP64 DMMA products, 2
+  // INT8 digit products with 34 pairs (as accurate as FP64 products), 0 the
+  // default (1: at 256 x 32 layers both take the same time per pass, and the
+  // FP64 form needs no digit split).  Plans without set_mixed(true) keep them
+  // in FP64.
+  void set_gj_update(int mode) { gj_update_ = mode; }
+  bool gj_update_int8() const { return mixed_ && gj_update_ == 2; }
   int panel_width(int max_n) const;
   bool mixed() const { return mixed_; }
   int* error_flag() const { return err_; }
@@ -220,7 +233,7 @@ class Plan {
   cudaStream_t graph_stream_ = nullptr;
   bool mixed_ = false;
   int oz_pairs_ = 34;
-  int gemm_form_ = 0, gj_nb_ = 0;
+  int gemm_form_ = 0, gj_nb_ = 0, gj_update_ = 0;
   int* err_ = nullptr;            // tensor-core wait time-out flag (device int)
   unsigned char* oz_pool_ = nullptr;  // digit-slice scratch shared by all mixed steps
   size_t oz_pool_bytes_ = 0;

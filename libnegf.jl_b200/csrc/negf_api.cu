@@ -259,7 +259,9 @@ int build_solver(negf_solver_s& S) {
     for (int x : dv->b)
       if (S.opts.gj_nb > 0 && x > 112 && zgj_panel_smem_bytes(x, S.opts.gj_nb) > max_panel_smem())
         return fail(NEGF_ERR_INVALID, "gj_nb too wide for the block size (shared memory)");
+  if (S.opts.gj_update < 0 || S.opts.gj_update > 2) return fail(NEGF_ERR_INVALID, "gj_update must be 0, 1 or 2");
   plan.set_schedule(S.opts.gemm_form, S.opts.gj_nb);
+  plan.set_gj_update(S.opts.gj_update);
 
   const bool sig_e = S.opts.sigma_per_energy != 0;
   std::vector<TriSystem> sys(nE);
@@ -1019,7 +1021,11 @@ int negf_solver_profile_read(negf_solver_t s, double* ms, double* flops, int64_t
       NEGF_TRY_CUDA(cudaEventElapsedTime(&x, ev[i], ev[i + 1]), "profile read");
       int k = static_cast<int>(steps[i].kind);
       t[k] += x;
-      f[k] += steps[i].kind == Step::OZ_SPLIT ? steps[i].bytes : steps[i].flops;
+      // kind 8: algorithmic bytes; kind 9: INT8 operations, 3 real products
+      // x digit pairs x 2mnk per complex product (8mnk flops)
+      f[k] += steps[i].kind == Step::OZ_SPLIT  ? steps[i].bytes
+              : steps[i].kind == Step::OZ_MMA ? steps[i].flops * (6.0 * steps[i].form / 8.0)
+                                              : steps[i].flops;
       n[k] += 1;
     }
   }
@@ -1257,7 +1263,8 @@ int negf_device_selected_inverse(negf_device_t dev, int32_t nE, const double* en
   if (int r = check_device()) return r;
   if (!dev || nE <= 0 || !energies || !opts || method < 0 || method > 2 || nlevels < 0 ||
       nlevels > NEGF_DDRGF_MAX_LEVELS || (nlevels > 0 && !block_size_d1) ||
-      (opts->precision != NEGF_PREC_FP64 && opts->precision != NEGF_PREC_MIXED))
+      (opts->precision != NEGF_PREC_FP64 && opts->precision != NEGF_PREC_MIXED) || opts->gj_update < 0 ||
+      opts->gj_update > 2)
     return fail(NEGF_ERR_INVALID, "negf_device_selected_inverse: bad arguments");
   if (opts->sigma_per_energy)
     return fail(NEGF_ERR_INVALID, "negf_device_selected_inverse: the device's constant self-energies are used");
@@ -1313,6 +1320,7 @@ int negf_device_selected_inverse(negf_device_t dev, int32_t nE, const double* en
       // errors more than RGF does: FP64-grade products (34 digit pairs) there
       plan.set_mixed(mixed, method == 0 ? 28 : 34);
       plan.set_schedule(opts->gemm_form, opts->gj_nb);
+      plan.set_gj_update(opts->gj_update);
       int* dinfo = static_cast<int*>(plan.alloc(sizeof(int) * (size_t)cnt * n));
       // output blocks of this chunk: the caller's device buffers, or plan memory
       // downloaded afterwards (every sweep writes all three kinds)

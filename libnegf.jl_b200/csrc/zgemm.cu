@@ -359,6 +359,170 @@ __global__ void __launch_bounds__(gemm3m::THREADS, 1)
       }
 }
 
+// ---------------------------------------------------------------------------
+// Small-K 3M variant for products with k <= 32 (the Gauss-Jordan rank-nb
+// updates W += F Bbuf and other thin products).  Such a tile has one or two
+// K slabs, so the 64 x 64 kernel (one CTA per SM at 246 registers) spends
+// most of its time waiting for its operand and Cin loads with nothing to
+// overlap them.  Here a CTA computes a 32 x 64 tile with 8 warps of 16 x 16
+// (24 accumulator doubles per thread), small enough for two CTAs per SM, so
+// one CTA's loads overlap the other's DMMA products.  Same staging scheme
+// (3-stage cp.async ring, 16 K per slab), same arithmetic as the 3M kernel.
+namespace gemm_sk {
+constexpr int BM = 32, BN = 64, BK = 16;
+constexpr int THREADS = 256;
+constexpr int STAGES = 3;
+constexpr int AS_LD = BM + 1;  // As[k][m]
+constexpr int BS_LD = BK + 1;  // Bs[n][k]
+constexpr int AS_SIZE = BK * AS_LD;
+constexpr int BS_SIZE = BN * BS_LD;
+constexpr int STAGE_SIZE = AS_SIZE + BS_SIZE;
+constexpr size_t SMEM_BYTES = size_t(STAGES) * STAGE_SIZE * sizeof(cplx);
+}  // namespace gemm_sk
+
+template <bool TA, bool TB>
+__device__ __forceinline__ void load_stage_sk(cplx* As, cplx* Bs, const ZGemmProblem& p, int m0, int n0, int k0,
+                                              int tid) {
+  using namespace gemm_sk;
+#pragma unroll
+  for (int i = 0; i < (BM * BK) / THREADS; ++i) {
+    const int idx = tid + i * THREADS;
+    int r, kk;
+    if (!TA) { r = idx % BM; kk = idx / BM; }
+    else     { kk = idx % BK; r = idx / BK; }
+    const int gr = m0 + r, gk = k0 + kk;
+    const bool ok = gr < p.m && gk < p.k;
+    const cplx* src = p.A;
+    if (ok) src = TA ? (p.A + gk + (size_t)gr * p.lda) : (p.A + gr + (size_t)gk * p.lda);
+    cp_async16(&As[kk * AS_LD + r], src, ok);
+  }
+#pragma unroll
+  for (int i = 0; i < (BN * BK) / THREADS; ++i) {
+    const int idx = tid + i * THREADS;
+    int c, kk;
+    if (!TB) { kk = idx % BK; c = idx / BK; }
+    else     { c = idx % BN; kk = idx / BN; }
+    const int gc = n0 + c, gk = k0 + kk;
+    const bool ok = gc < p.n && gk < p.k;
+    const cplx* src = p.B;
+    if (ok) src = TB ? (p.B + gc + (size_t)gk * p.ldb) : (p.B + gk + (size_t)gc * p.ldb);
+    cp_async16(&Bs[c * BS_LD + kk], src, ok);
+  }
+}
+
+template <bool TA, bool CA, bool TB, bool CB, bool PRE>
+__global__ void __launch_bounds__(gemm_sk::THREADS, 2)
+    zgemm3m_smallk_kernel(const ZGemmProblem* __restrict__ probs, const int* __restrict__ tile_start, int nprob) {
+  using namespace gemm_sk;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx* smem = reinterpret_cast<cplx*>(smem_raw);
+  const int bid = blockIdx.x;
+  int lo = 0, hi = nprob - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tile_start[mid] <= bid) lo = mid; else hi = mid - 1;
+  }
+  const ZGemmProblem p = probs[lo];
+  const int t = bid - tile_start[lo];
+  const int tiles_m = (p.m + BM - 1) / BM;
+  const int m0 = (t % tiles_m) * BM;
+  const int n0 = (t / tiles_m) * BN;
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, tq = lane & 3;
+  const int wm = (warp & 1) * 16, wn = (warp >> 1) * 16;
+
+  const bool preload = PRE && p.k > 0 && p.Cin != nullptr;
+  const double pre_sign = p.alpha.x * p.beta.x;
+  double P1[2][4], P2[2][4], P3[2][4];
+#pragma unroll
+  for (int b = 0; b < 2; ++b)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      P1[b][c] = 0.0; P2[b][c] = 0.0; P3[b][c] = 0.0;
+      if (preload) {
+        const int r = m0 + wm + g + ((c >> 1) << 3);
+        const int cc = n0 + wn + b * 8 + 2 * tq + (c & 1);
+        if (r < p.m && cc < p.n) {
+          const cplx v = p.Cin[r + (size_t)cc * p.ldcin];
+          P1[b][c] = pre_sign * v.x;
+          P3[b][c] = pre_sign * v.x + pre_sign * v.y;
+        }
+      }
+    }
+
+  const int nk = (p.k + BK - 1) / BK;
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < nk) load_stage_sk<TA, TB>(smem + s * STAGE_SIZE, smem + s * STAGE_SIZE + AS_SIZE, p, m0, n0, s * BK, tid);
+    cp_async_commit();
+  }
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    const int kn = kt + STAGES - 1;
+    if (kn < nk) {
+      const int s = kn % STAGES;
+      load_stage_sk<TA, TB>(smem + s * STAGE_SIZE, smem + s * STAGE_SIZE + AS_SIZE, p, m0, n0, kn * BK, tid);
+    }
+    cp_async_commit();
+    const cplx* As = smem + (kt % STAGES) * STAGE_SIZE;
+    const cplx* Bs = As + AS_SIZE;
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 4) {
+      double ar[2], ai[2], as[2], br[2], bi[2], bs[2];
+      const cplx x0 = As[(kk + tq) * AS_LD + wm + g];
+      const cplx x1 = As[(kk + tq) * AS_LD + wm + g + 8];
+      ar[0] = x0.x; ai[0] = CA ? -x0.y : x0.y; as[0] = ar[0] + ai[0];
+      ar[1] = x1.x; ai[1] = CA ? -x1.y : x1.y; as[1] = ar[1] + ai[1];
+#pragma unroll
+      for (int ni = 0; ni < 2; ++ni) {
+        const cplx y = Bs[(wn + ni * 8 + g) * BS_LD + kk + tq];
+        br[ni] = y.x;
+        bi[ni] = CB ? -y.y : y.y;
+        bs[ni] = br[ni] + bi[ni];
+      }
+#pragma unroll
+      for (int ni = 0; ni < 2; ++ni) {
+        double* p1 = P1[ni];
+        double* p2 = P2[ni];
+        double* p3 = P3[ni];
+        dmma16x8x4(p1[0], p1[1], p1[2], p1[3], ar[0], ar[1], br[ni]);
+        dmma16x8x4(p2[0], p2[1], p2[2], p2[3], ai[0], ai[1], bi[ni]);
+        dmma16x8x4(p3[0], p3[1], p3[2], p3[3], as[0], as[1], bs[ni]);
+      }
+    }
+  }
+  cp_async_wait<0>();
+
+  const bool has_ab = p.k > 0;
+  const bool has_cin = (p.beta.x != 0.0 || p.beta.y != 0.0) && p.Cin != nullptr && !preload;
+  const cplx dg = p.diag_ptr ? *p.diag_ptr : p.diag;
+#pragma unroll
+  for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int r = m0 + wm + g + ((e >> 1) << 3);
+      const int c = n0 + wn + ni * 8 + 2 * tq + (e & 1);
+      if (r < p.m && c < p.n) {
+        cplx v = make_double2(0.0, 0.0);
+        if (has_ab) {
+          const double xr = P1[ni][e] - P2[ni][e];
+          const double xi = P3[ni][e] - P1[ni][e] - P2[ni][e];
+          v.x = p.alpha.x * xr - p.alpha.y * xi;
+          v.y = p.alpha.x * xi + p.alpha.y * xr;
+        }
+        if (has_cin) {
+          const cplx ci = p.Cin[r + (size_t)c * p.ldcin];
+          v.x += p.beta.x * ci.x - p.beta.y * ci.y;
+          v.y += p.beta.x * ci.y + p.beta.y * ci.x;
+        }
+        if (r == c) { v.x += dg.x; v.y += dg.y; }
+        p.C[r + (size_t)c * p.ldc] = v;
+      }
+    }
+}
+
 using ZGemmKernel = void (*)(const ZGemmProblem*, const int*, int);
 
 template <bool PRE, bool G3M>
@@ -388,6 +552,27 @@ static bool use_3m() {
   return v;
 }
 
+template <bool PRE>
+static ZGemmKernel pick_smallk_t(int ia, int ib) {
+  switch (ia * 3 + ib) {
+    case 0: return zgemm3m_smallk_kernel<false, false, false, false, PRE>;
+    case 1: return zgemm3m_smallk_kernel<false, false, true, false, PRE>;
+    case 2: return zgemm3m_smallk_kernel<false, false, true, true, PRE>;
+    case 3: return zgemm3m_smallk_kernel<true, false, false, false, PRE>;
+    case 4: return zgemm3m_smallk_kernel<true, false, true, false, PRE>;
+    case 5: return zgemm3m_smallk_kernel<true, false, true, true, PRE>;
+    case 6: return zgemm3m_smallk_kernel<true, true, false, false, PRE>;
+    case 7: return zgemm3m_smallk_kernel<true, true, true, false, PRE>;
+    default: return zgemm3m_smallk_kernel<true, true, true, true, PRE>;
+  }
+}
+
+static ZGemmKernel pick_smallk(char opA, char opB, bool pre) {
+  const int ia = opA == 'N' ? 0 : (opA == 'T' ? 1 : 2);
+  const int ib = opB == 'N' ? 0 : (opB == 'T' ? 1 : 2);
+  return pre ? pick_smallk_t<true>(ia, ib) : pick_smallk_t<false>(ia, ib);
+}
+
 static ZGemmKernel pick_kernel(char opA, char opB, bool pre, bool g3m) {
   int ia = opA == 'N' ? 0 : (opA == 'T' ? 1 : 2);
   int ib = opB == 'N' ? 0 : (opB == 'T' ? 1 : 2);
@@ -406,7 +591,28 @@ cudaError_t zgemm_prepare(char opA, char opB) {
                                          (int)gemm::SMEM_BYTES);
     if (e != cudaSuccess) return e;
   }
+  for (int v = 0; v < 2; ++v) {
+    cudaError_t e = cudaFuncSetAttribute(pick_smallk(opA, opB, v & 1), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)gemm_sk::SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+  }
   return cudaSuccess;
+}
+
+// The small-K kernel serves steps whose problems all have k <= 32 when the
+// 3M form is in use (form 2, or the default without NEGF_ZGEMM=4m);
+// NEGF_ZGEMM_SMALLK=0 keeps them on the 64 x 64 kernel.
+bool zgemm_smallk_ok(int form, int max_k) {
+  static const bool on = [] {
+    const char* e = std::getenv("NEGF_ZGEMM_SMALLK");
+    return !(e && e[0] == '0');
+  }();
+  return on && max_k <= 32 && (form == 2 || (form == 0 && use_3m()));
+}
+
+int zgemm_tiles_smallk(int m, int n) {
+  if (m <= 0 || n <= 0) return 0;
+  return ((m + gemm_sk::BM - 1) / gemm_sk::BM) * ((n + gemm_sk::BN - 1) / gemm_sk::BN);
 }
 
 // True when the problem qualifies for the accumulator preload variant.
@@ -423,6 +629,11 @@ cudaError_t launch_zgemm_batched_ex(char opA, char opB, bool preload, const ZGem
                                     const int* tile_start_dev, int nprob, int total_tiles, cudaStream_t stream,
                                     int form) {
   if (nprob <= 0 || total_tiles <= 0) return cudaSuccess;
+  if (form == 3) {  // small-K 3M kernel; tiles counted by zgemm_tiles_smallk
+    pick_smallk(opA, opB, preload)<<<total_tiles, gemm_sk::THREADS, gemm_sk::SMEM_BYTES, stream>>>(
+        probs_dev, tile_start_dev, nprob);
+    return cudaGetLastError();
+  }
   const bool g3m = form == 0 ? use_3m() : form == 2;
   pick_kernel(opA, opB, preload, g3m)<<<total_tiles, g3m ? gemm3m::THREADS : gemm::THREADS, gemm::SMEM_BYTES,
                                         stream>>>(probs_dev, tile_start_dev, nprob);

@@ -36,7 +36,7 @@ class SolveOpts(ctypes.Structure):
                 ("kT", ctypes.c_double), ("want_gr", ctypes.c_int32), ("want_gl", ctypes.c_int32),
                 ("want_t", ctypes.c_int32), ("max_chunk", ctypes.c_int32), ("hbm_budget_gb", ctypes.c_double),
                 ("precision", ctypes.c_int32), ("gemm_form", ctypes.c_int32), ("gj_nb", ctypes.c_int32),
-                ("sigma_per_energy", ctypes.c_int32)]
+                ("sigma_per_energy", ctypes.c_int32), ("gj_update", ctypes.c_int32)]
 
 
 NEGF_PREC_FP64 = 0

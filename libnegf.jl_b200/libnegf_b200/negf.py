@@ -26,10 +26,12 @@ def _host_blocks(blocks):
 
 
 def make_opts(eta=1e-6, mu_l=0.1, mu_r=-0.1, kT=0.025, want_gr=True, want_gl=True, want_t=True, max_chunk=0,
-              hbm_budget_gb=0.0, precision="fp64", gemm_form=0, gj_nb=0, sigma_per_energy=False):
+              hbm_budget_gb=0.0, precision="fp64", gemm_form=0, gj_nb=0, sigma_per_energy=False, gj_update=0):
     """precision: "fp64" (every product in FP64) or "mixed" (Schur products on
     the INT8 tensor cores with FP64-accurate digit splitting).  gemm_form /
-    gj_nb: schedule knobs (0 = library default; see libnegf_b200.autotune)."""
+    gj_nb: schedule knobs (0 = library default; see libnegf_b200.autotune).
+    gj_update (mixed only): the Gauss-Jordan rank-nb updates as INT8 digit
+    products with 34 pairs (2) or FP64 products (1); 0 = library default."""
     o = _lib.SolveOpts()
     o.eta, o.mu_l, o.mu_r, o.kT = eta, mu_l, mu_r, kT
     o.want_gr, o.want_gl, o.want_t = int(want_gr), int(want_gl), int(want_t)
@@ -39,6 +41,7 @@ def make_opts(eta=1e-6, mu_l=0.1, mu_r=-0.1, kT=0.025, want_gr=True, want_gl=Tru
     o.gemm_form = int(gemm_form)
     o.gj_nb = int(gj_nb)
     o.sigma_per_energy = int(bool(sigma_per_energy))
+    o.gj_update = int(gj_update)
     return o
 
 
@@ -87,7 +90,7 @@ class Device:
             pass
 
     def solve(self, energies, eta=1e-6, mu_l=0.1, mu_r=-0.1, kT=0.025, want_gr=True, want_gl=True, want_t=True,
-              max_chunk=0, precision="fp64"):
+              max_chunk=0, precision="fp64", gj_update=0):
         """G^R / G^< diagonal blocks and T(E) for every energy (host arrays).
 
         Returns (gr, gl, t): gr/gl are lists (per energy) of lists (per layer)
@@ -98,7 +101,8 @@ class Device:
         gr = np.empty(nE * per, dtype=np.complex128) if want_gr else None
         gl = np.empty(nE * per, dtype=np.complex128) if want_gl else None
         t = np.empty(nE, dtype=np.float64) if want_t else None
-        o = make_opts(eta, mu_l, mu_r, kT, want_gr, want_gl, want_t, max_chunk, precision=precision)
+        o = make_opts(eta, mu_l, mu_r, kT, want_gr, want_gl, want_t, max_chunk, precision=precision,
+                      gj_update=gj_update)
         check(load().negf_solve(self._handle, nE, E.ctypes.data_as(_lib.c_double_p), ctypes.byref(o),
                                 gr.ctypes.data if gr is not None else None,
                                 gl.ctypes.data if gl is not None else None,
