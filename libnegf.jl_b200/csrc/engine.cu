@@ -451,6 +451,10 @@ void Plan::gemm_fp64(char opA, char opB, const std::vector<ZGemmProblem>& probs)
   s.opB = opB;
   s.preload = pre;
   s.form = small ? 3 : gemm_form_;
+  s.uniform_tiles = total / (int)v.size();
+  if ((long long)s.uniform_tiles * (long long)v.size() != total) s.uniform_tiles = 0;
+  for (size_t i = 1; i < starts.size() && s.uniform_tiles; ++i)
+    if (starts[i] - starts[i - 1] != s.uniform_tiles) s.uniform_tiles = 0;
   s.off = push_bytes(v.data(), v.size() * sizeof(ZGemmProblem));
   s.tiles_off = push_bytes(starts.data(), starts.size() * sizeof(int));
   s.count = static_cast<int>(v.size());
@@ -750,7 +754,8 @@ cudaError_t Plan::launch_step(const Step& s, const unsigned char* base, cudaStre
     switch (s.kind) {
       case Step::GEMM:
         e = launch_zgemm_batched_ex(s.opA, s.opB, s.preload, reinterpret_cast<const ZGemmProblem*>(base + s.off),
-                                    reinterpret_cast<const int*>(base + s.tiles_off), s.count, s.total_tiles, stream, s.form);
+                                    reinterpret_cast<const int*>(base + s.tiles_off), s.count, s.total_tiles, stream, s.form,
+                                    s.uniform_tiles);
         break;
       case Step::GJ_PANEL:
         e = launch_zgj_panel(reinterpret_cast<const ZInvProblem*>(base + s.off), s.count, s.k0, s.nb, s.blocked,

@@ -24,7 +24,7 @@ cudaError_t launch_zgemm_batched(char opA, char opB, const ZGemmProblem* probs_d
                                  int nprob, int total_tiles, cudaStream_t stream);
 cudaError_t launch_zgemm_batched_ex(char opA, char opB, bool preload, const ZGemmProblem* probs_dev,
                                     const int* tile_start_dev, int nprob, int total_tiles, cudaStream_t stream,
-                                    int form = 0);
+                                    int form = 0, int uniform_tiles = 0);
 bool zgemm_preload_ok(const ZGemmProblem& p);
 int zgemm_tiles(int m, int n);
 // small-K 3M kernel (32 x 64 tiles, two CTAs per SM) for steps with every
@@ -143,6 +143,7 @@ struct Step {
   int k0 = 0, nb = 0, blocked = 0;
   bool preload = false;  // GEMM: accumulators start from Cin (all problems alpha, beta = +-1)
   int form = 0;          // GEMM: 0 default, 1 four real products, 2 3M, 3 small-K 3M; OZ_MMA: digit pairs (34 or 28)
+  int uniform_tiles = 0; // GEMM: tiles of every problem when all have the same count, else 0
   size_t smem = 0;
   double flops = 0.0;    // real flops of the step (8mnk per complex GEMM)
   double bytes = 0.0;    // OZ_SPLIT: algorithmic bytes (operands read once, digit slices and scales written)

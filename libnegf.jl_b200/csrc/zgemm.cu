@@ -52,6 +52,27 @@ __device__ __forceinline__ void dmma16x8x4(double& c0, double& c1, double& c2, d
       : "d"(a0), "d"(a1), "d"(b0));
 }
 
+// CTA -> (problem, tile).  nprob > 0: binary search over the exclusive
+// prefix sum tile_start; nprob < 0: every problem has -nprob tiles (the
+// host's uniform batches), so the problem is a division away and the CTA
+// skips the chain of dependent loads of the search.
+__device__ __forceinline__ void zgemm_locate(int bid, const int* __restrict__ tile_start, int nprob, int& prob,
+                                             int& tile) {
+  if (nprob < 0) {
+    const int T = -nprob;
+    prob = bid / T;
+    tile = bid - prob * T;
+    return;
+  }
+  int lo = 0, hi = nprob - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tile_start[mid] <= bid) lo = mid; else hi = mid - 1;
+  }
+  prob = lo;
+  tile = bid - tile_start[lo];
+}
+
 // Stage one K-slab of A (BM x BK of op(A)) and B (BK x BN of op(B)).
 template <bool TA, bool TB>
 __device__ __forceinline__ void load_stage(cplx* As, cplx* Bs, const ZGemmProblem& p, int m0, int n0, int k0,
@@ -92,15 +113,9 @@ __global__ void __launch_bounds__(gemm::THREADS, 2)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx* smem = reinterpret_cast<cplx*>(smem_raw);
 
-  // map CTA -> (problem, tile) by binary search over the tile prefix sum
-  int bid = blockIdx.x;
-  int lo = 0, hi = nprob - 1;
-  while (lo < hi) {
-    int mid = (lo + hi + 1) >> 1;
-    if (tile_start[mid] <= bid) lo = mid; else hi = mid - 1;
-  }
+  int lo, t;
+  zgemm_locate(blockIdx.x, tile_start, nprob, lo, t);
   const ZGemmProblem p = probs[lo];
-  int t = bid - tile_start[lo];
   int tiles_m = (p.m + BM - 1) / BM;
   int m0 = (t % tiles_m) * BM;
   int n0 = (t / tiles_m) * BN;
@@ -240,14 +255,9 @@ __global__ void __launch_bounds__(gemm3m::THREADS, 1)
   using namespace gemm;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx* smem = reinterpret_cast<cplx*>(smem_raw);
-  int bid = blockIdx.x;
-  int lo = 0, hi = nprob - 1;
-  while (lo < hi) {
-    int mid = (lo + hi + 1) >> 1;
-    if (tile_start[mid] <= bid) lo = mid; else hi = mid - 1;
-  }
+  int lo, t;
+  zgemm_locate(blockIdx.x, tile_start, nprob, lo, t);
   const ZGemmProblem p = probs[lo];
-  const int t = bid - tile_start[lo];
   const int tiles_m = (p.m + BM - 1) / BM;
   const int m0 = (t % tiles_m) * BM;
   const int n0 = (t / tiles_m) * BN;
@@ -416,14 +426,9 @@ __global__ void __launch_bounds__(gemm_sk::THREADS, 2)
   using namespace gemm_sk;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx* smem = reinterpret_cast<cplx*>(smem_raw);
-  const int bid = blockIdx.x;
-  int lo = 0, hi = nprob - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (tile_start[mid] <= bid) lo = mid; else hi = mid - 1;
-  }
+  int lo, t;
+  zgemm_locate(blockIdx.x, tile_start, nprob, lo, t);
   const ZGemmProblem p = probs[lo];
-  const int t = bid - tile_start[lo];
   const int tiles_m = (p.m + BM - 1) / BM;
   const int m0 = (t % tiles_m) * BM;
   const int n0 = (t / tiles_m) * BN;
@@ -627,8 +632,15 @@ bool zgemm_preload_ok(const ZGemmProblem& p) {
 // problem of the launch.
 cudaError_t launch_zgemm_batched_ex(char opA, char opB, bool preload, const ZGemmProblem* probs_dev,
                                     const int* tile_start_dev, int nprob, int total_tiles, cudaStream_t stream,
-                                    int form) {
+                                    int form, int uniform_tiles) {
   if (nprob <= 0 || total_tiles <= 0) return cudaSuccess;
+  static const bool uniform_on = [] {
+    const char* e = std::getenv("NEGF_ZGEMM_UNIFORM");
+    return !(e && e[0] == '0');
+  }();
+  // every problem has uniform_tiles tiles: the kernels locate their problem by
+  // division (signalled by a negative count)
+  if (uniform_on && uniform_tiles > 0 && (long long)uniform_tiles * nprob == total_tiles) nprob = -uniform_tiles;
   if (form == 3) {  // small-K 3M kernel; tiles counted by zgemm_tiles_smallk
     pick_smallk(opA, opB, preload)<<<total_tiles, gemm_sk::THREADS, gemm_sk::SMEM_BYTES, stream>>>(
         probs_dev, tile_start_dev, nprob);
