@@ -5,7 +5,9 @@ the reference's library).  The program runs the host-only entry points (the
 DDRGF partition helpers and the reference's partition search) and its output
 is checked against the oracle; calls that need a GPU are only linked."""
 
+import ctypes
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -92,3 +94,65 @@ def test_host_entry_points_from_c(c_program):
             n_o += 1
     assert n_t == 39 * 6 and n_o == 4
     assert "version 100" in r.stdout
+
+
+LAYOUT_PROG = r"""
+#include <stddef.h>
+#include <stdio.h>
+#include "negf_b200.h"
+#define F(T, f) printf("%s %s %zu %zu\n", #T, #f, offsetof(T, f), sizeof(((T*)0)->f))
+int main(void) {
+  printf("size negf_solve_opts %zu\n", sizeof(negf_solve_opts));
+  F(negf_solve_opts, eta); F(negf_solve_opts, mu_l); F(negf_solve_opts, mu_r); F(negf_solve_opts, kT);
+  F(negf_solve_opts, want_gr); F(negf_solve_opts, want_gl); F(negf_solve_opts, want_t);
+  F(negf_solve_opts, max_chunk); F(negf_solve_opts, hbm_budget_gb); F(negf_solve_opts, precision);
+  F(negf_solve_opts, gemm_form); F(negf_solve_opts, gj_nb); F(negf_solve_opts, sigma_per_energy);
+  F(negf_solve_opts, gj_update);
+  printf("size negf_zgemm_problem %zu\n", sizeof(negf_zgemm_problem));
+  F(negf_zgemm_problem, A); F(negf_zgemm_problem, B); F(negf_zgemm_problem, Cin); F(negf_zgemm_problem, C);
+  F(negf_zgemm_problem, m); F(negf_zgemm_problem, n); F(negf_zgemm_problem, k); F(negf_zgemm_problem, lda);
+  F(negf_zgemm_problem, ldb); F(negf_zgemm_problem, ldc); F(negf_zgemm_problem, ldcin);
+  F(negf_zgemm_problem, alpha); F(negf_zgemm_problem, beta); F(negf_zgemm_problem, diag);
+  printf("size CCscMatrix %zu\n", sizeof(CCscMatrix));
+  F(CCscMatrix, m); F(CCscMatrix, n); F(CCscMatrix, nnz); F(CCscMatrix, colptr); F(CCscMatrix, rowval);
+  F(CCscMatrix, nzval);
+  return 0;
+}
+"""
+
+
+def test_struct_layouts_match_the_bindings(tmp_path):
+    """Every struct of include/negf_b200.h that a binding mirrors has the same
+    fields, in the same order, at the same offsets and sizes in the Python
+    ctypes layer (libnegf_b200/_lib.py), and the Julia mirror of
+    negf_solve_opts in INTEGRATION.md names the same fields in the same order."""
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    sys.path.insert(0, os.path.join(ROOT, "libnegf.jl_b200"))
+    from libnegf_b200 import _lib
+    src = tmp_path / "layout.c"
+    src.write_text(LAYOUT_PROG)
+    exe = tmp_path / "layout"
+    r = subprocess.run([cc, "-std=c11", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-o",
+                        str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60).stdout.splitlines()
+    c_fields, c_size = {}, {}
+    for line in out:
+        f = line.split()
+        if f[0] == "size":
+            c_size[f[1]] = int(f[2])
+        else:
+            c_fields.setdefault(f[0], []).append((f[1], int(f[2]), int(f[3])))
+    mirrors = {"negf_solve_opts": _lib.SolveOpts, "negf_zgemm_problem": _lib.ZGemmProblem,
+               "CCscMatrix": _lib.CCscMatrix}
+    for cname, py in mirrors.items():
+        assert ctypes.sizeof(py) == c_size[cname], cname
+        py_fields = [(name, getattr(py, name).offset, getattr(py, name).size) for name, _ in py._fields_]
+        assert py_fields == c_fields[cname], cname
+    # the Julia struct in INTEGRATION.md
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    body = re.search(r"struct NegfOpts\n(.*?)\nend", text, re.S).group(1)
+    jl_names = re.findall(r"(\w+)::", body)
+    assert jl_names == [f[0] for f in c_fields["negf_solve_opts"]]
