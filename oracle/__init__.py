@@ -19,6 +19,11 @@ test oracles -- a dense inverse (``test_matinvertndiag_general_rgf.jl``,
 and through committed fixtures under ``tests/golden/`` made by
 ``tests/golden/make_golden.py``.  Parity with the reference itself is therefore
 "unpinned" in the strict sense.
+
+Two modules are not restatements of the reference: ``ddtruth`` (a
+double-double truth for the parity tests) and ``ozaki`` (a host model of the
+library's mixed-precision digit products, which the reference does not have,
+used to check their accuracy claims against that truth).
 """
 
 from .blockmatrix import BlockMatrix, bm_convert_dense, bm_from_dense, bm_copy  # noqa: F401
