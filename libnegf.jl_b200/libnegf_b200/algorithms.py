@@ -13,6 +13,7 @@ and run them in the same launches.
 import ctypes
 
 import numpy as np
+import scipy.sparse as sp
 
 from ._lib import check, ptr_array, int_array, load
 from .blockmatrix import (BlockMatrix, Block, bm_copy, bm_blocks_define_, dzeros, dptr, stream_handle,
@@ -359,6 +360,38 @@ def bndiag_of_inv_ddrgf_create_permuted_matrix(M, permVec):
         if (i, j) in M.M:
             Mhat.M[(permVec[i], permVec[j])] = M.M[(i, j)]
     return Mhat
+
+
+def bndiag_of_inv_ddrgf_create_sparse_permutator(permVec, blockSizes):
+    """bndiag_of_inv_ddrgf_create_sparse_permutator (blockmatrix.jl:194-222):
+    the sparse permutation matrix P (n x n, n the sum of the block sizes)
+    whose identity block for layer j sits at the rows of its new position
+    permVec[j] (0-based), so that P M P^T is the element form of
+    bndiag_of_inv_ddrgf_create_permuted_matrix(M, permVec)."""
+    npl = len(blockSizes)
+    sizes_perm = [0] * npl
+    for i in range(npl):
+        sizes_perm[permVec[i]] = blockSizes[i]
+    off_p = np.concatenate([[0], np.cumsum(sizes_perm)]).astype(int)
+    off = np.concatenate([[0], np.cumsum(blockSizes)]).astype(int)
+    rows, cols = [], []
+    for j in range(npl):
+        i = permVec[j]
+        rows.extend(range(off_p[i], off_p[i + 1]))
+        cols.extend(range(off[j], off[j + 1]))
+    n = int(off[-1])
+    return sp.csc_matrix((np.ones(n, dtype=np.complex128), (rows, cols)), shape=(n, n))
+
+
+def check_if_enough_mem_ddrgf(npl, blockSize, itemsize=8):
+    """check_if_enough_mem_ddrgf (ddrgf_utils.jl:1-34): the memory estimate
+    of DDRGF in MB -- the RGF buffers (1 block-diagonal, 3 block-tridiagonal)
+    plus DDRGF's own (buffTHat and buffMout, and one block diagonal for its
+    other allocations).  The reference's comparison against 80 % of the
+    memory is disabled there, so this raises nothing either; it returns the
+    estimate."""
+    return (required_mem_non_symm(npl, itemsize, 1, 3, blockSize) +
+            required_mem_non_symm(npl, itemsize, 1, 2, blockSize))
 
 
 def bndiag_of_inv_ddrgf_check_nr_threads(nrThreads, nrTasks):

@@ -475,6 +475,109 @@ def get_row_sizes(A, npl):
     return [A[(i, i)].row for i in range(npl)]
 
 
+def _block_dims(A):
+    """(rows, cols) of a block dict: one past its largest assigned indices
+    (a Julia Matrix{Block} carries its size; the dict does not)."""
+    if not A:
+        return 0, 0
+    return 1 + max(i for i, _ in A), 1 + max(j for _, j in A)
+
+
+def _ends(A, rowE, colE):
+    r, c = _block_dims(A)
+    return (r - 1 if rowE is None else rowE), (c - 1 if colE is None else colE)
+
+
+def get_rc_index(A, nrows=None, ncols=None):
+    """get_rc_index (block.jl:348-364): the row and column indices (0-based)
+    of the assigned blocks among the first nrows rows and ncols columns,
+    row by row."""
+    r, c = _block_dims(A)
+    nrows = r if nrows is None else nrows
+    ncols = c if ncols is None else ncols
+    rows, cols = [], []
+    for i in range(nrows):
+        for j in range(ncols):
+            if (i, j) in A:
+                rows.append(i)
+                cols.append(j)
+    return rows, cols
+
+
+def get_rc_index_at_(rcInd, A, rowB=0, rowE=None, colB=0, colE=None, flag_row=True):
+    """get_rc_index_at! (block.jl:377-394): rcInd (emptied first) receives the
+    row (flag_row) or column index of every assigned block in rows
+    rowB..rowE and columns colB..colE (0-based, ends included as in the
+    reference's ranges), row by row."""
+    rowE, colE = _ends(A, rowE, colE)
+    del rcInd[:]
+    for i in range(rowB, rowE + 1):
+        for j in range(colB, colE + 1):
+            if (i, j) in A:
+                rcInd.append(i if flag_row else j)
+
+
+def get_rc_index_at(A, rowB=0, rowE=None, colB=0, colE=None, flag_row=True):
+    """get_rc_index_at (block.jl:396-412): the list get_rc_index_at_ fills."""
+    out = []
+    get_rc_index_at_(out, A, rowB, rowE, colB, colE, flag_row)
+    return out
+
+
+def _index_at(A, rowB, rowE, colB, colE, flag_row):
+    rowE, colE = _ends(A, rowE, colE)
+    slots = (rowE - rowB + 1) if flag_row else (colE - colB + 1)
+    out = get_rc_index_at(A, rowB, rowE, colB, colE, flag_row)
+    if len(out) > max(slots, 0):
+        # the reference writes into a vector of that many slots (BoundsError)
+        raise IndexError("more assigned blocks than %s in the range" % ("rows" if flag_row else "columns"))
+    return out
+
+
+def get_row_index_at(A, rowB=0, rowE=None, colB=0, colE=None):
+    """get_row_index_at (block.jl:414-430): the row index of every assigned
+    block in the range, row by row; at most one per row of the range."""
+    return _index_at(A, rowB, rowE, colB, colE, True)
+
+
+def get_col_index_at(A, rowB=0, rowE=None, colB=0, colE=None):
+    """get_col_index_at (block.jl:432-447): the column index of every
+    assigned block in the range, row by row; at most one per column of the
+    range."""
+    return _index_at(A, rowB, rowE, colB, colE, False)
+
+
+def get_colSizes(A, npl=None):
+    """get_colSizes (block.jl:476-482): column sizes of the diagonal blocks."""
+    npl = _block_dims(A)[0] if npl is None else npl
+    return [A[(i, i)].col for i in range(npl)]
+
+
+def get_blockSizes(A, npl=None):
+    """get_blockSizes (block.jl:493-501): (row sizes, column sizes) of the
+    diagonal blocks."""
+    npl = _block_dims(A)[0] if npl is None else npl
+    return get_row_sizes(A, npl), get_colSizes(A, npl)
+
+
+def _host_block(x):
+    return None if x is None else (to_host(x) if isinstance(x, torch.Tensor) else np.asarray(x))
+
+
+def bm_equal(A, B):
+    """bm_equal (block.jl:223-243): the same blocks assigned in A and B and
+    every pair equal (shape and entries)."""
+    if set(A) != set(B):
+        return False
+    for k in A:
+        a, b = _host_block(A[k].Full), _host_block(B[k].Full)
+        if (a is None) != (b is None):
+            return False
+        if a is not None and not (a.shape == b.shape and np.array_equal(a, b)):
+            return False
+    return True
+
+
 def full(A, npl=None):
     """full(A) (block.jl:547-569): dense host matrix of a block dict."""
     if npl is None:
